@@ -1,0 +1,225 @@
+/*
+ * libgrid-b200 CUDA layer: the thin C ABI between the C host library and the
+ * sm_100a kernels.  Plain pointers, sizes and plain-old-data parameter
+ * structs only.  Every call is stream-ordered on the library's single CUDA
+ * stream and returns 0 on success or a nonzero error code (also latched in
+ * gb_last_error()).  Device pointers refer to the library's device-resident
+ * grids; the C host layer (libgrid API) maps host grids onto them.
+ *
+ * These entry points replace the reference's CUDA dispatch layer, whose
+ * wrappers return 0 (done on the GPU) or -1 (fall back to the CPU): here there
+ * is no fallback, so any nonzero status is an error.  Each declaration cites
+ * the reference wrapper or kernel it replaces.
+ */
+#ifndef LIBGRID_B200_GB_CUDA_H
+#define LIBGRID_B200_GB_CUDA_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Device arithmetic of a device buffer. */
+#define GB_FP64 0 /* complex128 / float64 storage */
+#define GB_FP32 1 /* complex64 / float32 storage */
+
+/* Grid geometry (row-major, z fastest; reference src/cgrid.c:4-7). */
+typedef struct {
+  long nx, ny, nz;
+  double step;
+  int prec; /* GB_FP64 or GB_FP32 */
+} gb_geom;
+
+/*
+ * Kinetic factor: psi_k *= scale * exp(tm * |k - k0|^2), zeroed where
+ * |k - k0|^2 >= kmax2 when cutoff != 0.  k_i = 2 pi (i or i - n) / (n step)
+ * with i <= n/2 non-negative (reference src/grid_wf_fft.c:141-193 and the
+ * cutoff variant :206-262).
+ */
+typedef struct {
+  double tm_re, tm_im;
+  double kx0, ky0, kz0;
+  double scale;
+  double kmax2;
+  int cutoff;
+} gb_kinetic;
+
+/* Potential kinds. */
+#define GB_POT_NONE 0
+#define GB_POT_COMPLEX 1 /* complex grid, rows of nz (16 B/pt in FP64) */
+#define GB_POT_REAL 2    /* real grid, padded rows of vrow = nz2 (8 B/pt) */
+
+/*
+ * Potential factor: psi *= exp(c * (cons + V + g |psi|^2)) with c complex
+ * (reference src/grid_wf.c:569-600: c = -i tstep / hbar).  When absorb != 0
+ * the time step becomes position dependent as in src/grid_wf.c:593-595 with
+ * the ramp of grid_wf_absorb (src/grid_wf.c:185-203):
+ *   c = -i ((1 - a) Re(tstep) - i Re(tstep) a) / hbar.
+ */
+typedef struct {
+  int kind;
+  const void *v; /* device pointer, or NULL for kind == GB_POT_NONE */
+  long vrow;     /* elements per (i, j) row of v */
+  double c_re, c_im;
+  double cons;
+  double g;
+  int absorb;
+  long lx, hx, ly, hy, lz, hz;
+  double treal; /* Re(tstep) / hbar, used when absorb != 0 */
+} gb_potential;
+
+/* ------------------------------------------------------------- runtime */
+int gb_init(int device);
+int gb_shutdown(void);
+int gb_last_error(void);
+const char *gb_last_error_where(void);
+void gb_clear_error(void);
+int gb_synchronize(void);
+void *gb_stream_handle(void);
+long gb_launch_count(void);
+void *gb_device_alloc(size_t bytes);
+void gb_device_free(void *p);
+void *gb_host_alloc(size_t bytes); /* page-locked when possible */
+void gb_host_free(void *p);
+int gb_h2d(void *dst, const void *src, size_t bytes);
+int gb_d2h(void *dst, const void *src, size_t bytes);
+int gb_d2d(void *dst, const void *src, size_t bytes);
+int gb_memset(void *dst, int value, size_t bytes);
+/* CUDA events on the library stream, slots 0..15 (timing). */
+int gb_event_record(int slot);
+float gb_event_elapsed_ms(int start_slot, int stop_slot);
+
+/* Precision conversion between FP64 and FP32 copies (n scalars). */
+int gb_convert_f64_to_f32(void *dst, const void *src, size_t n);
+int gb_convert_f32_to_f64(void *dst, const void *src, size_t n);
+/* Host FP64 array <-> device FP32 array (n scalars), staged on the device. */
+int gb_upload_f64_as_f32(void *dev32, const void *host64, size_t n);
+int gb_download_f32_as_f64(void *host64, const void *dev32, size_t n);
+/* Status word of the bounded device-side waits (0 = none timed out). */
+int gb_cn_error_flag(void);
+
+/* ----------------------------------------------------------------- FFT */
+/* In-place 3-D complex FFT, unnormalised, then multiplied by scale
+ * (replaces cuFFT Z2Z/C2C in src/cgrid_fft-cuda.c:41-174).  sign = -1 forward,
+ * +1 inverse. */
+int gb_fft3d(void *data, const gb_geom *g, int sign, double scale);
+
+/* One 2nd-order split-operator step K(dt/2) V(dt) K(dt/2) in place, with the
+ * FFTs, the kinetic factors (1/N folded in), the potential and the optional
+ * g |psi|^2 term fused into the line passes
+ * (replaces src/grid_wf.c:424-430 = 4 cuFFT calls + 5 kernels).
+ * kin->scale must hold the 1/(nx ny nz) normalisation. */
+int gb_split_step(void *psi, const gb_geom *g, const gb_kinetic *kin, const gb_potential *pot);
+
+/* k-space multipliers on unshifted frequencies (src/cgrid_diff.c:454-807):
+ * dst = src * (-k^2) or src * (i k_axis). */
+#define GB_K_LAPLACE 1
+#define GB_K_GRADIENT_X 2
+#define GB_K_GRADIENT_Y 3
+#define GB_K_GRADIENT_Z 4
+int gb_kspace_op(int op, void *dst, const void *src, const gb_geom *g);
+
+/* Pointwise kinetic factor on a k-space grid
+ * (src/grid_wf_fft-cuda2.cu:23-99 and :108-138). */
+int gb_kinetic_multiply(void *psi, const gb_geom *g, const gb_kinetic *kin);
+/* Pointwise potential factor on a real-space grid (src/grid_wf-cuda2.cu:26-104). */
+int gb_potential_multiply(void *psi, const gb_geom *g, const gb_potential *pot);
+
+/* Sum of |k|^2 |psi_k|^2 over the forward FFT of psi (psi unchanged), no k0
+ * shift, times fft_norm2 (src/cgrid_diff.c:817-879 after cgrid_fft).
+ * work is a device buffer of the same size as psi. */
+int gb_fft_ksq_sum(const void *psi, void *work, const gb_geom *g, double *out);
+
+/* ------------------------------------------------------- pointwise ops */
+#define GB_OP_CONST 1          /* c = d */
+#define GB_OP_SCALE 2          /* c = c * d */
+#define GB_OP_ADD_CONST 3      /* c = c + d */
+#define GB_OP_SUM 4            /* c = a + b */
+#define GB_OP_DIFF 5           /* c = a - b */
+#define GB_OP_PRODUCT 6        /* c = a * b */
+#define GB_OP_CONJ_PRODUCT 7   /* c = conj(a) * b */
+#define GB_OP_ADD_SCALED 8     /* c = c + d * a */
+#define GB_OP_ADD_SCALED_PRODUCT 9 /* c = c + d * a * b */
+#define GB_OP_COPY 10          /* c = a */
+/* Complex elementwise ops over n elements (src/cgrid-cuda2.cu:41-900). */
+int gb_complex_op(int op, void *c, const void *a, const void *b, size_t n, double d_re, double d_im, int prec);
+/* Real elementwise ops over n scalars (src/rgrid-cuda2.cu). */
+int gb_real_op(int op, void *c, const void *a, const void *b, size_t n, double d, int prec);
+
+/* Mixed real/complex ops on (nx, ny, nz) with real rows of rrow scalars
+ * (src/ngrid-cuda2.cu, src/grid_wf-cuda2.cu:111-123). */
+#define GB_MIX_REAL_TO_COMPLEX_RE 1   /* c = (complex) r */
+#define GB_MIX_PRODUCT_NORM 2         /* r = r1 * |c|^2 */
+#define GB_MIX_PRODUCT_COMPLEX_REAL 3 /* c = c * r */
+#define GB_MIX_DENSITY 4              /* r = |c|^2 */
+int gb_mixed_op(int op, void *c, void *r, const void *r1, const gb_geom *g, long rrow, int cprec, int rprec);
+
+/* Real-FFT layout helpers for the padded rgrid (src/rgrid_fft-cuda.c):
+ * pack the kz <= nz/2 half of a complex spectrum into rows of nz2 reals;
+ * rebuild the full Hermitian spectrum from such rows; take real parts. */
+int gb_r2c_pack(void *r, const void *c, const gb_geom *g);
+int gb_c2r_unpack(void *c, const void *r, const gb_geom *g);
+int gb_complex_real_part(void *r, const void *c, const gb_geom *g, long rrow);
+
+/* Absorbing-boundary blend dst = (1 - a) wr + a wi (src/grid_wf-cuda2.cu:165-176). */
+int gb_wf_merge(void *dst, const void *wr, const void *wi, const gb_geom *g, long lx, long hx, long ly, long hy, long lz, long hz);
+
+/* ---------------------------------------------------------- reductions */
+/* Deterministic FP64 reductions over the (nx, ny, nz) grid; out[0..1] gets
+ * the (complex) sum without the step^d factor (src/cgrid-cuda2.cu:914-1395,
+ * src/ngrid-cuda2.cu:511). */
+#define GB_RED_SUM 1          /* sum a (complex) */
+#define GB_RED_NORM2 2        /* sum |a|^2 */
+#define GB_RED_CONJ_PRODUCT 3 /* sum conj(a) b (complex) */
+#define GB_RED_EXPECT_COMPLEX 4 /* sum |a|^2 b, b complex */
+#define GB_RED_EXPECT_REAL 5  /* sum |a|^2 b, b real with rows of brow */
+#define GB_RED_REAL_SUM 6     /* sum a, a real with rows of arow */
+#define GB_RED_KSQ_NORM2 7    /* sum |k|^2 |a|^2 on the unshifted frequency grid */
+int gb_reduce(int op, const void *a, const void *b, const gb_geom *g, long arow, long brow, int bprec, double *out);
+
+/* --------------------------------------------------- finite differences */
+#define GB_BC_DIRICHLET 0
+#define GB_BC_NEUMANN 1
+#define GB_BC_PERIODIC 2
+#define GB_FD_LAPLACE 1
+#define GB_FD_LAPLACE_X 2
+#define GB_FD_LAPLACE_Y 3
+#define GB_FD_LAPLACE_Z 4
+#define GB_FD_GRADIENT_X 5
+#define GB_FD_GRADIENT_Y 6
+#define GB_FD_GRADIENT_Z 7
+/* dst = stencil(src) with boundary values per bc (Dirichlet constant
+ * outside = (out_re, out_im)); coef = 1/h^2 (Laplacians) or 1/(2h)
+ * (gradients).  is_real selects real padded rows of row scalars
+ * (src/cgrid_diff.c:201-442, src/rgrid_diff.c:309-343). */
+int gb_fd(int op, void *dst, const void *src, const gb_geom *g, int bc, double out_re, double out_im, double coef, int is_real, long row);
+/* sum conj(psi) * Laplacian_FD(psi) without writing the Laplacian
+ * (src/grid_wf_cn.c:37-49 fused). */
+int gb_fd_kinetic_sum(const void *psi, const gb_geom *g, int bc, double out_re, double out_im, double inv_h2, double *out);
+
+/* --------------------------------------------------------- Crank-Nicolson */
+/*
+ * One dimension-split Crank-Nicolson kinetic step exp(-i T tstep / hbar) on
+ * psi in place (src/grid_wf_cn.c:65-469 with src/linalg.c:62-92 and
+ * :206-230), including the reference's end-row quirks.  pre and post are
+ * optional potential factors applied before the x sweep and after the z
+ * sweep (kind GB_POT_NONE to skip).
+ */
+typedef struct {
+  int boundary;             /* WF_DIRICHLET_BOUNDARY=1, NEUMANN=2, PERIODIC=3 */
+  double tstep_re, tstep_im;
+  double mass;
+  double kx0, ky0, kz0;
+  double omega;
+  double x0, y0;
+  int absorb;
+  long lx, hx, ly, hy, lz, hz;
+} gb_cn_params;
+int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, const gb_potential *pre, const gb_potential *post);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,142 @@
+// Shared device helpers for the libgrid-b200 CUDA layer (sm_100a).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "gb_cuda.h"
+
+// Complex storage type per arithmetic precision.
+template <typename T> struct cplx_of;
+template <> struct cplx_of<double> { using type = double2; };
+template <> struct cplx_of<float> { using type = float2; };
+template <typename T> using C2 = typename cplx_of<T>::type;
+
+template <typename T2> __device__ __forceinline__ T2 cadd(T2 a, T2 b) { return T2{a.x + b.x, a.y + b.y}; }
+template <typename T2> __device__ __forceinline__ T2 csub(T2 a, T2 b) { return T2{a.x - b.x, a.y - b.y}; }
+template <typename T2> __device__ __forceinline__ T2 cmul(T2 a, T2 b) {
+  return T2{a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+// conj(a) * b
+template <typename T2> __device__ __forceinline__ T2 cconjmul(T2 a, T2 b) {
+  return T2{a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x};
+}
+template <typename T2, typename S> __device__ __forceinline__ T2 cscale(T2 a, S s) { return T2{a.x * s, a.y * s}; }
+template <typename T2> __device__ __forceinline__ auto cnorm2(T2 a) { return a.x * a.x + a.y * a.y; }
+
+// Multiply by S*i (S = -1 forward, +1 inverse transform sign).
+template <int S, typename T2> __device__ __forceinline__ T2 mul_si(T2 a) {
+  if constexpr (S > 0) return T2{-a.y, a.x};
+  else return T2{a.y, -a.x};
+}
+
+// Complex division a / b with scaling against overflow (FP64 use).
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+  double s = fabs(b.x) + fabs(b.y);
+  double inv_s = 1.0 / s;
+  double br = b.x * inv_s, bi = b.y * inv_s;
+  double ar = a.x * inv_s, ai = a.y * inv_s;
+  double d = br * br + bi * bi;
+  return double2{(ar * br + ai * bi) / d, (ai * br - ar * bi) / d};
+}
+
+template <typename T> __device__ __forceinline__ C2<T> to_c2(double re, double im) {
+  return C2<T>{(T) re, (T) im};
+}
+
+// 2 pi split into a double-rounded leading part and the rounded remainder
+// (Cody-Waite style), used to reduce phase arguments in FP64 before the FP32
+// sincosf of the FP32 propagation mode.  HI = RN(2 pi); LO = RN(2 pi - HI).
+#define GB_TWO_PI_HI 6.283185307179586231995926937088
+#define GB_TWO_PI_LO 2.4492935982947063e-16
+#define GB_INV_TWO_PI 0.15915494309189533577
+
+// exp(a + i b) as a complex number of type T, with both a and b evaluated in
+// FP64.  FP64 mode: exp and sincos in FP64.  FP32 mode: b is reduced into
+// [-pi, pi] in FP64, then sincosf/expf in FP32.
+template <typename T> __device__ __forceinline__ C2<T> cexp_phase(double a, double b, bool has_a) {
+  if constexpr (sizeof(T) == 8) {
+    double s, c;
+    sincos(b, &s, &c);
+    if (has_a) {
+      double m = exp(a);
+      return C2<T>{m * c, m * s};
+    }
+    return C2<T>{c, s};
+  } else {
+    double n = rint(b * GB_INV_TWO_PI);
+    double r = fma(-n, GB_TWO_PI_HI, b);
+    r = fma(-n, GB_TWO_PI_LO, r);
+    float s, c;
+    sincosf((float) r, &s, &c);
+    if (has_a) {
+      float m = (float) exp(a);
+      return C2<T>{m * c, m * s};
+    }
+    return C2<T>{c, s};
+  }
+}
+
+// Host-side launch bookkeeping (defined in gb_runtime.cu).
+extern "C" void gb__count_launch(void);
+extern "C" int gb__set_error(int code, const char *where);
+extern "C" cudaStream_t gb__stream(void);
+
+#define GB_CHECK_LAUNCH(where)                                     \
+  do {                                                             \
+    gb__count_launch();                                            \
+    cudaError_t e_ = cudaGetLastError();                           \
+    if (e_ != cudaSuccess) return gb__set_error((int) e_, where);  \
+  } while (0)
+
+// ------------------------------------------------------------------------
+// Bulk asynchronous copies (TMA, non-tensor form) and mbarriers.
+// All waits are bounded: after GB_WAIT_LIMIT polls the caller gets `false`
+// and must record an error and leave without touching the data.
+#define GB_WAIT_LIMIT (1u << 22)
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned) __cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned phase) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(phase)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned phase) {
+  for (unsigned it = 0; it < GB_WAIT_LIMIT; it++)
+    if (mbar_try_wait(bar, phase)) return true;
+  return false;
+}
+// global -> shared, completion signalled on bar (bytes multiple of 16,
+// both addresses 16-byte aligned)
+__device__ __forceinline__ void bulk_g2s(void *sdst, const void *gsrc, unsigned bytes, uint64_t *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(sdst)),
+               "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+// shared -> global in the calling thread's bulk group
+__device__ __forceinline__ void bulk_s2g(void *gdst, const void *ssrc, unsigned bytes) {
+  asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_u32(ssrc)), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+#define GB_TRYC(x)          \
+  do {                      \
+    int rc_ = (x);          \
+    if (rc_) return rc_;    \
+  } while (0)

@@ -1,0 +1,246 @@
+// C ABI for the FFT / split-operator path, kinetic-factor tables, the
+// standalone pointwise kinetic and potential factors, and the deterministic
+// partial-sum finisher.
+#include <math.h>
+#include <string.h>
+
+#include "gb_fft_impl.cuh"
+#include "gb_internal_cuda.h"
+
+using gbfft::PassArgs;
+
+// ---------------------------------------------------------- kinetic tables
+
+// Per-axis kinetic quantities, one thread per (axis, index):
+//   k = (i <= n/2 ? i : i - n) * l - k0,   l = 2 pi / (n step)
+//   ksq = k^2, fac = exp(tm * k^2)
+// (reference src/grid_wf_fft.c:152-190).
+template <typename T>
+__global__ void k_kin_tables(C2<T> *fac, double *ksq, long nx, long ny, long nz, double lx, double ly, double lz,
+                             double kx0, double ky0, double kz0, double tm_re, double tm_im) {
+  const long tot = nx + ny + nz;
+  for (long t = blockIdx.x * (long) blockDim.x + threadIdx.x; t < tot; t += (long) gridDim.x * blockDim.x) {
+    long n, i;
+    double l, k0;
+    if (t < nx) {
+      n = nx;
+      i = t;
+      l = lx;
+      k0 = kx0;
+    } else if (t < nx + ny) {
+      n = ny;
+      i = t - nx;
+      l = ly;
+      k0 = ky0;
+    } else {
+      n = nz;
+      i = t - nx - ny;
+      l = lz;
+      k0 = kz0;
+    }
+    const double k = (i <= n / 2 ? (double) i : (double) (i - n)) * l - k0;
+    const double k2 = k * k;
+    ksq[t] = k2;
+    double s, c;
+    sincos(tm_im * k2, &s, &c);
+    const double m = (tm_re != 0.0) ? exp(tm_re * k2) : 1.0;
+    fac[t] = C2<T>{(T) (m * c), (T) (m * s)};
+  }
+}
+
+struct KinKey {
+  long nx, ny, nz;
+  double step, tm_re, tm_im, kx0, ky0, kz0;
+  int prec, unshifted;
+};
+static KinKey g_kin_key;
+static bool g_kin_valid = false;
+
+int gb__kin_tables(const gb_geom *g, const gb_kinetic *kin, int unshifted, GbKinTables *out) {
+  const long tot = g->nx + g->ny + g->nz;
+  const size_t facb = (size_t) tot * 16, sqb = (size_t) tot * 8;
+  unsigned char *base = (unsigned char *) gb__scratch(GB_SCR_KIN, facb + sqb);
+  if (!base) return gb_last_error();
+  KinKey key;
+  memset(&key, 0, sizeof(key));
+  key.nx = g->nx;
+  key.ny = g->ny;
+  key.nz = g->nz;
+  key.step = g->step;
+  key.tm_re = unshifted ? 0.0 : kin->tm_re;
+  key.tm_im = unshifted ? 0.0 : kin->tm_im;
+  key.kx0 = unshifted ? 0.0 : kin->kx0;
+  key.ky0 = unshifted ? 0.0 : kin->ky0;
+  key.kz0 = unshifted ? 0.0 : kin->kz0;
+  key.prec = g->prec;
+  key.unshifted = unshifted;
+  double *ksq = (double *) (base + facb);
+  const size_t esz = (g->prec == GB_FP32) ? 8 : 16;
+  if (!g_kin_valid || memcmp(&key, &g_kin_key, sizeof(key)) != 0) {
+    const double lx = 2.0 * M_PI / (g->step * (double) g->nx);
+    const double ly = 2.0 * M_PI / (g->step * (double) g->ny);
+    const double lz = 2.0 * M_PI / (g->step * (double) g->nz);
+    const unsigned nb = (unsigned) ((tot + 255) / 256);
+    if (g->prec == GB_FP32)
+      k_kin_tables<float><<<nb, 256, 0, gb__stream()>>>((float2 *) base, ksq, g->nx, g->ny, g->nz, lx, ly, lz,
+                                                         key.kx0, key.ky0, key.kz0, key.tm_re, key.tm_im);
+    else
+      k_kin_tables<double><<<nb, 256, 0, gb__stream()>>>((double2 *) base, ksq, g->nx, g->ny, g->nz, lx, ly, lz,
+                                                          key.kx0, key.ky0, key.kz0, key.tm_re, key.tm_im);
+    GB_CHECK_LAUNCH("kinetic tables");
+    g_kin_key = key;
+    g_kin_valid = true;
+  }
+  out->kfac[0] = base;
+  out->kfac[1] = base + esz * (size_t) g->nx;
+  out->kfac[2] = base + esz * (size_t) (g->nx + g->ny);
+  out->ksq[0] = ksq;
+  out->ksq[1] = ksq + g->nx;
+  out->ksq[2] = ksq + g->nx + g->ny;
+  return 0;
+}
+
+// ------------------------------------------------------ partial-sum finisher
+
+__global__ void k_sum_partials(const double *__restrict__ p, long n, double *out) {
+  __shared__ double sbuf[32];
+  double s = 0.0;
+  for (long i = threadIdx.x; i < n; i += blockDim.x) s += p[i];
+  double r = gbfft::block_sum<1024>(s, sbuf);
+  if (threadIdx.x == 0) *out = r;
+}
+
+int gb__sum_partials(const double *partial, long n, double *out_host) {
+  double *res = (double *) gb__scratch(GB_SCR_RESULT, 64);
+  if (!res) return gb_last_error();
+  k_sum_partials<<<1, 1024, 0, gb__stream()>>>(partial, n, res);
+  GB_CHECK_LAUNCH("sum partials");
+  return gb_d2h(out_host, res, sizeof(double));
+}
+
+// ------------------------------------------------- standalone pointwise ops
+
+// psi_k *= exp(tm |k - k0|^2) (zero beyond the cutoff), evaluated per point
+// as in src/grid_wf_fft.c:173-190 / :238-259.
+template <typename T>
+__global__ void k_kinetic_multiply(C2<T> *psi, long nx, long ny, long nz, double lx, double ly, double lz, gb_kinetic kin) {
+  const long n = nx * ny * nz;
+  for (long g = blockIdx.x * (long) blockDim.x + threadIdx.x; g < n; g += (long) gridDim.x * blockDim.x) {
+    const long k = g % nz, ij = g / nz, j = ij % ny, i = ij / ny;
+    const double kx = (i <= nx / 2 ? (double) i : (double) (i - nx)) * lx - kin.kx0;
+    const double ky = (j <= ny / 2 ? (double) j : (double) (j - ny)) * ly - kin.ky0;
+    const double kz = (k <= nz / 2 ? (double) k : (double) (k - nz)) * lz - kin.kz0;
+    const double tot = kx * kx + ky * ky + kz * kz;
+    C2<T> v = psi[g];
+    if (kin.cutoff && !(tot < kin.kmax2)) {
+      v = C2<T>{(T) 0, (T) 0};
+    } else {
+      C2<T> f = cexp_phase<T>(kin.tm_re * tot, kin.tm_im * tot, kin.tm_re != 0.0);
+      v = cmul(v, f);
+      if (kin.scale != 1.0) v = cscale(v, (T) kin.scale);
+    }
+    psi[g] = v;
+  }
+}
+
+template <typename T> __global__ void k_potential_multiply(C2<T> *psi, PassArgs a) {
+  const long n = a.nx * a.ny * a.nz;
+  for (long g = blockIdx.x * (long) blockDim.x + threadIdx.x; g < n; g += (long) gridDim.x * blockDim.x) {
+    const long k = g % a.nz, ij = g / a.nz, j = ij % a.ny, i = ij / a.ny;
+    psi[g] = gbfft::pot_factor_apply<T>(psi[g], i, j, k, a);
+  }
+}
+
+// dst = src * (-k^2) (src/cgrid_diff.c:601-665) or src * i k_axis
+// (src/cgrid_diff.c:454-599), with the reference's own expressions for k.
+template <typename T>
+__global__ void k_kspace(int op, C2<T> *dst, const C2<T> *src, long nx, long ny, long nz, double step) {
+  const long n = nx * ny * nz;
+  const double lx = 2.0 * M_PI / (step * (double) nx);
+  const double ly = 2.0 * M_PI / (step * (double) ny);
+  const double lz = 2.0 * M_PI / (step * (double) nz);
+  for (long g = blockIdx.x * (long) blockDim.x + threadIdx.x; g < n; g += (long) gridDim.x * blockDim.x) {
+    const long k = g % nz, ij = g / nz, j = ij % ny, i = ij / ny;
+    const C2<T> v = src[g];
+    C2<T> r;
+    if (op == GB_K_LAPLACE) {
+      const double kx = (i <= nx / 2 ? (double) i : (double) (i - nx)) * lx;
+      const double ky = (j <= ny / 2 ? (double) j : (double) (j - ny)) * ly;
+      const double kz = (k <= nz / 2 ? (double) k : (double) (k - nz)) * lz;
+      const T f = (T) (-(kx * kx + ky * ky + kz * kz));
+      r = cscale(v, f);
+    } else {
+      double kk;
+      if (op == GB_K_GRADIENT_X)
+        kk = 2.0 * M_PI * (double) (i <= nx / 2 ? i : i - nx) / ((double) nx * step);
+      else if (op == GB_K_GRADIENT_Y)
+        kk = 2.0 * M_PI * (double) (j <= ny / 2 ? j : j - ny) / ((double) ny * step);
+      else
+        kk = (k <= nz / 2 ? (double) k : (double) (k - nz)) * lz;
+      // v * (i kk)
+      r = C2<T>{(T) (-(double) v.y * kk), (T) ((double) v.x * kk)};
+    }
+    dst[g] = r;
+  }
+}
+
+static unsigned pw_blocks(long n) {
+  long b = (n + 255) / 256;
+  if (b > 148 * 16) b = 148 * 16;
+  return (unsigned) (b < 1 ? 1 : b);
+}
+
+// ---------------------------------------------------------------- C ABI
+
+extern "C" int gb_fft3d(void *data, const gb_geom *g, int sign, double scale) {
+  if (g->prec == GB_FP32) return gb__fft3d_t<float>(data, g, sign, scale);
+  return gb__fft3d_t<double>(data, g, sign, scale);
+}
+
+extern "C" int gb_split_step(void *psi, const gb_geom *g, const gb_kinetic *kin, const gb_potential *pot) {
+  if (g->prec == GB_FP32) return gb__split_step_t<float>(psi, g, kin, pot);
+  return gb__split_step_t<double>(psi, g, kin, pot);
+}
+
+extern "C" int gb_fft_ksq_sum(const void *psi, void *work, const gb_geom *g, double *out) {
+  if (g->prec == GB_FP32) return gb__ksq_sum_t<float>(psi, work, g, out);
+  return gb__ksq_sum_t<double>(psi, work, g, out);
+}
+
+extern "C" int gb_kspace_op(int op, void *dst, const void *src, const gb_geom *g) {
+  const long n = g->nx * g->ny * g->nz;
+  if (g->prec == GB_FP32)
+    k_kspace<float><<<pw_blocks(n), 256, 0, gb__stream()>>>(op, (float2 *) dst, (const float2 *) src, g->nx, g->ny, g->nz, g->step);
+  else
+    k_kspace<double><<<pw_blocks(n), 256, 0, gb__stream()>>>(op, (double2 *) dst, (const double2 *) src, g->nx, g->ny, g->nz,
+                                                             g->step);
+  GB_CHECK_LAUNCH("kspace op");
+  return 0;
+}
+
+extern "C" int gb_kinetic_multiply(void *psi, const gb_geom *g, const gb_kinetic *kin) {
+  const double lx = 2.0 * M_PI / (g->step * (double) g->nx);
+  const double ly = 2.0 * M_PI / (g->step * (double) g->ny);
+  const double lz = 2.0 * M_PI / (g->step * (double) g->nz);
+  const long n = g->nx * g->ny * g->nz;
+  if (g->prec == GB_FP32)
+    k_kinetic_multiply<float><<<pw_blocks(n), 256, 0, gb__stream()>>>((float2 *) psi, g->nx, g->ny, g->nz, lx, ly, lz, *kin);
+  else
+    k_kinetic_multiply<double><<<pw_blocks(n), 256, 0, gb__stream()>>>((double2 *) psi, g->nx, g->ny, g->nz, lx, ly, lz, *kin);
+  GB_CHECK_LAUNCH("kinetic multiply");
+  return 0;
+}
+
+extern "C" int gb_potential_multiply(void *psi, const gb_geom *g, const gb_potential *pot) {
+  PassArgs a;
+  memset(&a, 0, sizeof(a));
+  a.nx = g->nx;
+  a.ny = g->ny;
+  a.nz = g->nz;
+  a.pot = *pot;
+  const long n = g->nx * g->ny * g->nz;
+  if (g->prec == GB_FP32) k_potential_multiply<float><<<pw_blocks(n), 256, 0, gb__stream()>>>((float2 *) psi, a);
+  else k_potential_multiply<double><<<pw_blocks(n), 256, 0, gb__stream()>>>((double2 *) psi, a);
+  GB_CHECK_LAUNCH("potential multiply");
+  return 0;
+}

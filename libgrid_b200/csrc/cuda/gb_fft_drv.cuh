@@ -1,0 +1,147 @@
+// Pass schedules built on the line-pass engine (gb_fft_impl.cuh).
+#pragma once
+
+#include "gb_fft_impl.cuh"
+#include "gb_internal_cuda.h"
+
+namespace gbfft {
+
+struct View {
+  long outer, n, inner;
+};
+
+inline View axis_view(const gb_geom *g, int axis) {
+  if (axis == 2) return View{g->nx * g->ny, g->nz, 1};
+  if (axis == 1) return View{g->nx, g->ny, g->nz};
+  return View{1, g->nx, g->ny * g->nz};
+}
+
+inline int active_axes(const gb_geom *g, int *ax) {
+  int na = 0;
+  if (g->nz > 1) ax[na++] = 2;
+  if (g->ny > 1) ax[na++] = 1;
+  if (g->nx > 1) ax[na++] = 0;
+  return na;
+}
+
+inline PassArgs base_args(const gb_geom *g) {
+  PassArgs a;
+  memset(&a, 0, sizeof(a));
+  a.nx = g->nx;
+  a.ny = g->ny;
+  a.nz = g->nz;
+  a.scale = 1.0;
+  a.kscale = 1.0;
+  return a;
+}
+
+template <typename T, int... Ops>
+int pass(const gb_geom *g, int axis, const void *src, void *dst, PassArgs a, OpL<Ops...> ops) {
+  const View v = axis_view(g, axis);
+  a.axis = axis;
+  a.tw = gb__twiddles(v.n, g->prec);
+  if (!a.tw) return gb_last_error();
+  return launch_pass<T>(v.n, src, dst, a, v.outer, v.inner, ops);
+}
+
+#define GB_TRY(x)               \
+  do {                          \
+    int rc_ = (x);              \
+    if (rc_) return rc_;        \
+  } while (0)
+
+}  // namespace gbfft
+
+template <typename T> int gb__fft3d_t(void *data, const gb_geom *g, int sign, double scale) {
+  using namespace gbfft;
+  int ax[3];
+  const int na = active_axes(g, ax);
+  if (na == 0) {
+    if (scale != 1.0) return gb_complex_op(GB_OP_SCALE, data, nullptr, nullptr, 1, scale, 0.0, g->prec);
+    return 0;
+  }
+  PassArgs a = base_args(g);
+  a.scale = scale;
+  for (int s = 0; s < na; s++) {
+    const bool last = (s == na - 1);
+    if (sign < 0) {
+      if (last && scale != 1.0) GB_TRY((pass<T>(g, ax[s], data, data, a, OpL<OP_FWD, OP_SCALE>{})));
+      else GB_TRY((pass<T>(g, ax[s], data, data, a, OpL<OP_FWD>{})));
+    } else {
+      if (last && scale != 1.0) GB_TRY((pass<T>(g, ax[s], data, data, a, OpL<OP_INV, OP_SCALE>{})));
+      else GB_TRY((pass<T>(g, ax[s], data, data, a, OpL<OP_INV>{})));
+    }
+  }
+  return 0;
+}
+
+template <typename T>
+int gb__split_step_t(void *psi, const gb_geom *g, const gb_kinetic *kin, const gb_potential *pot) {
+  using namespace gbfft;
+  int ax[3];
+  const int na = active_axes(g, ax);
+  PassArgs a = base_args(g);
+  GbKinTables kt;
+  GB_TRY(gb__kin_tables(g, kin, 0, &kt));
+  for (int d = 0; d < 3; d++) {
+    a.kfac[d] = kt.kfac[d];
+    a.ksq[d] = kt.ksq[d];
+  }
+  a.kscale = kin->scale;
+  a.cutoff = kin->cutoff;
+  a.kmax2 = kin->kmax2;
+  const bool has_pot = (pot != nullptr);
+  if (has_pot) a.pot = *pot;
+  if (na == 0) return gb__set_error(1004, "split step: empty grid");
+  if (na == 1) {
+    if (has_pot)
+      return pass<T>(g, ax[0], psi, psi, a, OpL<OP_FWD, OP_KIN, OP_INV, OP_POT, OP_FWD, OP_KIN, OP_INV>{});
+    return pass<T>(g, ax[0], psi, psi, a, OpL<OP_FWD, OP_KIN, OP_INV, OP_FWD, OP_KIN, OP_INV>{});
+  }
+  const int last = ax[na - 1];
+  // forward along all but the outermost axis
+  for (int s = 0; s < na - 1; s++) GB_TRY((pass<T>(g, ax[s], psi, psi, a, OpL<OP_FWD>{})));
+  // outermost axis: forward, kinetic factor (1/N folded in), inverse
+  GB_TRY((pass<T>(g, last, psi, psi, a, OpL<OP_FWD, OP_KIN, OP_INV>{})));
+  for (int s = na - 2; s >= 1; s--) GB_TRY((pass<T>(g, ax[s], psi, psi, a, OpL<OP_INV>{})));
+  // innermost axis: back to real space, potential factor, forward again
+  if (has_pot) GB_TRY((pass<T>(g, ax[0], psi, psi, a, OpL<OP_INV, OP_POT, OP_FWD>{})));
+  else GB_TRY((pass<T>(g, ax[0], psi, psi, a, OpL<OP_INV, OP_FWD>{})));
+  for (int s = 1; s < na - 1; s++) GB_TRY((pass<T>(g, ax[s], psi, psi, a, OpL<OP_FWD>{})));
+  GB_TRY((pass<T>(g, last, psi, psi, a, OpL<OP_FWD, OP_KIN, OP_INV>{})));
+  for (int s = na - 2; s >= 1; s--) GB_TRY((pass<T>(g, ax[s], psi, psi, a, OpL<OP_INV>{})));
+  GB_TRY((pass<T>(g, ax[0], psi, psi, a, OpL<OP_INV>{})));
+  return 0;
+}
+
+template <typename T> int gb__ksq_sum_t(const void *psi, void *work, const gb_geom *g, double *out) {
+  using namespace gbfft;
+  int ax[3];
+  const int na = active_axes(g, ax);
+  if (na == 0) {
+    *out = 0.0;
+    return 0;
+  }
+  gb_kinetic kin;
+  memset(&kin, 0, sizeof(kin));
+  kin.scale = 1.0;
+  GbKinTables kt;
+  GB_TRY(gb__kin_tables(g, &kin, 1, &kt));
+  PassArgs a = base_args(g);
+  for (int d = 0; d < 3; d++) {
+    a.kfac[d] = kt.kfac[d];
+    a.ksq[d] = kt.ksq[d];
+  }
+  const void *src = psi;
+  for (int s = 0; s < na - 1; s++) {
+    GB_TRY((pass<T>(g, ax[s], src, work, a, OpL<OP_FWD>{})));
+    src = work;
+  }
+  const View v = axis_view(g, ax[na - 1]);
+  const long nb = blocks_for(v.n, v.outer, v.inner);
+  double *partial = (double *) gb__scratch(GB_SCR_PARTIAL, sizeof(double) * (size_t) nb);
+  if (!partial) return gb_last_error();
+  a.partial = partial;
+  GB_TRY((pass<T>(g, ax[na - 1], src, nullptr, a, OpL<OP_FWD, OP_KSQ>{})));
+  return gb__sum_partials(partial, nb, out);
+}

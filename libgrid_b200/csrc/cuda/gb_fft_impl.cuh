@@ -1,0 +1,524 @@
+// Line-pass FFT engine for the libgrid-b200 split-operator path (sm_100a).
+//
+// A 3-D grid (nx, ny, nz), z fastest, is viewed per axis as [outer][N][inner]:
+//   z: outer = nx*ny, inner = 1      (contiguous lines)
+//   y: outer = nx,    inner = nz
+//   x: outer = 1,     inner = ny*nz
+// One "pass" reads each element of the grid once from HBM, applies a short
+// program of line operations (forward/inverse FFT along the axis, kinetic
+// factor, potential factor, scale, k^2 reduction) and writes it once.
+//
+// Each line of N points is transformed by TL = N/P threads.  Thread t always
+// holds the P elements at positions t + TL*m (m < P) in registers, both on
+// entry and on exit of the transform, so the first radix stage loads straight
+// from HBM and the last stage stores straight to HBM with unit stride across
+// threads; only the exchanges between radix stages go through shared memory.
+// Stages follow the Stockham autosort scheme: with Ns the product of the
+// previous radices, butterfly j (k = j mod Ns) takes x[j + r N/R], applies
+// exp(s 2 pi i k r / (Ns R)), does a radix-R DFT and writes
+// (j - k) R + k + r Ns.  Strided passes interleave BZ adjacent columns in
+// shared memory (column index fastest, conflict-free); contiguous passes pad
+// one element every R0 so the stride-R0 writes of the first stage are
+// conflict-free.
+#pragma once
+
+#include "gb_common.cuh"
+
+namespace gbfft {
+
+enum : int { OP_END = 0, OP_FWD = 1, OP_INV = 2, OP_KIN = 3, OP_POT = 4, OP_SCALE = 5, OP_KSQ = 6 };
+
+template <int... Ops> struct OpL {};
+template <int... Rs> struct IL {};
+
+// cos(pi/8), sin(pi/8), sqrt(1/2)
+constexpr double kC1 = 0.92387953251128675613;
+constexpr double kS1 = 0.38268343236508977173;
+constexpr double kSQH = 0.70710678118654752440;
+
+// o * (wr + S i wi)
+template <int S, typename T2> __device__ __forceinline__ T2 wmul(T2 o, double wr, double wi) {
+  using T = decltype(o.x);
+  const T r = (T) wr, i = (T) (S * wi);
+  return T2{o.x * r - o.y * i, o.x * i + o.y * r};
+}
+
+template <int R, int S, typename T2> struct DFT;
+template <int S, typename T2> struct DFT<2, S, T2> {
+  static __device__ __forceinline__ void run(T2 *v) {
+    T2 a = v[0];
+    v[0] = cadd(a, v[1]);
+    v[1] = csub(a, v[1]);
+  }
+};
+template <int S, typename T2> struct DFT<4, S, T2> {
+  static __device__ __forceinline__ void run(T2 *v) {
+    T2 a0 = cadd(v[0], v[2]), a1 = csub(v[0], v[2]);
+    T2 a2 = cadd(v[1], v[3]), a3 = mul_si<S>(csub(v[1], v[3]));
+    v[0] = cadd(a0, a2);
+    v[2] = csub(a0, a2);
+    v[1] = cadd(a1, a3);
+    v[3] = csub(a1, a3);
+  }
+};
+template <int S, typename T2> struct DFT<8, S, T2> {
+  static __device__ __forceinline__ void run(T2 *v) {
+    T2 e[4] = {v[0], v[2], v[4], v[6]};
+    T2 o[4] = {v[1], v[3], v[5], v[7]};
+    DFT<4, S, T2>::run(e);
+    DFT<4, S, T2>::run(o);
+    o[1] = wmul<S>(o[1], kSQH, kSQH);
+    o[2] = mul_si<S>(o[2]);
+    o[3] = wmul<S>(o[3], -kSQH, kSQH);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+      v[k] = cadd(e[k], o[k]);
+      v[k + 4] = csub(e[k], o[k]);
+    }
+  }
+};
+template <int S, typename T2> struct DFT<16, S, T2> {
+  static __device__ __forceinline__ void run(T2 *v) {
+    T2 e[8], o[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      e[k] = v[2 * k];
+      o[k] = v[2 * k + 1];
+    }
+    DFT<8, S, T2>::run(e);
+    DFT<8, S, T2>::run(o);
+    o[1] = wmul<S>(o[1], kC1, kS1);
+    o[2] = wmul<S>(o[2], kSQH, kSQH);
+    o[3] = wmul<S>(o[3], kS1, kC1);
+    o[4] = mul_si<S>(o[4]);
+    o[5] = wmul<S>(o[5], -kS1, kC1);
+    o[6] = wmul<S>(o[6], -kSQH, kSQH);
+    o[7] = wmul<S>(o[7], -kC1, kS1);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+      v[k] = cadd(e[k], o[k]);
+      v[k + 8] = csub(e[k], o[k]);
+    }
+  }
+};
+
+// Radix schedule per line length: P = registers (elements) per thread.
+template <int N> struct Sched;
+template <> struct Sched<2> { static constexpr int P = 2; using R = IL<2>; };
+template <> struct Sched<4> { static constexpr int P = 4; using R = IL<4>; };
+template <> struct Sched<8> { static constexpr int P = 8; using R = IL<8>; };
+template <> struct Sched<16> { static constexpr int P = 16; using R = IL<16>; };
+template <> struct Sched<32> { static constexpr int P = 8; using R = IL<8, 4>; };
+template <> struct Sched<64> { static constexpr int P = 8; using R = IL<8, 8>; };
+template <> struct Sched<128> { static constexpr int P = 16; using R = IL<16, 8>; };
+template <> struct Sched<256> { static constexpr int P = 16; using R = IL<16, 16>; };
+template <> struct Sched<512> { static constexpr int P = 8; using R = IL<8, 8, 8>; };
+template <> struct Sched<1024> { static constexpr int P = 16; using R = IL<16, 16, 4>; };
+template <> struct Sched<2048> { static constexpr int P = 16; using R = IL<16, 16, 8>; };
+template <> struct Sched<4096> { static constexpr int P = 16; using R = IL<16, 16, 16>; };
+
+template <int R0, int... Rest> __host__ __device__ constexpr int first_radix(IL<R0, Rest...>) { return R0; }
+
+__host__ __device__ constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v / 2); }
+
+// Shared-memory views.
+template <typename T2, int BZ> struct SmStrided {
+  T2 *p;
+  __device__ __forceinline__ T2 &operator()(int pos) const { return p[pos * BZ]; }
+};
+template <typename T2, int SH> struct SmContig {
+  T2 *p;
+  __device__ __forceinline__ T2 &operator()(int pos) const { return p[pos + (pos >> SH)]; }
+};
+
+// One Stockham stage; v holds positions t + TL*m on entry and exit.
+template <typename T2, int S, int N, int P, int NS, int R, bool FIRST, bool LAST, class SM>
+__device__ __forceinline__ void fft_stage(T2 (&v)[P], int t, const SM &sm, const T2 *__restrict__ tw) {
+  constexpr int TL = N / P;
+  constexpr int B = P / R;
+#pragma unroll
+  for (int u = 0; u < B; u++) {
+    const int j = t + u * TL;
+    const int k = j & (NS - 1);
+    T2 w[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) w[r] = v[u + r * B];
+    if constexpr (!FIRST) {
+      constexpr int STRIDE = N / (NS * R);
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        T2 tt = tw[k * r * STRIDE];
+        if constexpr (S > 0) tt.y = -tt.y;
+        w[r] = cmul(w[r], tt);
+      }
+    }
+    DFT<R, S, T2>::run(w);
+    if constexpr (LAST) {
+#pragma unroll
+      for (int r = 0; r < R; r++) v[u + r * B] = w[r];
+    } else {
+      const int base = (j - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; r++) sm(base + r * NS) = w[r];
+    }
+  }
+  if constexpr (!LAST) {
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < P; m++) v[m] = sm(t + TL * m);
+    __syncthreads();
+  }
+}
+
+template <typename T2, int S, int N, int P, int NS, bool FIRST, class SM, int R0, int... Rest>
+__device__ __forceinline__ void fft_run(T2 (&v)[P], int t, const SM &sm, const T2 *tw, IL<R0, Rest...>) {
+  fft_stage<T2, S, N, P, NS, R0, FIRST, (sizeof...(Rest) == 0), SM>(v, t, sm, tw);
+  if constexpr (sizeof...(Rest) > 0) fft_run<T2, S, N, P, NS * R0, false, SM>(v, t, sm, tw, IL<Rest...>{});
+}
+
+template <typename T2, int S, int N, class SM>
+__device__ __forceinline__ void fft_line(T2 (&v)[Sched<N>::P], int t, const SM &sm, const T2 *tw) {
+  fft_run<T2, S, N, Sched<N>::P, 1, true, SM>(v, t, sm, tw, typename Sched<N>::R{});
+}
+
+// Arguments shared by all pass kernels (plain data, passed by value).
+struct PassArgs {
+  long nx, ny, nz;
+  int axis;             // 0 = x, 1 = y, 2 = z
+  const void *tw;       // twiddle table exp(-2 pi i m / N), element type T2
+  const void *kfac[3];  // per-axis kinetic factors exp(tm k_a^2) (T2)
+  const double *ksq[3]; // per-axis k_a^2 (double), cutoff only
+  double kmax2;
+  int cutoff;
+  double kscale;        // real scale folded into the kinetic factor
+  double scale;         // OP_SCALE
+  gb_potential pot;
+  double *partial;      // OP_KSQ: one partial sum per block
+};
+
+// Decode (i, j, k) of axis position p for a line given by (o, q).
+__device__ __forceinline__ void decode(const PassArgs &a, long o, int p, long q, long &i, long &j, long &k) {
+  if (a.axis == 2) {
+    i = o / a.ny;
+    j = o - i * a.ny;
+    k = p;
+  } else if (a.axis == 1) {
+    i = o;
+    j = p;
+    k = q;
+  } else {
+    i = p;
+    j = q / a.nz;
+    k = q - j * a.nz;
+  }
+}
+
+__device__ __forceinline__ double absorb_ramp(long i, long j, long k, const gb_potential &pt) {
+  // src/grid_wf.c:185-203
+  double t = 0.0;
+  if (i < pt.lx) t += (double) (pt.lx - i) / (double) pt.lx;
+  else if (i > pt.hx) t += (double) (i - pt.hx) / (double) pt.lx;
+  if (j < pt.ly) t += (double) (pt.ly - j) / (double) pt.ly;
+  else if (j > pt.hy) t += (double) (j - pt.hy) / (double) pt.ly;
+  if (k < pt.lz) t += (double) (pt.lz - k) / (double) pt.lz;
+  else if (k > pt.hz) t += (double) (k - pt.hz) / (double) pt.lz;
+  t *= 2.0 / 3.0;
+  return t > 1.0 ? 1.0 : t;
+}
+
+// psi * exp(c (cons + V + g |psi|^2)) for one element (src/grid_wf.c:593-597).
+template <typename T>
+__device__ __forceinline__ C2<T> pot_factor_apply(C2<T> x, long i, long j, long k, const PassArgs &a) {
+  const gb_potential &pt = a.pot;
+  double wr = pt.cons, wi = 0.0;
+  const long vidx = (i * a.ny + j) * pt.vrow + k;
+  if (pt.kind == GB_POT_COMPLEX) {
+    const C2<T> vv = ((const C2<T> *) pt.v)[vidx];
+    wr += (double) vv.x;
+    wi += (double) vv.y;
+  } else if (pt.kind == GB_POT_REAL) {
+    wr += (double) ((const T *) pt.v)[vidx];
+  }
+  if (pt.g != 0.0) wr += pt.g * ((double) x.x * (double) x.x + (double) x.y * (double) x.y);
+  double cr = pt.c_re, ci = pt.c_im;
+  if (pt.absorb) {
+    const double am = absorb_ramp(i, j, k, pt);
+    cr = -pt.treal * am;
+    ci = -pt.treal * (1.0 - am);
+  }
+  const double ar = cr * wr - ci * wi;
+  const double ai = cr * wi + ci * wr;
+  return cmul(x, cexp_phase<T>(ar, ai, ar != 0.0));
+}
+
+template <int Op, int... Rest> struct OpsHead {
+  static constexpr int value = Op;
+};
+
+// Apply the program OpL<...> to a thread's register line.
+template <typename T, int N, class SM, int... Ops> struct Program;
+
+template <typename T, int N, class SM> struct Program<T, N, SM> {
+  // o, q identify the line; thread holds positions t + TL*m
+  static __device__ __forceinline__ void run(C2<T> (&)[Sched<N>::P], int, const SM &, const PassArgs &, long, long,
+                                             double &) {}
+};
+
+template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N, SM, Op, Rest...> {
+  static __device__ __forceinline__ void run(C2<T> (&v)[Sched<N>::P], int t, const SM &sm, const PassArgs &a, long o,
+                                             long q, double &acc) {
+    using T2 = C2<T>;
+    constexpr int P = Sched<N>::P;
+    constexpr int TL = N / P;
+    const T2 *tw = (const T2 *) a.tw;
+    if constexpr (Op == OP_FWD) {
+      fft_line<T2, -1, N>(v, t, sm, tw);
+    } else if constexpr (Op == OP_INV) {
+      fft_line<T2, +1, N>(v, t, sm, tw);
+    } else if constexpr (Op == OP_SCALE) {
+      const T s = (T) a.scale;
+#pragma unroll
+      for (int m = 0; m < P; m++) v[m] = cscale(v[m], s);
+    } else if constexpr (Op == OP_KIN) {
+      // Line factor from the two other axes, times kscale; element factor
+      // from the pass axis.
+      long i, j, k;
+      decode(a, o, 0, q, i, j, k);
+      const int ax = a.axis;
+      const int b0 = (ax == 0) ? 1 : 0, b1 = (ax == 2) ? 1 : 2;
+      const long idx[3] = {i, j, k};
+      const T2 *fa = (const T2 *) a.kfac[ax];
+      const T2 f0 = ((const T2 *) a.kfac[b0])[idx[b0]];
+      const T2 f1 = ((const T2 *) a.kfac[b1])[idx[b1]];
+      T2 lf = cmul(f0, f1);
+      lf = cscale(lf, (T) a.kscale);
+      double k2line = 0.0;
+      if (a.cutoff) k2line = a.ksq[b0][idx[b0]] + a.ksq[b1][idx[b1]];
+#pragma unroll
+      for (int m = 0; m < P; m++) {
+        const int p = t + TL * m;
+        T2 f = cmul(lf, fa[p]);
+        if (a.cutoff && (k2line + a.ksq[ax][p] >= a.kmax2)) f = T2{(T) 0, (T) 0};
+        v[m] = cmul(v[m], f);
+      }
+    } else if constexpr (Op == OP_POT) {
+#pragma unroll
+      for (int m = 0; m < P; m++) {
+        long i, j, k;
+        decode(a, o, t + TL * m, q, i, j, k);
+        v[m] = pot_factor_apply<T>(v[m], i, j, k, a);
+      }
+    } else if constexpr (Op == OP_KSQ) {
+      // sum |k|^2 |v|^2 with k from the unshifted frequency grid
+      long i, j, k;
+      decode(a, o, 0, q, i, j, k);
+      const int ax = a.axis;
+      const int b0 = (ax == 0) ? 1 : 0, b1 = (ax == 2) ? 1 : 2;
+      const long idx[3] = {i, j, k};
+      const double k2line = a.ksq[b0][idx[b0]] + a.ksq[b1][idx[b1]];
+#pragma unroll
+      for (int m = 0; m < P; m++) {
+        const int p = t + TL * m;
+        acc += (k2line + a.ksq[ax][p]) * ((double) v[m].x * (double) v[m].x + (double) v[m].y * (double) v[m].y);
+      }
+    }
+    Program<T, N, SM, Rest...>::run(v, t, sm, a, o, q, acc);
+  }
+};
+
+template <int... Ops> __host__ __device__ constexpr bool has_ksq(OpL<Ops...>) { return ((Ops == OP_KSQ) || ...); }
+
+// Deterministic block sum (fixed shuffle tree, fixed warp order).
+template <int THREADS> __device__ __forceinline__ double block_sum(double v, double *sbuf) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+  constexpr int NW = (THREADS + 31) / 32;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) sbuf[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0) {
+#pragma unroll 1
+    for (int q = 0; q < NW; q++) r += sbuf[q];
+  }
+  return r;
+}
+
+// ---------------------------------------------------------------- kernels
+
+template <int N> struct ContigCfg {
+  static constexpr int P = Sched<N>::P;
+  static constexpr int TL = N / P;
+  static constexpr int L = (256 / TL) > 0 ? (256 / TL) : 1;
+  static constexpr int THREADS = TL * L;
+  static constexpr int SH = ilog2c(first_radix(typename Sched<N>::R{}));
+  static constexpr int LINE = N + (N >> SH);
+};
+
+// Contiguous lines (inner == 1): L lines of N per block.
+template <typename T, int N, int... Ops>
+__global__ void __launch_bounds__(ContigCfg<N>::THREADS)
+    k_pass_contig(const C2<T> *__restrict__ src, C2<T> *__restrict__ dst, long nlines, PassArgs a) {
+  using T2 = C2<T>;
+  using Cfg = ContigCfg<N>;
+  constexpr int P = Cfg::P, TL = Cfg::TL;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T2 *smem = (T2 *) smraw;
+  const int t = threadIdx.x % TL;
+  const int l = threadIdx.x / TL;
+  const long line = (long) blockIdx.x * Cfg::L + l;
+  const bool ok = line < nlines;
+  const T2 *s = src + line * N;
+  T2 v[P];
+#pragma unroll
+  for (int m = 0; m < P; m++) v[m] = ok ? s[t + TL * m] : T2{(T) 0, (T) 0};
+  SmContig<T2, Cfg::SH> sm{smem + l * Cfg::LINE};
+  double acc = 0.0;
+  Program<T, N, SmContig<T2, Cfg::SH>, Ops...>::run(v, t, sm, a, ok ? line : 0, 0, acc);
+  if constexpr (has_ksq(OpL<Ops...>{})) {
+    __shared__ double sbuf[(Cfg::THREADS + 31) / 32];
+    double r = block_sum<Cfg::THREADS>(ok ? acc : 0.0, sbuf);
+    if (threadIdx.x == 0) a.partial[blockIdx.x] = r;
+  } else {
+    if (ok) {
+      T2 *d = dst + line * N;
+#pragma unroll
+      for (int m = 0; m < P; m++) d[t + TL * m] = v[m];
+    }
+  }
+}
+
+template <int N> struct StridedCfg {
+  static constexpr int P = Sched<N>::P;
+  static constexpr int TL = N / P;
+  static constexpr int BZ = (N <= 256) ? 16 : ((N <= 512) ? 8 : 4);
+  static constexpr int THREADS = TL * BZ;
+};
+
+// Strided lines: block = (column block of BZ adjacent inner indices, outer).
+template <typename T, int N, int BZ, int... Ops>
+__global__ void __launch_bounds__((N / Sched<N>::P) * BZ)
+    k_pass_strided(const C2<T> *__restrict__ src, C2<T> *__restrict__ dst, long inner, PassArgs a) {
+  using T2 = C2<T>;
+  constexpr int P = Sched<N>::P, TL = N / P;
+  constexpr int THREADS = TL * BZ;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T2 *smem = (T2 *) smraw;
+  const int c = threadIdx.x % BZ;
+  const int t = threadIdx.x / BZ;
+  const long o = blockIdx.y;
+  const long q = (long) blockIdx.x * BZ + c;
+  const long off = o * (long) N * inner + q;
+  const T2 *s = src + off;
+  T2 v[P];
+#pragma unroll
+  for (int m = 0; m < P; m++) v[m] = s[(long) (t + TL * m) * inner];
+  SmStrided<T2, BZ> sm{smem + c};
+  double acc = 0.0;
+  Program<T, N, SmStrided<T2, BZ>, Ops...>::run(v, t, sm, a, o, q, acc);
+  if constexpr (has_ksq(OpL<Ops...>{})) {
+    __shared__ double sbuf[(THREADS + 31) / 32];
+    double r = block_sum<THREADS>(acc, sbuf);
+    if (threadIdx.x == 0) a.partial[(long) blockIdx.y * gridDim.x + blockIdx.x] = r;
+  } else {
+    T2 *d = dst + off;
+#pragma unroll
+    for (int m = 0; m < P; m++) d[(long) (t + TL * m) * inner] = v[m];
+  }
+}
+
+// Launch one pass of program Ops along `axis` for line length N.
+template <typename T, int N, int... Ops>
+int launch_pass_n(const void *src, void *dst, const PassArgs &a, long outer, long inner, long *nblocks) {
+  using T2 = C2<T>;
+  cudaStream_t st = gb__stream();
+  if (inner == 1) {
+    using Cfg = ContigCfg<N>;
+    const size_t sm = (size_t) Cfg::L * Cfg::LINE * sizeof(T2);
+    auto kern = k_pass_contig<T, N, Ops...>;
+    static bool attr_set = false;
+    if (!attr_set) {
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
+      attr_set = true;
+    }
+    const long nb = (outer + Cfg::L - 1) / Cfg::L;
+    if (nblocks) *nblocks = nb;
+    kern<<<(unsigned) nb, Cfg::THREADS, sm, st>>>((const T2 *) src, (T2 *) dst, outer, a);
+  } else {
+    constexpr int BZ = StridedCfg<N>::BZ;
+    if (inner % BZ == 0 && outer <= 65535) {
+      const size_t sm = (size_t) N * BZ * sizeof(T2);
+      auto kern = k_pass_strided<T, N, BZ, Ops...>;
+      static bool attr_set = false;
+      if (!attr_set) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
+        attr_set = true;
+      }
+      dim3 grid((unsigned) (inner / BZ), (unsigned) outer);
+      if (nblocks) *nblocks = (long) grid.x * grid.y;
+      kern<<<grid, (N / Sched<N>::P) * BZ, sm, st>>>((const T2 *) src, (T2 *) dst, inner, a);
+    } else if (outer <= 65535) {
+      const size_t sm = (size_t) N * sizeof(T2);
+      auto kern = k_pass_strided<T, N, 1, Ops...>;
+      static bool attr_set = false;
+      if (!attr_set) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
+        attr_set = true;
+      }
+      dim3 grid((unsigned) inner, (unsigned) outer);
+      if (nblocks) *nblocks = (long) grid.x * grid.y;
+      kern<<<grid, N / Sched<N>::P, sm, st>>>((const T2 *) src, (T2 *) dst, inner, a);
+    } else {
+      return gb__set_error(1001, "fft pass: outer extent above 65535");
+    }
+  }
+  GB_CHECK_LAUNCH("fft pass");
+  return 0;
+}
+
+// Number of blocks a pass will launch (for sizing OP_KSQ partials).
+template <int N> long pass_blocks(long outer, long inner) {
+  if (inner == 1) return (outer + ContigCfg<N>::L - 1) / ContigCfg<N>::L;
+  constexpr int BZ = StridedCfg<N>::BZ;
+  if (inner % BZ == 0) return (inner / BZ) * outer;
+  return inner * outer;
+}
+
+template <typename T, int... Ops>
+int launch_pass(long n, const void *src, void *dst, const PassArgs &a, long outer, long inner, OpL<Ops...>) {
+  switch (n) {
+    case 2: return launch_pass_n<T, 2, Ops...>(src, dst, a, outer, inner, nullptr);
+    case 4: return launch_pass_n<T, 4, Ops...>(src, dst, a, outer, inner, nullptr);
+    case 8: return launch_pass_n<T, 8, Ops...>(src, dst, a, outer, inner, nullptr);
+    case 16: return launch_pass_n<T, 16, Ops...>(src, dst, a, outer, inner, nullptr);
+    case 32: return launch_pass_n<T, 32, Ops...>(src, dst, a, outer, inner, nullptr);
+    case 64: return launch_pass_n<T, 64, Ops...>(src, dst, a, outer, inner, nullptr);
+    case 128: return launch_pass_n<T, 128, Ops...>(src, dst, a, outer, inner, nullptr);
+    case 256: return launch_pass_n<T, 256, Ops...>(src, dst, a, outer, inner, nullptr);
+    case 512: return launch_pass_n<T, 512, Ops...>(src, dst, a, outer, inner, nullptr);
+    case 1024: return launch_pass_n<T, 1024, Ops...>(src, dst, a, outer, inner, nullptr);
+    case 2048: return launch_pass_n<T, 2048, Ops...>(src, dst, a, outer, inner, nullptr);
+    case 4096: return launch_pass_n<T, 4096, Ops...>(src, dst, a, outer, inner, nullptr);
+    default: return gb__set_error(1002, "fft pass: line length must be a power of two in [2, 4096]");
+  }
+}
+
+inline long blocks_for(long n, long outer, long inner) {
+  switch (n) {
+    case 2: return pass_blocks<2>(outer, inner);
+    case 4: return pass_blocks<4>(outer, inner);
+    case 8: return pass_blocks<8>(outer, inner);
+    case 16: return pass_blocks<16>(outer, inner);
+    case 32: return pass_blocks<32>(outer, inner);
+    case 64: return pass_blocks<64>(outer, inner);
+    case 128: return pass_blocks<128>(outer, inner);
+    case 256: return pass_blocks<256>(outer, inner);
+    case 512: return pass_blocks<512>(outer, inner);
+    case 1024: return pass_blocks<1024>(outer, inner);
+    case 2048: return pass_blocks<2048>(outer, inner);
+    case 4096: return pass_blocks<4096>(outer, inner);
+    default: return 0;
+  }
+}
+
+}  // namespace gbfft

@@ -1,0 +1,36 @@
+// Internal declarations shared by the libgrid-b200 CUDA translation units.
+#pragma once
+
+#include <stddef.h>
+
+#include "gb_cuda.h"
+
+// Library-owned device scratch slots.
+enum {
+  GB_SCR_KIN = 0,      // kinetic factor tables
+  GB_SCR_PARTIAL = 1,  // reduction partial sums
+  GB_SCR_RESULT = 2,   // final reduction results
+  GB_SCR_CN = 3,       // line-solver coefficient tables
+  GB_SCR_WORK = 4,     // temporary full grids
+  GB_SCR_STAGE = 5,    // precision-conversion staging
+  GB_SCR_COUNT = 8
+};
+
+void *gb__scratch(int slot, size_t bytes);
+const void *gb__twiddles(long n, int prec);
+
+// Kinetic factor tables for (g, kin): per-axis complex factors exp(tm k_a^2)
+// in the storage precision of g and per-axis k_a^2 in FP64.
+struct GbKinTables {
+  const void *kfac[3];
+  const double *ksq[3];
+};
+int gb__kin_tables(const gb_geom *g, const gb_kinetic *kin, int unshifted, GbKinTables *out);
+
+// Precision-specific drivers (gb_fft_f64.cu / gb_fft_f32.cu).
+template <typename T> int gb__fft3d_t(void *data, const gb_geom *g, int sign, double scale);
+template <typename T> int gb__split_step_t(void *psi, const gb_geom *g, const gb_kinetic *kin, const gb_potential *pot);
+template <typename T> int gb__ksq_sum_t(const void *psi, void *work, const gb_geom *g, double *out);
+
+// Deterministic sum of n partials into out (FP64), on the library stream.
+int gb__sum_partials(const double *partial, long n, double *out_host);

@@ -1,0 +1,265 @@
+// libgrid-b200 CUDA runtime: device selection, the library stream, error
+// latch, launch counter, memory helpers, timing events, library-owned device
+// scratch and FFT twiddle tables.
+//
+// Replaces the reference's GPU memory manager for this path (src/cuda.c):
+// one GPU, device-resident buffers owned by the host layer, no swap cache,
+// no CPU fallback.  Library scratch (twiddles, kinetic tables, reduction
+// partials, line-solver coefficients) lives in named slots that grow on
+// demand and are released at gb_shutdown.
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include "gb_common.cuh"
+#include "gb_internal_cuda.h"
+
+static int g_device = -1;
+static cudaStream_t g_stream = nullptr;
+static int g_err = 0;
+static char g_err_where[160] = "";
+static long g_launches = 0;
+static cudaEvent_t g_events[16];
+static bool g_events_made = false;
+
+struct Scratch {
+  void *p;
+  size_t bytes;
+};
+static Scratch g_scratch[GB_SCR_COUNT];
+
+struct Twiddle {
+  void *d64;
+  void *d32;
+};
+static Twiddle g_tw[13];  // index log2(n), n = 2 .. 4096
+
+extern "C" void gb__count_launch(void) { g_launches++; }
+
+extern "C" int gb__set_error(int code, const char *where) {
+  if (!g_err) {
+    g_err = code ? code : -1;
+    snprintf(g_err_where, sizeof(g_err_where), "%s", where ? where : "");
+  }
+  return g_err;
+}
+
+extern "C" cudaStream_t gb__stream(void) { return g_stream; }
+
+extern "C" int gb_init(int device) {
+  if (g_stream && device == g_device) return 0;
+  cudaError_t e = cudaSetDevice(device);
+  if (e != cudaSuccess) return gb__set_error((int) e, "cudaSetDevice");
+  e = cudaStreamCreateWithFlags(&g_stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return gb__set_error((int) e, "cudaStreamCreate");
+  g_device = device;
+  if (!g_events_made) {
+    for (int i = 0; i < 16; i++) cudaEventCreate(&g_events[i]);
+    g_events_made = true;
+  }
+  return 0;
+}
+
+extern "C" int gb_shutdown(void) {
+  if (!g_stream) return 0;
+  cudaStreamSynchronize(g_stream);
+  for (int i = 0; i < GB_SCR_COUNT; i++) {
+    if (g_scratch[i].p) cudaFree(g_scratch[i].p);
+    g_scratch[i].p = nullptr;
+    g_scratch[i].bytes = 0;
+  }
+  for (int i = 0; i < 13; i++) {
+    if (g_tw[i].d64) cudaFree(g_tw[i].d64);
+    if (g_tw[i].d32) cudaFree(g_tw[i].d32);
+    g_tw[i].d64 = g_tw[i].d32 = nullptr;
+  }
+  return 0;
+}
+
+extern "C" int gb_last_error(void) { return g_err; }
+extern "C" const char *gb_last_error_where(void) { return g_err_where; }
+extern "C" void gb_clear_error(void) {
+  g_err = 0;
+  g_err_where[0] = 0;
+}
+
+extern "C" int gb_synchronize(void) {
+  cudaError_t e = cudaStreamSynchronize(g_stream);
+  if (e != cudaSuccess) return gb__set_error((int) e, "cudaStreamSynchronize");
+  return g_err;
+}
+
+extern "C" void *gb_stream_handle(void) { return (void *) g_stream; }
+extern "C" long gb_launch_count(void) { return g_launches; }
+
+extern "C" void *gb_device_alloc(size_t bytes) {
+  void *p = nullptr;
+  cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    gb__set_error((int) e, "cudaMalloc");
+    return nullptr;
+  }
+  return p;
+}
+
+extern "C" void gb_device_free(void *p) {
+  if (p) {
+    cudaStreamSynchronize(g_stream);
+    cudaFree(p);
+  }
+}
+
+extern "C" void *gb_host_alloc(size_t bytes) {
+  void *p = nullptr;
+  if (cudaHostAlloc(&p, bytes ? bytes : 16, cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return p;
+}
+
+extern "C" void gb_host_free(void *p) {
+  if (p) cudaFreeHost(p);
+}
+
+extern "C" int gb_h2d(void *dst, const void *src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, g_stream);
+  if (e != cudaSuccess) return gb__set_error((int) e, "h2d");
+  return 0;
+}
+
+extern "C" int gb_d2h(void *dst, const void *src, size_t bytes) {
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, g_stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g_stream);
+  if (e != cudaSuccess) return gb__set_error((int) e, "d2h");
+  return 0;
+}
+
+extern "C" int gb_d2d(void *dst, const void *src, size_t bytes) {
+  if (dst == src) return 0;
+  cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, g_stream);
+  if (e != cudaSuccess) return gb__set_error((int) e, "d2d");
+  return 0;
+}
+
+extern "C" int gb_memset(void *dst, int value, size_t bytes) {
+  cudaError_t e = cudaMemsetAsync(dst, value, bytes, g_stream);
+  if (e != cudaSuccess) return gb__set_error((int) e, "memset");
+  return 0;
+}
+
+extern "C" int gb_event_record(int slot) {
+  if (slot < 0 || slot >= 16) return gb__set_error(1003, "event slot");
+  cudaError_t e = cudaEventRecord(g_events[slot], g_stream);
+  if (e != cudaSuccess) return gb__set_error((int) e, "cudaEventRecord");
+  return 0;
+}
+
+extern "C" float gb_event_elapsed_ms(int a, int b) {
+  float ms = -1.0f;
+  if (a < 0 || a >= 16 || b < 0 || b >= 16) return -1.0f;
+  cudaEventSynchronize(g_events[b]);
+  if (cudaEventElapsedTime(&ms, g_events[a], g_events[b]) != cudaSuccess) {
+    cudaGetLastError();
+    return -1.0f;
+  }
+  return ms;
+}
+
+void *gb__scratch(int slot, size_t bytes) {
+  if (slot < 0 || slot >= GB_SCR_COUNT) return nullptr;
+  Scratch &s = g_scratch[slot];
+  if (s.bytes >= bytes && s.p) return s.p;
+  if (s.p) {
+    cudaStreamSynchronize(g_stream);
+    cudaFree(s.p);
+  }
+  s.p = nullptr;
+  s.bytes = 0;
+  size_t want = bytes < 4096 ? 4096 : bytes;
+  if (cudaMalloc(&s.p, want) != cudaSuccess) {
+    cudaGetLastError();
+    gb__set_error(2, "scratch cudaMalloc");
+    s.p = nullptr;
+    return nullptr;
+  }
+  s.bytes = want;
+  return s.p;
+}
+
+// ------------------------------------------------------------ conversions
+
+template <typename A, typename B> __global__ void k_convert(B *__restrict__ dst, const A *__restrict__ src, size_t n) {
+  for (size_t i = blockIdx.x * (size_t) blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+    dst[i] = (B) src[i];
+}
+
+static unsigned grid_for(size_t n, int threads) {
+  size_t b = (n + threads - 1) / threads;
+  if (b > 148u * 32u) b = 148u * 32u;
+  if (b < 1) b = 1;
+  return (unsigned) b;
+}
+
+extern "C" int gb_convert_f64_to_f32(void *dst, const void *src, size_t n) {
+  k_convert<double, float><<<grid_for(n, 256), 256, 0, g_stream>>>((float *) dst, (const double *) src, n);
+  GB_CHECK_LAUNCH("convert f64->f32");
+  return 0;
+}
+
+extern "C" int gb_convert_f32_to_f64(void *dst, const void *src, size_t n) {
+  k_convert<float, double><<<grid_for(n, 256), 256, 0, g_stream>>>((double *) dst, (const float *) src, n);
+  GB_CHECK_LAUNCH("convert f32->f64");
+  return 0;
+}
+
+extern "C" int gb_upload_f64_as_f32(void *dev32, const void *host64, size_t n) {
+  void *st = gb__scratch(GB_SCR_STAGE, n * sizeof(double));
+  if (!st) return gb_last_error();
+  if (gb_h2d(st, host64, n * sizeof(double))) return g_err;
+  return gb_convert_f64_to_f32(dev32, st, n);
+}
+
+extern "C" int gb_download_f32_as_f64(void *host64, const void *dev32, size_t n) {
+  void *st = gb__scratch(GB_SCR_STAGE, n * sizeof(double));
+  if (!st) return gb_last_error();
+  if (gb_convert_f32_to_f64(st, dev32, n)) return g_err;
+  return gb_d2h(host64, st, n * sizeof(double));
+}
+
+// ---------------------------------------------------------------- twiddles
+
+// exp(-2 pi i m / n) for m < n, rounded from extended precision on the host.
+const void *gb__twiddles(long n, int prec) {
+  int lg = 0;
+  while ((1L << lg) < n) lg++;
+  if ((1L << lg) != n || lg < 1 || lg > 12) {
+    gb__set_error(1002, "twiddles: unsupported length");
+    return nullptr;
+  }
+  Twiddle &t = g_tw[lg];
+  if (!t.d64) {
+    double2 *h64 = (double2 *) malloc(sizeof(double2) * (size_t) n);
+    float2 *h32 = (float2 *) malloc(sizeof(float2) * (size_t) n);
+    for (long m = 0; m < n; m++) {
+      long double a = 6.283185307179586476925286766559005768L * (long double) m / (long double) n;
+      double c = (double) cosl(a), s = -(double) sinl(a);
+      h64[m] = make_double2(c, s);
+      h32[m] = make_float2((float) c, (float) s);
+    }
+    if (cudaMalloc(&t.d64, sizeof(double2) * (size_t) n) != cudaSuccess ||
+        cudaMalloc(&t.d32, sizeof(float2) * (size_t) n) != cudaSuccess) {
+      cudaGetLastError();
+      free(h64);
+      free(h32);
+      gb__set_error(2, "twiddles cudaMalloc");
+      return nullptr;
+    }
+    cudaMemcpy(t.d64, h64, sizeof(double2) * (size_t) n, cudaMemcpyHostToDevice);
+    cudaMemcpy(t.d32, h32, sizeof(float2) * (size_t) n, cudaMemcpyHostToDevice);
+    free(h64);
+    free(h32);
+  }
+  return prec == GB_FP32 ? t.d32 : t.d64;
+}

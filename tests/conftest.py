@@ -1,0 +1,42 @@
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (runs the sm_100a kernels)")
+
+
+@pytest.fixture(scope="session")
+def b200():
+    import libgrid_b200
+
+    return libgrid_b200.load()
+
+
+@pytest.fixture(scope="session")
+def restate():
+    from oracle import pyoracle
+
+    return pyoracle.restatement()
+
+
+@pytest.fixture(scope="session")
+def ref():
+    from oracle import pyoracle
+
+    if not pyoracle.reference_available():
+        pytest.skip("reference CPU build (oracle/_ref) not present")
+    return pyoracle.reference(min(8, os.cpu_count() or 1))
+
+
+def rel(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    return float(np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300))
