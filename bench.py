@@ -1,0 +1,400 @@
+"""Benchmark: 256^3 Gross-Pitaevskii split-operator steps/s on the B200.
+
+Workload (the GP configuration): 256^3 complex grid, step 0.5 bohr, mass
+4 amu, V_ext = 8 seeded Gaussian wells, g = 0.0025, Thomas-Fermi start with
+1% seeded complex noise, dt = 1 au, 2nd-order FFT split operator with
+V_ext + g|psi|^2 built in-kernel (grid_wf_propagate_gp).  A "step" is one
+split-operator step of that wavefunction.
+
+  value     FP64 steps/s with psi and V_ext resident in HBM (whole job: all
+            ranks' replicas), timed with CUDA events on the library stream
+  e2e       the same metric through the public C API from pinned host
+            buffers: the timed region starts from host arrays (upload of psi
+            and V_ext at first use), runs K steps reading the norm back after
+            every step (the reference's propagation-loop idiom) and ends with
+            psi copied back to the host
+  fp32      the same step in the FP32 mode (FP64 phase reduction and FP64
+            reductions), with its relative L2 distance from the FP64 result
+  roofline  the dominant line-pass kernel (per the ncu launch list): its
+            algorithmic bytes per launch (32 B/pt: one read + one write of
+            complex128) over its mean CUDA-event duration in the timed region
+  step_roofline  264 B/pt per step (4 transforms x 2 passes x 32 B + 8 B
+            real V_ext) over the step time
+
+The grid (268 MB psi + 135 MB V_ext) exceeds the 126 MB L2, so no L2 flush
+is needed between steps.  Multi-GPU: independent replicas, one per GPU (the
+path does not shard); no data-path collective.
+
+`--impl reference` times the reference's own CPU implementation of the same
+step (oracle/_ref, all host threads) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "GP 256^3 split-operator steps/s (FP64, resident in HBM)"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+BYTES_PER_POINT_STEP = 264
+BYTES_PER_POINT_PASS = 32
+# pass kinds reported by gb_pass_timing_report: 5 * axis + program
+KIND_NAMES = {}
+for _ax, _an in enumerate("xyz"):
+    for _p, _pn in enumerate(["fwd", "inv", "fwd_kin_inv", "inv_pot_fwd", "other"]):
+        KIND_NAMES[5 * _ax + _p] = "%s_%s" % (_an, _pn)
+
+
+def hbm_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    Q = (
+        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+        "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
+    )
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE,
+                stderr=subprocess.DEVNULL,
+                text=True,
+            )
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.p:
+            self.p.terminate()
+            try:
+                self.out, _ = self.p.communicate(timeout=5)
+            except Exception:
+                self.p.kill()
+        return False
+
+    def summary(self):
+        sms, maxs, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sms.append(float(f[1]))
+                maxs.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sms:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {
+            "sm_mhz": float(np.median(sms)),
+            "sm_max_mhz": float(max(maxs)),
+            "reasons": sorted(reasons),
+            "samples": len(sms),
+        }
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def allmax(world, x):
+    if world <= 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(x)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(size: int, steps: int, warmup: int, threads: int | None = None):
+    env = dict(os.environ)
+    env.setdefault("OMP_PROC_BIND", "TRUE")
+    env.setdefault("OMP_WAIT_POLICY", "ACTIVE")
+    cmd = [sys.executable, "-m", "oracle.refbench", "--size", str(size), "--steps", str(steps), "--warmup", str(warmup)]
+    if threads:
+        cmd += ["--threads", str(threads)]
+    p = subprocess.run(cmd, cwd=ROOT, env=env, capture_output=True, text=True, timeout=1800)
+    for line in p.stdout.splitlines()[::-1]:
+        line = line.strip()
+        if line.startswith("{"):
+            return json.loads(line)
+    raise RuntimeError("cpu baseline failed: %s" % p.stderr[-2000:])
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return 0
+    nproc = len(os.sched_getaffinity(0))
+    r = cpu_baseline(args.size, args.steps, args.warmup)
+    line = {
+        "impl": "reference",
+        "metric": METRIC.replace("(FP64, resident in HBM)", "(FP64)"),
+        "value": r["steps_per_s"],
+        "unit": "steps/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 / r["steps_per_s"],
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded Gaussian wells + Thomas-Fermi start)",
+        "config": {"workload": "gp_split_step_256", "grid": [args.size] * 3, "dt": 1.0, "g": 0.0025,
+                   "propagator": "2nd-order FFT split operator", "host_threads": nproc},
+        "cpu_baseline": {"value": r["steps_per_s"], "unit": "steps/s", "cores": r["cores"], "kind": r["kind"],
+                         "sample": r["sample"] + "; libgrid CPU path with the project's FFTW stand-in"},
+        "e2e": {"value": r["steps_per_s"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_b200(args, world, rank, local):
+    import libgrid_b200 as gb
+    from libgrid_b200 import capi, workloads
+
+    api = gb.load()
+    dev = (C_int_array(local))
+    api.lib.cuda_enable(b"\x01", 1, dev)
+    lib = api.lib
+    n = args.size
+    shape, step, g, dt = (n, n, n), 0.5, 0.0025, 1.0
+    mass = 4.0 / capi.GRID_AUTOAMU
+    psi0, v = workloads.gp_wells(shape, step, g, seed=2)
+    N = n**3
+
+    def make():
+        w = api.wf(*shape, step, mass, capi.WF_PERIODIC_BOUNDARY, capi.WF_2ND_ORDER_FFT, values=psi0)
+        vx = api.rgrid(*shape, step, values=v)
+        return w, vx
+
+    # ---------------------------------------------- FP64, resident in HBM
+    w, vx = make()
+    for _ in range(args.warmup):
+        w.propagate_gp(vx, g, dt)
+    lib.gb_synchronize()
+    lib.gb_pass_timing(1)
+    barrier(world)
+    lib.gb_synchronize()
+    l0 = lib.gb_launch_count()
+    with ClockSampler(local) as clk:
+        lib.gb_event_record(0)
+        for _ in range(args.steps):
+            w.propagate_gp(vx, g, dt)
+        lib.gb_event_record(1)
+        lib.gb_synchronize()
+    launches = lib.gb_launch_count() - l0
+    ms = lib.gb_event_elapsed_ms(0, 1)
+    barrier(world)
+    ms_max = allmax(world, ms)
+    kinds = 15
+    import ctypes as C
+
+    kms = (C.c_double * kinds)()
+    kcnt = (C.c_long * kinds)()
+    lib.gb_pass_timing_report.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_long), C.c_int]
+    lib.gb_pass_timing_report(kms, kcnt, kinds)
+    lib.gb_pass_timing(0)
+    per_kind = {KIND_NAMES[k]: {"ms_total": kms[k], "launches": kcnt[k]} for k in range(kinds) if kcnt[k]}
+    psi64 = w.grid.get()
+    api.free(w)
+    api.free(vx)
+
+    # ------------------------------------------------------------- FP32
+    w, vx = make()
+    w.precision(capi.GRID_PREC_FP32)
+    for _ in range(args.warmup):
+        w.propagate_gp(vx, g, dt)
+    lib.gb_synchronize()
+    barrier(world)
+    lib.gb_event_record(2)
+    for _ in range(args.steps):
+        w.propagate_gp(vx, g, dt)
+    lib.gb_event_record(3)
+    lib.gb_synchronize()
+    ms32 = allmax(world, lib.gb_event_elapsed_ms(2, 3))
+    psi32 = w.grid.get()
+    err32 = float(np.linalg.norm(psi32 - psi64) / np.linalg.norm(psi64))
+    api.free(w)
+    api.free(vx)
+
+    # ------------------------------------------------ e2e through the C API
+    # fresh grids whose data is only on the host: the first propagate call
+    # uploads psi and V_ext inside the timed region
+    w, vx = make()
+    barrier(world)
+    lib.gb_synchronize()
+    t0 = time.perf_counter()
+    for s in range(args.steps):
+        w.propagate_gp(vx, g, dt)
+        w.norm()  # D2H of the step's result (8 B)
+    api.sync_host(w.grid)  # final psi back to the host
+    e2e_s = allmax(world, time.perf_counter() - t0)
+    api.free(w)
+    api.free(vx)
+
+    # ------------------------------------------------------------ report
+    if rank != 0:
+        return 0
+    peak, peak_kind = hbm_peak()
+    step_ms = ms_max / args.steps
+    value = world * args.steps / (ms_max * 1e-3)
+    # dominant kernel = largest total time among pass kinds
+    dom = max(per_kind.items(), key=lambda kv: kv[1]["ms_total"])
+    dom_ms = dom[1]["ms_total"] / dom[1]["launches"]
+    dom_bytes = BYTES_PER_POINT_PASS * N
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    step_gbs = BYTES_PER_POINT_STEP * N / (step_ms * 1e-3) / 1e9
+    h2d = (N * 16 + n * n * 2 * (n // 2 + 1) * 8) / args.steps
+    d2h = 8 + N * 16 / args.steps
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": step_ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded Gaussian wells + Thomas-Fermi start)",
+        "config": {
+            "workload": "gp_split_step_256",
+            "grid": [n, n, n],
+            "step_bohr": step,
+            "mass_amu": 4.0,
+            "g": g,
+            "dt": dt,
+            "propagator": "2nd-order FFT split operator, V_ext + g|psi|^2 in-kernel",
+            "l2": "inputs (403 MB) larger than L2 (126 MB); no flush",
+            "parallelism": "replicas x%d" % world,
+        },
+        "fp32": {
+            "value": world * args.steps / (ms32 * 1e-3),
+            "unit": "steps/s",
+            "ms_per_step": ms32 / args.steps,
+            "speedup_vs_fp64": ms_max / ms32,
+            "rel_l2_vs_fp64_after_steps": err32,
+            "steps_compared": args.warmup + args.steps,
+        },
+        "roofline": {
+            "bound": "hbm",
+            "kernel": dom[0],
+            "achieved": achieved,
+            "peak": peak,
+            "unit": "GB/s",
+            "frac": achieved / peak,
+            "peak_source": peak_kind,
+            "traffic": None,
+            "algorithmic_bytes_per_launch": dom_bytes,
+            "mean_launch_ms": dom_ms,
+        },
+        "step_roofline": {"bytes_per_point": BYTES_PER_POINT_STEP, "achieved": step_gbs, "frac": step_gbs / peak},
+        "passes": per_kind,
+        "gpu_launches": int(launches),
+        "e2e": {
+            "value": world * args.steps / e2e_s,
+            "unit": "steps/s",
+            "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h),
+            "note": "psi and V_ext uploaded once from pinned host memory, norm read back every step, psi read back at the end; bytes amortised over the timed steps",
+        },
+        "clocks": clk.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            r = cpu_baseline(n, args.cpu_steps, 1)
+            line["cpu_baseline"] = {
+                "value": r["steps_per_s"],
+                "unit": "steps/s",
+                "cores": r["cores"],
+                "kind": r["kind"],
+                "sample": r["sample"] + "; libgrid CPU path with the project's FFTW stand-in",
+            }
+        except Exception as e:  # the GPU number stands without it
+            line["cpu_baseline"] = {"value": None, "error": str(e)[-300:]}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def C_int_array(v):
+    import ctypes as C
+
+    return (C.c_int * 1)(v)
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=256)
+    ap.add_argument("--cpu-steps", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    world, rank, local = dist_setup()
+    try:
+        if args.impl == "reference":
+            return run_reference(args, world, rank)
+        return run_b200(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -90,6 +90,15 @@ int gb_memset(void *dst, int value, size_t bytes);
 int gb_event_record(int slot);
 float gb_event_elapsed_ms(int start_slot, int stop_slot);
 
+/* Per-pass timing of the FFT line passes with CUDA events on the library
+ * stream (benchmark instrumentation).  Kinds are 5 * axis + program with
+ * axis 0 x, 1 y, 2 z and program 0 forward FFT, 1 inverse FFT,
+ * 2 forward + kinetic + inverse, 3 inverse + potential + forward, 4 other.
+ * report() fills ms[k] / count[k] for k < nkinds and returns the number of
+ * timed passes. */
+int gb_pass_timing(int on);
+int gb_pass_timing_report(double *ms, long *count, int nkinds);
+
 /* Precision conversion between FP64 and FP32 copies (n scalars). */
 int gb_convert_f64_to_f32(void *dst, const void *src, size_t n);
 int gb_convert_f32_to_f64(void *dst, const void *src, size_t n);

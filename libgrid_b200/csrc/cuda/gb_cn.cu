@@ -157,19 +157,40 @@ __device__ __forceinline__ double2 cn_rhs(long i, long n, int bc, double2 cp, do
   return cs(cs(cs(cm(cp, p0), ca(cs(pm, two_p0), pfirst)), cm(c2, dif)), cm(c3y, dif));
 }
 
-// Shared-memory element (l, i) of a tile.
-template <bool CONTIG> __device__ __forceinline__ double2 &tile_at(double2 *sm, int l, long i, long n, int lpc) {
-  if constexpr (CONTIG) return sm[(long) l * (n + 1) + i];
-  else return sm[i * lpc + l];
+// Segments per line in the fast kernel (= warps per CTA).
+constexpr int kSeg = 8;
+
+// Contiguous tile rows are padded to an odd number of 16-byte elements so a
+// warp's lane-per-line accesses fall in distinct shared-memory banks.
+__host__ __device__ inline long contig_row(long n) { return (n & 1) ? n : n + 1; }
+
+// Shared-memory element (l, i) of a tile; row = padded line length
+// (contiguous) or lines per tile (strided).
+template <bool CONTIG> __device__ __forceinline__ double2 &tile_at(double2 *sm, int l, long i, long row) {
+  if constexpr (CONTIG) return sm[(long) l * row + i];
+  else return sm[i * row + l];
 }
 
-template <bool CONTIG> __global__ void __launch_bounds__(32) k_cn_fast(double2 *__restrict__ psi, CnAxis a) {
+// Fast path.  A CTA of 8 warps owns up to 32 lines (lane = line); warp s
+// owns segment s = [s S, (s+1) S) of every line, S = ceil(n / 8).  Both
+// Thomas recurrences are linear with line-independent coefficients:
+//   forward  v_i = b_i - m_i v_{i-1}
+//   backward x_i = rb_i v_i + Q_i x_{i+1},   Q_i = -rb_i c_i
+// so each warp runs the particular recurrence of its segment from a zero
+// carry-in, one warp chains the 8 segment carries per line, and every
+// element then adds (carry-in) x (homogeneous response), whose tables
+// H_i = prod(-m_j) and G_i = prod(Q_j) over the segment are precomputed.
+template <bool CONTIG> __global__ void __launch_bounds__(32 * kSeg) k_cn_fast(double2 *__restrict__ psi, CnAxis a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ __align__(8) uint64_t bar;
+  __shared__ double2 s_end[kSeg][32];
+  __shared__ double2 s_in[kSeg][32];
+  __shared__ double2 s_fact[32];
   double2 *sm = (double2 *) smraw;
-  const int lane = threadIdx.x;
+  const int tid = threadIdx.x, lane = tid & 31, seg = tid >> 5;
   const long n = a.n;
   const int lpc = a.lpc;
+  const long row = CONTIG ? contig_row(n) : (long) lpc;
   long line0 = 0, o = 0, col0 = 0;
   int nl;
   if constexpr (CONTIG) {
@@ -181,29 +202,30 @@ template <bool CONTIG> __global__ void __launch_bounds__(32) k_cn_fast(double2 *
     col0 = (long) blockIdx.x * lpc;
     nl = lpc;
   }
+  const double2 zero = make_double2(0.0, 0.0);
 
-  if (lane == 0) {
+  // ---- tile load (bulk copies, one mbarrier, bounded wait)
+  if (tid == 0) {
     mbar_init(&bar, 1);
     fence_mbar_init();
+    mbar_arrive_expect_tx(&bar, (unsigned) (nl * n * 16));
   }
-  __syncwarp();
-  if (lane == 0) mbar_arrive_expect_tx(&bar, (unsigned) (nl * n * 16));
-  __syncwarp();
+  __syncthreads();
   if constexpr (CONTIG) {
-    for (int l = lane; l < nl; l += 32) bulk_g2s(sm + (long) l * (n + 1), psi + (line0 + l) * n, (unsigned) (n * 16), &bar);
+    for (int l = tid; l < nl; l += 32 * kSeg) bulk_g2s(sm + (long) l * row, psi + (line0 + l) * n, (unsigned) (n * 16), &bar);
   } else {
-    for (long i = lane; i < n; i += 32)
-      bulk_g2s(sm + i * lpc, psi + o * n * a.inner + i * a.inner + col0, (unsigned) (nl * 16), &bar);
+    for (long i = tid; i < n; i += 32 * kSeg)
+      bulk_g2s(sm + i * row, psi + o * n * a.inner + i * a.inner + col0, (unsigned) (nl * 16), &bar);
   }
   if (!mbar_wait_bounded(&bar, 0)) {
-    if (lane == 0) atomicExch(a.err, 1);
+    if (tid == 0) atomicExch(a.err, 1);
     mbar_wait_bounded(&bar, 0);
     return;
   }
 
-  // Optional first potential half-step, applied in place.
+  // ---- optional first potential half-step (all threads, element-parallel)
   if (a.pre.kind != GB_POT_NONE || a.pre.g != 0.0) {
-    for (long e = lane; e < (long) nl * n; e += 32) {
+    for (long e = tid; e < (long) nl * n; e += 32 * kSeg) {
       long l, i;
       if constexpr (CONTIG) {
         l = e / n;
@@ -214,74 +236,109 @@ template <bool CONTIG> __global__ void __launch_bounds__(32) k_cn_fast(double2 *
       }
       long ix, iy, iz;
       cn_decode(a, CONTIG ? line0 + l : o, i, col0 + l, ix, iy, iz);
-      double2 &r = tile_at<CONTIG>(sm, (int) l, i, n, lpc);
+      double2 &r = tile_at<CONTIG>(sm, (int) l, i, row);
       r = cn_pot(r, ix, iy, iz, a, a.pre);
     }
-    __syncwarp();
   }
+  __syncthreads();
 
+  const double2 *tm = a.tab, *trb = a.tab + n, *tz = a.tab + 2 * n, *tH = a.tab + 3 * n, *tQ = a.tab + 4 * n,
+                *tG = a.tab + 5 * n;
+  const long S = (n + kSeg - 1) / kSeg;
+  const long a0 = seg * S, e0 = (a0 + S < n) ? a0 + S : n;
+  const bool active = (lane < nl) && (a0 < e0);
+  const int bc = a.boundary;
+
+  // ---- neighbours of the segment, read before anything is overwritten
+  double2 pfirst = zero, plast = zero, p_before = zero, p_after = zero;
   if (lane < nl) {
-    const double2 *tm = a.tab, *trb = a.tab + n, *tz = a.tab + 2 * n;
-    const double2 zero = make_double2(0.0, 0.0);
-    const double2 c3y = zero;  // fast path: no rotation
-    const double2 pfirst = tile_at<CONTIG>(sm, lane, 0, n, lpc);
-    const double2 plast = tile_at<CONTIG>(sm, lane, n - 1, n, lpc);
-    double2 pm = plast, p0 = pfirst, vprev = zero;
-    // right-hand side and forward elimination
-    for (long i = 0; i < n; i++) {
-      const double2 pp = (i + 1 < n) ? tile_at<CONTIG>(sm, lane, i + 1, n, lpc) : pfirst;
-      const double2 b = cn_rhs(i, n, a.boundary, a.cp, a.c2, c3y, pm, p0, pp, pfirst, plast);
-      const double2 v = (i == 0) ? b : cs(b, cm(tm[i], vprev));
-      tile_at<CONTIG>(sm, lane, i, n, lpc) = v;
-      vprev = v;
+    pfirst = tile_at<CONTIG>(sm, lane, 0, row);
+    plast = tile_at<CONTIG>(sm, lane, n - 1, row);
+  }
+  if (active) {
+    p_before = (a0 > 0) ? tile_at<CONTIG>(sm, lane, a0 - 1, row) : plast;
+    p_after = (e0 < n) ? tile_at<CONTIG>(sm, lane, e0, row) : pfirst;
+  }
+  __syncthreads();
+
+  // ---- right-hand side + forward particular recurrence (zero carry-in)
+  double2 u = zero;
+  if (active) {
+    double2 pm = p_before, p0 = tile_at<CONTIG>(sm, lane, a0, row);
+    for (long i = a0; i < e0; i++) {
+      const double2 pp = (i + 1 < e0) ? tile_at<CONTIG>(sm, lane, i + 1, row) : p_after;
+      const double2 b = cn_rhs(i, n, bc, a.cp, a.c2, zero, pm, p0, pp, pfirst, plast);
+      u = (i == a0) ? b : cs(b, cm(tm[i], u));
+      tile_at<CONTIG>(sm, lane, i, row) = u;
       pm = p0;
       p0 = pp;
     }
-    // back substitution
-    const double2 cc = make_double2(1.0 + a.c2.x, a.c2.y);
-    double2 x = cm(vprev, trb[n - 1]);
-    tile_at<CONTIG>(sm, lane, n - 1, n, lpc) = x;
-    const double2 xlast = x;
-    for (long i = n - 2; i >= 0; i--) {
-      const double2 ci = (i == 0 && a.boundary != 3) ? make_double2(2.0, 0.0) : cc;
-      x = cm(cs(tile_at<CONTIG>(sm, lane, i, n, lpc), cm(ci, x)), trb[i]);
-      tile_at<CONTIG>(sm, lane, i, n, lpc) = x;
-    }
-    if (a.boundary == 3) {
-      // Sherman-Morrison correction: x -= fact z
-      const double2 num = ca(x, cm(a.beta, cm(xlast, a.gamma)));  // gamma holds 1/gamma here
-      const double2 fact = cm(num, a.den);                           // den holds 1/den here
-      for (long i = 0; i < n; i++) {
-        double2 &r = tile_at<CONTIG>(sm, lane, i, n, lpc);
-        r = cs(r, cm(fact, tz[i]));
-      }
+  }
+  if (lane < nl) s_end[seg][lane] = u;
+  __syncthreads();
+  if (seg == 0 && lane < nl) {
+    double2 vin = zero;
+    for (int s = 0; s < kSeg; s++) {
+      const long as = s * S, es = (as + S < n) ? as + S : n;
+      s_in[s][lane] = vin;
+      if (as < es) vin = ca(s_end[s][lane], cm(tH[es - 1], vin));
     }
   }
-  __syncwarp();
+  __syncthreads();
 
-  if (a.post.kind != GB_POT_NONE || a.post.g != 0.0) {
-    for (long e = lane; e < (long) nl * n; e += 32) {
-      long l, i;
-      if constexpr (CONTIG) {
-        l = e / n;
-        i = e - l * n;
-      } else {
-        i = e / nl;
-        l = e - i * nl;
+  // ---- forward fix-up fused with the backward particular recurrence
+  double2 y = zero;
+  if (active) {
+    const double2 vin = s_in[seg][lane];
+    for (long i = e0 - 1; i >= a0; i--) {
+      const double2 v = ca(tile_at<CONTIG>(sm, lane, i, row), cm(tH[i], vin));
+      y = (i == e0 - 1) ? cm(trb[i], v) : ca(cm(trb[i], v), cm(tQ[i], y));
+      tile_at<CONTIG>(sm, lane, i, row) = y;
+    }
+  }
+  if (lane < nl) s_end[seg][lane] = y;
+  __syncthreads();
+  if (seg == 0 && lane < nl) {
+    double2 xin = zero;
+    for (int s = kSeg - 1; s >= 0; s--) {
+      const long as = s * S, es = (as + S < n) ? as + S : n;
+      s_in[s][lane] = xin;
+      if (as < es) xin = ca(s_end[s][lane], cm(tG[as], xin));
+    }
+    if (bc == 3) {
+      // Sherman-Morrison: fact = (x_0 + beta x_{n-1} / gamma) / den; the
+      // segment holding n-1 has a zero carry-in, so x_{n-1} = y_{n-1}.
+      const double2 xl = tile_at<CONTIG>(sm, lane, n - 1, row);
+      s_fact[lane] = cm(ca(xin, cm(a.beta, cm(xl, a.gamma))), a.den);  // gamma, den hold reciprocals
+    }
+  }
+  __syncthreads();
+
+  // ---- backward fix-up, periodic correction, second potential half-step
+  const bool post = (a.post.kind != GB_POT_NONE || a.post.g != 0.0);
+  if (active) {
+    const double2 xin = s_in[seg][lane];
+    const double2 fact = (bc == 3) ? s_fact[lane] : zero;
+    for (long i = a0; i < e0; i++) {
+      double2 x = ca(tile_at<CONTIG>(sm, lane, i, row), cm(tG[i], xin));
+      if (bc == 3) x = cs(x, cm(fact, tz[i]));
+      if (post) {
+        long ix, iy, iz;
+        cn_decode(a, CONTIG ? line0 + lane : o, i, col0 + lane, ix, iy, iz);
+        x = cn_pot(x, ix, iy, iz, a, a.post);
       }
-      long ix, iy, iz;
-      cn_decode(a, CONTIG ? line0 + l : o, i, col0 + l, ix, iy, iz);
-      double2 &r = tile_at<CONTIG>(sm, (int) l, i, n, lpc);
-      r = cn_pot(r, ix, iy, iz, a, a.post);
+      tile_at<CONTIG>(sm, lane, i, row) = x;
     }
   }
 
+  // ---- tile store
   fence_proxy_async_smem();
-  __syncwarp();
+  __syncthreads();
   if constexpr (CONTIG) {
-    for (int l = lane; l < nl; l += 32) bulk_s2g(psi + (line0 + l) * n, sm + (long) l * (n + 1), (unsigned) (n * 16));
+    for (int l = tid; l < nl; l += 32 * kSeg) bulk_s2g(psi + (line0 + l) * n, sm + (long) l * row, (unsigned) (n * 16));
   } else {
-    for (long i = lane; i < n; i += 32) bulk_s2g(psi + o * n * a.inner + i * a.inner + col0, sm + i * lpc, (unsigned) (nl * 16));
+    for (long i = tid; i < n; i += 32 * kSeg)
+      bulk_s2g(psi + o * n * a.inner + i * a.inner + col0, sm + i * row, (unsigned) (nl * 16));
   }
   bulk_commit();
   bulk_wait_all();
@@ -403,16 +460,18 @@ __global__ void k_cn_general(double2 *__restrict__ psi, CnAxis a) {
   }
 }
 
-// Host-side uniform tables (m, 1/b', z) for one axis and the periodic scalars.
+// Host-side uniform tables for one axis: m, 1/b', z (periodic), and the
+// segment responses H (forward) and G (backward) with Q_i = -c_i / b'_i,
+// plus the periodic scalars.
 struct FastTables {
-  std::vector<double2> tab;  // 3 n
+  std::vector<double2> tab;  // 6 n: m, rb, z, H, Q, G
   double2 beta, inv_gamma, inv_den;
 };
 
 static void build_fast_tables(long n, int bc, cd cp, cd c2, FastTables &t) {
-  t.tab.assign(3 * n, make_double2(0.0, 0.0));
+  t.tab.assign(6 * n, make_double2(0.0, 0.0));
   const cd d = cp - 2.0;
-  std::vector<cd> bmod(n, d), m(n, 0.0), rb(n);
+  std::vector<cd> bmod(n, d), m(n, 0.0), rb(n), q(n), H(n), G(n);
   cd alpha = 1.0 + c2, beta = 1.0 - c2, gamma = -d;
   if (bc == 3) {
     bmod[0] = d - gamma;
@@ -433,23 +492,36 @@ static void build_fast_tables(long n, int bc, cd cp, cd c2, FastTables &t) {
     bp = bmod[i] - m[i] * sup;
     rb[i] = 1.0 / bp;
   }
+  for (long i = 0; i < n; i++) {
+    const cd ci = (i == 0 && bc != 3) ? cd(2.0) : 1.0 + c2;
+    q[i] = -rb[i] * ci;
+  }
+  const long S = (n + kSeg - 1) / kSeg;
+  for (long s = 0; s < kSeg; s++) {
+    const long as = s * S, es = (as + S < n) ? as + S : n;
+    for (long i = as; i < es; i++) H[i] = (i == as) ? -m[i] : H[i - 1] * (-m[i]);
+    for (long i = es - 1; i >= as; i--) G[i] = (i == es - 1) ? q[i] : q[i] * G[i + 1];
+  }
   std::vector<cd> z(n, 0.0);
   cd den = 1.0;
   if (bc == 3) {
     std::vector<cd> v(n, 0.0);
     v[0] = gamma;
     v[n - 1] += alpha;
-    if (n == 1) v[0] = gamma + alpha;
     for (long i = 1; i < n; i++) v[i] -= m[i] * v[i - 1];
     z[n - 1] = v[n - 1] * rb[n - 1];
     for (long i = n - 2; i >= 0; i--) z[i] = (v[i] - (1.0 + c2) * z[i + 1]) * rb[i];
     den = 1.0 + z[0] + beta * z[n - 1] / gamma;
   }
-  for (long i = 0; i < n; i++) {
-    t.tab[i] = make_double2(m[i].real(), m[i].imag());
-    t.tab[n + i] = make_double2(rb[i].real(), rb[i].imag());
-    t.tab[2 * n + i] = make_double2(z[i].real(), z[i].imag());
-  }
+  auto put = [&](long base, const std::vector<cd> &x) {
+    for (long i = 0; i < n; i++) t.tab[base + i] = make_double2(x[i].real(), x[i].imag());
+  };
+  put(0, m);
+  put(n, rb);
+  put(2 * n, z);
+  put(3 * n, H);
+  put(4 * n, q);
+  put(5 * n, G);
   const cd ig = 1.0 / gamma, id = 1.0 / den;
   t.beta = make_double2(beta.real(), beta.imag());
   t.inv_gamma = make_double2(ig.real(), ig.imag());
@@ -482,17 +554,17 @@ static double2 *fast_tables(int slot, long n, int bc, cd cp, cd c2, cudaStream_t
     gb__set_error(1013, "cn: line length above 4096");
     return nullptr;
   }
-  double2 *base = (double2 *) gb__scratch(GB_SCR_CN, sizeof(double2) * (size_t) (3 * nmax) * 3);
+  double2 *base = (double2 *) gb__scratch(GB_SCR_CN, sizeof(double2) * (size_t) (6 * nmax) * 3);
   if (!base) return nullptr;
   if (base != g_cn_tab_base) {
     for (int i = 0; i < 3; i++) g_cn_cache[i].valid = false;
     g_cn_tab_base = base;
   }
-  double2 *tab = base + (size_t) (3 * nmax) * slot;
+  double2 *tab = base + (size_t) (6 * nmax) * slot;
   CnCacheEntry &e = g_cn_cache[slot];
   if (!(e.valid && e.n == n && e.bc == bc && e.cp == cp && e.c2 == c2)) {
     build_fast_tables(n, bc, cp, c2, e.ft);
-    if (cudaMemcpyAsync(tab, e.ft.tab.data(), sizeof(double2) * (size_t) (3 * n), cudaMemcpyHostToDevice, st) !=
+    if (cudaMemcpyAsync(tab, e.ft.tab.data(), sizeof(double2) * (size_t) (6 * n), cudaMemcpyHostToDevice, st) !=
             cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {
       gb__set_error(3, "cn tables h2d");
@@ -595,16 +667,18 @@ extern "C" int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, co
       if (!tab) return gb_last_error();
       a.tab = tab;
       a.cp = make_double2(cp.real(), cp.imag());
-      const size_t budget = 110 * 1024;
+      // tile budget: two CTAs (tile + ~8.7 KB static) per SM
+      const size_t budget = 100 * 1024;
       if (contig) {
-        long lpc = (long) (budget / ((a.n + 1) * 16));
+        const long row = contig_row(a.n);
+        long lpc = (long) (budget / (row * 16));
         if (lpc > 32) lpc = 32;
         if (lpc < 1) return gb__set_error(1011, "cn: line too long for a shared-memory tile");
         a.lpc = (int) lpc;
-        const size_t sm = (size_t) lpc * (a.n + 1) * 16;
+        const size_t sm = (size_t) lpc * row * 16;
         cudaFuncSetAttribute(k_cn_fast<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
         const long nb = (a.outer + lpc - 1) / lpc;
-        k_cn_fast<true><<<(unsigned) nb, 32, sm, st>>>((double2 *) psi, a);
+        k_cn_fast<true><<<(unsigned) nb, 32 * kSeg, sm, st>>>((double2 *) psi, a);
       } else {
         long cap = (long) (budget / (a.n * 16));
         if (cap > 32) cap = 32;
@@ -615,7 +689,7 @@ extern "C" int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, co
         cudaFuncSetAttribute(k_cn_fast<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
         if (a.outer > 65535) return gb__set_error(1012, "cn: outer extent above 65535");
         dim3 grid((unsigned) (a.inner / lpc), (unsigned) a.outer);
-        k_cn_fast<false><<<grid, 32, sm, st>>>((double2 *) psi, a);
+        k_cn_fast<false><<<grid, 32 * kSeg, sm, st>>>((double2 *) psi, a);
       }
       GB_CHECK_LAUNCH("cn fast");
     } else {

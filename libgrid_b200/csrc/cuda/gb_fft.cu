@@ -147,7 +147,8 @@ template <typename T> __global__ void k_potential_multiply(C2<T> *psi, PassArgs 
   const long n = a.nx * a.ny * a.nz;
   for (long g = blockIdx.x * (long) blockDim.x + threadIdx.x; g < n; g += (long) gridDim.x * blockDim.x) {
     const long k = g % a.nz, ij = g / a.nz, j = ij % a.ny, i = ij / a.ny;
-    psi[g] = gbfft::pot_factor_apply<T>(psi[g], i, j, k, a);
+    const long vidx = (i * a.ny + j) * a.pot.vrow + k;
+    psi[g] = gbfft::pot_factor_apply<T>(psi[g], i, j, k, (unsigned) vidx, a);
   }
 }
 
@@ -192,17 +193,32 @@ static unsigned pw_blocks(long n) {
 
 // ---------------------------------------------------------------- C ABI
 
+// The line-pass FFT takes power-of-two lengths up to 4096 on every axis of
+// length > 1 and grids below 2^31 points (32-bit in-tile offsets).
+static int fft_geom_ok(const gb_geom *g) {
+  const long n[3] = {g->nx, g->ny, g->nz};
+  for (int d = 0; d < 3; d++)
+    if (n[d] < 1 || (n[d] > 1 && ((n[d] & (n[d] - 1)) != 0 || n[d] > 4096)))
+      return gb__set_error(1002, "FFT line length must be a power of two in [2, 4096]");
+  if ((double) g->nx * (double) g->ny * (double) g->nz >= 2147483648.0)
+    return gb__set_error(1006, "FFT grid must have fewer than 2^31 points");
+  return 0;
+}
+
 extern "C" int gb_fft3d(void *data, const gb_geom *g, int sign, double scale) {
+  if (fft_geom_ok(g)) return gb_last_error();
   if (g->prec == GB_FP32) return gb__fft3d_t<float>(data, g, sign, scale);
   return gb__fft3d_t<double>(data, g, sign, scale);
 }
 
 extern "C" int gb_split_step(void *psi, const gb_geom *g, const gb_kinetic *kin, const gb_potential *pot) {
+  if (fft_geom_ok(g)) return gb_last_error();
   if (g->prec == GB_FP32) return gb__split_step_t<float>(psi, g, kin, pot);
   return gb__split_step_t<double>(psi, g, kin, pot);
 }
 
 extern "C" int gb_fft_ksq_sum(const void *psi, void *work, const gb_geom *g, double *out) {
+  if (fft_geom_ok(g)) return gb_last_error();
   if (g->prec == GB_FP32) return gb__ksq_sum_t<float>(psi, work, g, out);
   return gb__ksq_sum_t<double>(psi, work, g, out);
 }
@@ -232,6 +248,8 @@ extern "C" int gb_kinetic_multiply(void *psi, const gb_geom *g, const gb_kinetic
 }
 
 extern "C" int gb_potential_multiply(void *psi, const gb_geom *g, const gb_potential *pot) {
+  if ((double) g->nx * (double) g->ny * (double) (pot->vrow > g->nz ? pot->vrow : g->nz) >= 4294967296.0)
+    return gb__set_error(1006, "potential grid must have fewer than 2^32 elements");
   PassArgs a;
   memset(&a, 0, sizeof(a));
   a.nx = g->nx;

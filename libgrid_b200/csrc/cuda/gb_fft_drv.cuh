@@ -35,13 +35,28 @@ inline PassArgs base_args(const gb_geom *g) {
   return a;
 }
 
+// Program id for pass timing: 0 {FWD}, 1 {INV}, 2 {FWD,KIN,INV},
+// 3 {INV,POT,FWD}, 4 anything else; kind = 5 * axis + id.
+template <int... Ops> constexpr int prog_id(OpL<Ops...>) {
+  constexpr int n = sizeof...(Ops);
+  constexpr int o[] = {Ops...};
+  if (n == 1 && o[0] == OP_FWD) return 0;
+  if (n == 1 && o[0] == OP_INV) return 1;
+  if (n == 3 && o[0] == OP_FWD && o[1] == OP_KIN && o[2] == OP_INV) return 2;
+  if (n == 3 && o[0] == OP_INV && o[1] == OP_POT && o[2] == OP_FWD) return 3;
+  return 4;
+}
+
 template <typename T, int... Ops>
 int pass(const gb_geom *g, int axis, const void *src, void *dst, PassArgs a, OpL<Ops...> ops) {
   const View v = axis_view(g, axis);
   a.axis = axis;
   a.tw = gb__twiddles(v.n, g->prec);
   if (!a.tw) return gb_last_error();
-  return launch_pass<T>(v.n, src, dst, a, v.outer, v.inner, ops);
+  const int slot = gb__pass_begin(5 * axis + prog_id(ops));
+  const int rc = launch_pass<T>(v.n, src, dst, a, v.outer, v.inner, ops);
+  gb__pass_end(slot);
+  return rc;
 }
 
 #define GB_TRY(x)               \

@@ -77,28 +77,44 @@ template <int S, typename T2> struct DFT<8, S, T2> {
     }
   }
 };
+// Radix-4 butterfly on four elements of v given by index (in place).
+template <int S, typename T2> __device__ __forceinline__ void bfly4(T2 &x0, T2 &x1, T2 &x2, T2 &x3) {
+  const T2 a0 = cadd(x0, x2), a1 = csub(x0, x2);
+  const T2 a2 = cadd(x1, x3), a3 = mul_si<S>(csub(x1, x3));
+  x0 = cadd(a0, a2);
+  x2 = csub(a0, a2);
+  x1 = cadd(a1, a3);
+  x3 = csub(a1, a3);
+}
+
+// 16-point DFT as 4 x 4: with input index 4a + b and output index k1 + 4 k2,
+//   X[k1 + 4 k2] = sum_b W16^{b k1} W4^{b k2} sum_a x[4a + b] W4^{a k1}.
+// Both butterfly layers work in place; the final index transpose is a
+// compile-time renaming of registers.
 template <int S, typename T2> struct DFT<16, S, T2> {
   static __device__ __forceinline__ void run(T2 *v) {
-    T2 e[8], o[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      e[k] = v[2 * k];
-      o[k] = v[2 * k + 1];
-    }
-    DFT<8, S, T2>::run(e);
-    DFT<8, S, T2>::run(o);
-    o[1] = wmul<S>(o[1], kC1, kS1);
-    o[2] = wmul<S>(o[2], kSQH, kSQH);
-    o[3] = wmul<S>(o[3], kS1, kC1);
-    o[4] = mul_si<S>(o[4]);
-    o[5] = wmul<S>(o[5], -kS1, kC1);
-    o[6] = wmul<S>(o[6], -kSQH, kSQH);
-    o[7] = wmul<S>(o[7], -kC1, kS1);
+    for (int b = 0; b < 4; b++) bfly4<S>(v[b], v[b + 4], v[b + 8], v[b + 12]);
+    // v[b + 4 k1] now holds Y[b][k1]; twiddle by W16^{b k1}
+    v[1 + 4] = wmul<S>(v[1 + 4], kC1, kS1);    // b=1,k1=1: W^1
+    v[1 + 8] = wmul<S>(v[1 + 8], kSQH, kSQH);  // b=1,k1=2: W^2
+    v[1 + 12] = wmul<S>(v[1 + 12], kS1, kC1);  // b=1,k1=3: W^3
+    v[2 + 4] = wmul<S>(v[2 + 4], kSQH, kSQH);  // b=2,k1=1: W^2
+    v[2 + 8] = mul_si<S>(v[2 + 8]);            // b=2,k1=2: W^4
+    v[2 + 12] = wmul<S>(v[2 + 12], -kSQH, kSQH);  // b=2,k1=3: W^6
+    v[3 + 4] = wmul<S>(v[3 + 4], kS1, kC1);    // b=3,k1=1: W^3
+    v[3 + 8] = wmul<S>(v[3 + 8], -kSQH, kSQH);  // b=3,k1=2: W^6
+    v[3 + 12] = wmul<S>(v[3 + 12], -kC1, -kS1);  // b=3,k1=3: W^9
 #pragma unroll
-    for (int k = 0; k < 8; k++) {
-      v[k] = cadd(e[k], o[k]);
-      v[k + 8] = csub(e[k], o[k]);
-    }
+    for (int k1 = 0; k1 < 4; k1++) bfly4<S>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+    // v[4 k1 + k2] holds X[k1 + 4 k2]; transpose the 4 x 4 index
+    T2 t;
+    t = v[1]; v[1] = v[4]; v[4] = t;
+    t = v[2]; v[2] = v[8]; v[8] = t;
+    t = v[3]; v[3] = v[12]; v[12] = t;
+    t = v[6]; v[6] = v[9]; v[9] = t;
+    t = v[7]; v[7] = v[13]; v[13] = t;
+    t = v[11]; v[11] = v[14]; v[14] = t;
   }
 };
 
@@ -196,20 +212,22 @@ struct PassArgs {
   double *partial;      // OP_KSQ: one partial sum per block
 };
 
-// Decode (i, j, k) of axis position p for a line given by (o, q).
-__device__ __forceinline__ void decode(const PassArgs &a, long o, int p, long q, long &i, long &j, long &k) {
+// Decode (i, j, k) of axis position p for a line given by (o, q).  Grids
+// handled by the passes hold fewer than 2^31 points (checked on the host),
+// so 32-bit arithmetic suffices.
+__device__ __forceinline__ void decode(const PassArgs &a, unsigned o, int p, unsigned q, int &i, int &j, int &k) {
   if (a.axis == 2) {
-    i = o / a.ny;
-    j = o - i * a.ny;
+    i = (int) (o / (unsigned) a.ny);
+    j = (int) (o - (unsigned) i * (unsigned) a.ny);
     k = p;
   } else if (a.axis == 1) {
-    i = o;
+    i = (int) o;
     j = p;
-    k = q;
+    k = (int) q;
   } else {
     i = p;
-    j = q / a.nz;
-    k = q - j * a.nz;
+    j = (int) (q / (unsigned) a.nz);
+    k = (int) (q - (unsigned) j * (unsigned) a.nz);
   }
 }
 
@@ -227,11 +245,11 @@ __device__ __forceinline__ double absorb_ramp(long i, long j, long k, const gb_p
 }
 
 // psi * exp(c (cons + V + g |psi|^2)) for one element (src/grid_wf.c:593-597).
+// vidx is the element's index in the potential array.
 template <typename T>
-__device__ __forceinline__ C2<T> pot_factor_apply(C2<T> x, long i, long j, long k, const PassArgs &a) {
+__device__ __forceinline__ C2<T> pot_factor_apply(C2<T> x, long i, long j, long k, unsigned vidx, const PassArgs &a) {
   const gb_potential &pt = a.pot;
   double wr = pt.cons, wi = 0.0;
-  const long vidx = (i * a.ny + j) * pt.vrow + k;
   if (pt.kind == GB_POT_COMPLEX) {
     const C2<T> vv = ((const C2<T> *) pt.v)[vidx];
     wr += (double) vv.x;
@@ -260,13 +278,13 @@ template <typename T, int N, class SM, int... Ops> struct Program;
 
 template <typename T, int N, class SM> struct Program<T, N, SM> {
   // o, q identify the line; thread holds positions t + TL*m
-  static __device__ __forceinline__ void run(C2<T> (&)[Sched<N>::P], int, const SM &, const PassArgs &, long, long,
-                                             double &) {}
+  static __device__ __forceinline__ void run(C2<T> (&)[Sched<N>::P], int, const SM &, const PassArgs &, unsigned,
+                                             unsigned, double &) {}
 };
 
 template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N, SM, Op, Rest...> {
-  static __device__ __forceinline__ void run(C2<T> (&v)[Sched<N>::P], int t, const SM &sm, const PassArgs &a, long o,
-                                             long q, double &acc) {
+  static __device__ __forceinline__ void run(C2<T> (&v)[Sched<N>::P], int t, const SM &sm, const PassArgs &a, unsigned o,
+                                             unsigned q, double &acc) {
     using T2 = C2<T>;
     constexpr int P = Sched<N>::P;
     constexpr int TL = N / P;
@@ -282,11 +300,11 @@ template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N,
     } else if constexpr (Op == OP_KIN) {
       // Line factor from the two other axes, times kscale; element factor
       // from the pass axis.
-      long i, j, k;
+      int i, j, k;
       decode(a, o, 0, q, i, j, k);
       const int ax = a.axis;
       const int b0 = (ax == 0) ? 1 : 0, b1 = (ax == 2) ? 1 : 2;
-      const long idx[3] = {i, j, k};
+      const int idx[3] = {i, j, k};
       const T2 *fa = (const T2 *) a.kfac[ax];
       const T2 f0 = ((const T2 *) a.kfac[b0])[idx[b0]];
       const T2 f1 = ((const T2 *) a.kfac[b1])[idx[b1]];
@@ -302,19 +320,35 @@ template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N,
         v[m] = cmul(v[m], f);
       }
     } else if constexpr (Op == OP_POT) {
+      // decode the line once; along the pass axis the potential index
+      // advances by a fixed stride
+      int i0, j0, k0;
+      decode(a, o, 0, q, i0, j0, k0);
+      const unsigned vrow = (unsigned) a.pot.vrow, ny = (unsigned) a.ny;
+      unsigned vbase, vstride;
+      if (a.axis == 2) {
+        vbase = ((unsigned) i0 * ny + (unsigned) j0) * vrow;
+        vstride = 1u;
+      } else if (a.axis == 1) {
+        vbase = (unsigned) i0 * ny * vrow + (unsigned) k0;
+        vstride = vrow;
+      } else {
+        vbase = (unsigned) j0 * vrow + (unsigned) k0;
+        vstride = ny * vrow;
+      }
 #pragma unroll
       for (int m = 0; m < P; m++) {
-        long i, j, k;
-        decode(a, o, t + TL * m, q, i, j, k);
-        v[m] = pot_factor_apply<T>(v[m], i, j, k, a);
+        const int p = t + TL * m;
+        const int i = (a.axis == 0) ? p : i0, j = (a.axis == 1) ? p : j0, k = (a.axis == 2) ? p : k0;
+        v[m] = pot_factor_apply<T>(v[m], i, j, k, vbase + (unsigned) p * vstride, a);
       }
     } else if constexpr (Op == OP_KSQ) {
       // sum |k|^2 |v|^2 with k from the unshifted frequency grid
-      long i, j, k;
+      int i, j, k;
       decode(a, o, 0, q, i, j, k);
       const int ax = a.axis;
       const int b0 = (ax == 0) ? 1 : 0, b1 = (ax == 2) ? 1 : 2;
-      const long idx[3] = {i, j, k};
+      const int idx[3] = {i, j, k};
       const double k2line = a.ksq[b0][idx[b0]] + a.ksq[b1][idx[b1]];
 #pragma unroll
       for (int m = 0; m < P; m++) {
@@ -357,7 +391,7 @@ template <int N> struct ContigCfg {
 
 // Contiguous lines (inner == 1): L lines of N per block.
 template <typename T, int N, int... Ops>
-__global__ void __launch_bounds__(ContigCfg<N>::THREADS)
+__global__ void __launch_bounds__(ContigCfg<N>::THREADS, 2)
     k_pass_contig(const C2<T> *__restrict__ src, C2<T> *__restrict__ dst, long nlines, PassArgs a) {
   using T2 = C2<T>;
   using Cfg = ContigCfg<N>;
@@ -366,22 +400,22 @@ __global__ void __launch_bounds__(ContigCfg<N>::THREADS)
   T2 *smem = (T2 *) smraw;
   const int t = threadIdx.x % TL;
   const int l = threadIdx.x / TL;
-  const long line = (long) blockIdx.x * Cfg::L + l;
-  const bool ok = line < nlines;
-  const T2 *s = src + line * N;
+  const unsigned line = blockIdx.x * (unsigned) Cfg::L + (unsigned) l;
+  const bool ok = line < (unsigned long) nlines;
+  const T2 *s = src + (size_t) line * N;
   T2 v[P];
 #pragma unroll
   for (int m = 0; m < P; m++) v[m] = ok ? s[t + TL * m] : T2{(T) 0, (T) 0};
   SmContig<T2, Cfg::SH> sm{smem + l * Cfg::LINE};
   double acc = 0.0;
-  Program<T, N, SmContig<T2, Cfg::SH>, Ops...>::run(v, t, sm, a, ok ? line : 0, 0, acc);
+  Program<T, N, SmContig<T2, Cfg::SH>, Ops...>::run(v, t, sm, a, ok ? line : 0u, 0u, acc);
   if constexpr (has_ksq(OpL<Ops...>{})) {
     __shared__ double sbuf[(Cfg::THREADS + 31) / 32];
     double r = block_sum<Cfg::THREADS>(ok ? acc : 0.0, sbuf);
     if (threadIdx.x == 0) a.partial[blockIdx.x] = r;
   } else {
     if (ok) {
-      T2 *d = dst + line * N;
+      T2 *d = dst + (size_t) line * N;
 #pragma unroll
       for (int m = 0; m < P; m++) d[t + TL * m] = v[m];
     }
@@ -397,7 +431,7 @@ template <int N> struct StridedCfg {
 
 // Strided lines: block = (column block of BZ adjacent inner indices, outer).
 template <typename T, int N, int BZ, int... Ops>
-__global__ void __launch_bounds__((N / Sched<N>::P) * BZ)
+__global__ void __launch_bounds__((N / Sched<N>::P) * BZ, 2)
     k_pass_strided(const C2<T> *__restrict__ src, C2<T> *__restrict__ dst, long inner, PassArgs a) {
   using T2 = C2<T>;
   constexpr int P = Sched<N>::P, TL = N / P;
@@ -406,13 +440,16 @@ __global__ void __launch_bounds__((N / Sched<N>::P) * BZ)
   T2 *smem = (T2 *) smraw;
   const int c = threadIdx.x % BZ;
   const int t = threadIdx.x / BZ;
-  const long o = blockIdx.y;
-  const long q = (long) blockIdx.x * BZ + c;
-  const long off = o * (long) N * inner + q;
+  const unsigned o = blockIdx.y;
+  const unsigned q = blockIdx.x * (unsigned) BZ + (unsigned) c;
+  const unsigned in32 = (unsigned) inner;
+  // element (line, t + TL m) sits at base + (t + TL m) * inner; the whole
+  // grid has fewer than 2^31 points, so the in-tile offsets fit 32 bits
+  const size_t off = (size_t) o * (size_t) N * (size_t) inner + q;
   const T2 *s = src + off;
   T2 v[P];
 #pragma unroll
-  for (int m = 0; m < P; m++) v[m] = s[(long) (t + TL * m) * inner];
+  for (int m = 0; m < P; m++) v[m] = s[(unsigned) (t + TL * m) * in32];
   SmStrided<T2, BZ> sm{smem + c};
   double acc = 0.0;
   Program<T, N, SmStrided<T2, BZ>, Ops...>::run(v, t, sm, a, o, q, acc);
@@ -423,7 +460,7 @@ __global__ void __launch_bounds__((N / Sched<N>::P) * BZ)
   } else {
     T2 *d = dst + off;
 #pragma unroll
-    for (int m = 0; m < P; m++) d[(long) (t + TL * m) * inner] = v[m];
+    for (int m = 0; m < P; m++) d[(unsigned) (t + TL * m) * in32] = v[m];
   }
 }
 

@@ -17,6 +17,9 @@ enum {
 };
 
 void *gb__scratch(int slot, size_t bytes);
+// Pass timing brackets (no-ops unless gb_pass_timing(1) was called).
+int gb__pass_begin(int kind);
+void gb__pass_end(int slot);
 const void *gb__twiddles(long n, int prec);
 
 // Kinetic factor tables for (g, kin): per-axis complex factors exp(tm k_a^2)

@@ -188,6 +188,62 @@ void *gb__scratch(int slot, size_t bytes) {
   return s.p;
 }
 
+// ------------------------------------------------------------ pass timing
+//
+// When enabled, every line pass of the FFT schedules is bracketed by two
+// events on the library stream; gb_pass_timing_report sums the elapsed time
+// per (program, axis) kind.  Used by the benchmark to time the dominant
+// kernel inside the timed region.
+#define GB_PASS_SLOTS 8192
+static int g_pt_on = 0;
+static int g_pt_used = 0;
+static cudaEvent_t *g_pt_ev = nullptr;  // 2 per slot
+static int *g_pt_kind = nullptr;
+
+extern "C" int gb_pass_timing(int on) {
+  if (on && !g_pt_ev) {
+    g_pt_ev = (cudaEvent_t *) malloc(sizeof(cudaEvent_t) * 2 * GB_PASS_SLOTS);
+    g_pt_kind = (int *) malloc(sizeof(int) * GB_PASS_SLOTS);
+    for (int i = 0; i < 2 * GB_PASS_SLOTS; i++) cudaEventCreate(&g_pt_ev[i]);
+  }
+  g_pt_on = on;
+  g_pt_used = 0;
+  return 0;
+}
+
+int gb__pass_begin(int kind) {
+  if (!g_pt_on || g_pt_used >= GB_PASS_SLOTS) return -1;
+  const int s = g_pt_used++;
+  g_pt_kind[s] = kind;
+  cudaEventRecord(g_pt_ev[2 * s], g_stream);
+  return s;
+}
+
+void gb__pass_end(int slot) {
+  if (slot >= 0) cudaEventRecord(g_pt_ev[2 * slot + 1], g_stream);
+}
+
+extern "C" int gb_pass_timing_report(double *ms, long *count, int nkinds) {
+  for (int k = 0; k < nkinds; k++) {
+    ms[k] = 0.0;
+    count[k] = 0;
+  }
+  cudaStreamSynchronize(g_stream);
+  for (int s = 0; s < g_pt_used; s++) {
+    float e = 0.f;
+    if (cudaEventElapsedTime(&e, g_pt_ev[2 * s], g_pt_ev[2 * s + 1]) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    const int k = g_pt_kind[s];
+    if (k >= 0 && k < nkinds) {
+      ms[k] += e;
+      count[k]++;
+    }
+  }
+  return g_pt_used;
+}
+
 // ------------------------------------------------------------ conversions
 
 template <typename A, typename B> __global__ void k_convert(B *__restrict__ dst, const A *__restrict__ src, size_t n) {

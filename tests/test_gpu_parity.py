@@ -44,6 +44,27 @@ def test_fft3d_matches_numpy(b200, shape):
     b200.free(g)
 
 
+def test_fft_non_power_of_two_fails_loudly():
+    """The GPU FFT takes power-of-two line lengths (as the reference's CUDA
+    build, src/cgrid.c:113-116); other lengths abort with a libgrid message
+    instead of computing anything on a fallback path."""
+    import subprocess
+    import sys
+
+    code = (
+        "import sys; sys.path.insert(0, %r)\n"
+        "import libgrid_b200 as gb\n"
+        "api = gb.load()\n"
+        "g = api.cgrid(12, 10, 14, 0.1)\n"
+        "api.lib.cgrid_fft(g.ptr)\n"
+        "print('returned')\n"
+    ) % (__import__("conftest").ROOT,)
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=300)
+    assert p.returncode != 0
+    assert "returned" not in p.stdout
+    assert "power of two" in p.stderr
+
+
 # ----------------------------------------------------- split-operator step
 
 
@@ -230,7 +251,7 @@ def test_norm_and_energies(b200, restate, shape):
         e = b200.lib.grid_wf_energy(w.ptr, vx.ptr)
         e_ref = t_ref + restate.potential_energy(psi, workloads.padded(v), step)
         assert abs(e - e_ref) <= 1e-12 * abs(e_ref) + 1e-13
-        if bc == PER:
+        if bc == PER and all(n & (n - 1) == 0 for n in shape):
             t_fft = b200.lib.grid_wf_kinetic_energy_fft(w.ptr)
             t_fft_ref = restate.kinetic_energy_fft(psi, step, mass)
             assert abs(t_fft - t_fft_ref) <= 1e-12 * abs(t_fft_ref)
@@ -345,6 +366,8 @@ def test_energy_and_error_vs_reference(b200, ref):
     x, y, z = workloads.mesh(*shape, step)
     v = (0.5 * 0.3 * (x * x + y * y + z * z)).astype(complex)
     psi = np.exp(-(x * x + y * y + z * z) / 5.0) * (1 + 0.2 * y)
+    # the error formula assumes a normalized state (src/grid_wf_diag.c:49-60)
+    psi = psi / np.sqrt(np.sum(np.abs(psi) ** 2) * step**3)
     res = []
     for api in (b200, ref):
         w = api.wf(*shape, step, mass, PER, FFT2, values=psi)
