@@ -67,7 +67,7 @@ class ClockSampler:
     """nvidia-smi clock/throttle samples during the timed region."""
 
     Q = (
-        "index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        "timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap"
     )
@@ -75,11 +75,13 @@ class ClockSampler:
     def __init__(self, gpu: int):
         self.gpu = gpu
         self.p = None
+        self.t0 = self.t1 = None
+        self.out = ""
 
-    def __enter__(self):
+    def start(self):
         try:
             self.p = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits", "-lms", "200"],
+                ["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q, "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE,
                 stderr=subprocess.DEVNULL,
                 text=True,
@@ -88,38 +90,52 @@ class ClockSampler:
             self.p = None
         return self
 
-    def __exit__(self, *exc):
-        self.out = ""
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_stop(self):
+        self.t1 = time.time()
+
+    def stop(self):
         if self.p:
+            time.sleep(0.12)
             self.p.terminate()
             try:
                 self.out, _ = self.p.communicate(timeout=5)
             except Exception:
                 self.p.kill()
-        return False
 
     def summary(self):
-        sms, maxs, reasons = [], [], set()
+        import datetime
+
+        sms, maxs, reasons, used = [], [], set(), 0
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in (self.out or "").strip().splitlines():
+        lines = (self.out or "").strip().splitlines()
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
+            if len(f) < 10:
                 continue
             try:
-                sms.append(float(f[1]))
-                maxs.append(float(f[2]))
+                ts = datetime.datetime.strptime(f[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                sm, mx = float(f[2]), float(f[3])
             except ValueError:
                 continue
-            for n, v in zip(names, f[5:9]):
+            # samples inside the timed region (plus one sampling period of slack)
+            if self.t0 is not None and not (self.t0 - 0.05 <= ts <= self.t1 + 0.05):
+                continue
+            used += 1
+            sms.append(sm)
+            maxs.append(mx)
+            for n, v in zip(names, f[6:10]):
                 if v.lower().startswith("active"):
                     reasons.add(n)
         if not sms:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "samples_total": len(lines)}
         return {
             "sm_mhz": float(np.median(sms)),
             "sm_max_mhz": float(max(maxs)),
             "reasons": sorted(reasons),
-            "samples": len(sms),
+            "samples": used,
         }
 
 
@@ -173,7 +189,9 @@ def run_reference(args, world, rank):
     if rank != 0:
         return 0
     nproc = len(os.sched_getaffinity(0))
-    r = cpu_baseline(args.size, args.steps, args.warmup)
+    # a bounded sample of the workload: at most 60 timed steps (~20 s on 16
+    # host cores at 256^3) after at most 2 warm-up steps
+    r = cpu_baseline(args.size, min(args.steps, 60), min(args.warmup, 2))
     line = {
         "impl": "reference",
         "metric": METRIC.replace("(FP64, resident in HBM)", "(FP64)"),
@@ -219,19 +237,29 @@ def run_b200(args, world, rank, local):
 
     # ---------------------------------------------- FP64, resident in HBM
     w, vx = make()
-    for _ in range(args.warmup):
+    clk = ClockSampler(local).start()
+    # warm-up: at least W steps and at least 1.5 s, so the clock sampler is
+    # running and the clocks have settled before the timed region
+    tw = time.perf_counter()
+    done = 0
+    while done < args.warmup or time.perf_counter() - tw < 1.5:
         w.propagate_gp(vx, g, dt)
+        done += 1
+        if done % 50 == 0:
+            lib.gb_synchronize()
     lib.gb_synchronize()
     lib.gb_pass_timing(1)
     barrier(world)
     lib.gb_synchronize()
     l0 = lib.gb_launch_count()
-    with ClockSampler(local) as clk:
-        lib.gb_event_record(0)
-        for _ in range(args.steps):
-            w.propagate_gp(vx, g, dt)
-        lib.gb_event_record(1)
-        lib.gb_synchronize()
+    clk.mark_start()
+    lib.gb_event_record(0)
+    for _ in range(args.steps):
+        w.propagate_gp(vx, g, dt)
+    lib.gb_event_record(1)
+    lib.gb_synchronize()
+    clk.mark_stop()
+    clk.stop()
     launches = lib.gb_launch_count() - l0
     ms = lib.gb_event_elapsed_ms(0, 1)
     barrier(world)
@@ -377,11 +405,11 @@ def C_int_array(v):
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=50)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", type=int, default=256)
-    ap.add_argument("--cpu-steps", type=int, default=8)
+    ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args(argv)
     world, rank, local = dist_setup()
