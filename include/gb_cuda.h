@@ -187,6 +187,21 @@ int gb_wf_merge(void *dst, const void *wr, const void *wi, const gb_geom *g, lon
 #define GB_RED_KSQ_NORM2 7    /* sum |k|^2 |a|^2 on the unshifted frequency grid */
 int gb_reduce(int op, const void *a, const void *b, const gb_geom *g, long arow, long brow, int bprec, double *out);
 
+/*
+ * gb_reduce without any device allocation: no reference counterpart.  For
+ * callers that cannot let a library allocate device memory (applications
+ * that own all device memory through their own pool or a fixed budget, and
+ * latency-critical loops where cudaMalloc or the synchronisation of cudaFree
+ * is not acceptable).  Same operations and arguments as gb_reduce; the
+ * partial sums live in a fixed file-scope __device__ array (8193 x 16 B) that
+ * limits a call to grids of at most 16,777,216 points (larger grids are
+ * rejected with an error before any launch).  All calls share that array:
+ * calls that overlap on the GPU race.  The first call on a device looks up
+ * the array's address (cudaGetSymbolAddress); make it before any stream
+ * capture.  Requires gb_init / cuda_enable first.
+ */
+int gb_reduce_noalloc(int op, const void *a, const void *b, const gb_geom *g, long arow, long brow, int bprec, double *out);
+
 /* --------------------------------------------------- finite differences */
 #define GB_BC_DIRICHLET 0
 #define GB_BC_NEUMANN 1

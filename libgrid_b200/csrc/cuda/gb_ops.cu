@@ -7,6 +7,7 @@
 // grid-stride pass with a fixed per-thread order, a fixed shuffle tree per
 // block and a fixed-order finish over the block partials, so the result does
 // not depend on scheduling.
+#include <stdio.h>
 #include <string.h>
 
 #include "gb_common.cuh"
@@ -336,4 +337,169 @@ extern "C" int gb_reduce(int op, const void *a, const void *b, const gb_geom *g,
   out[0] = h.x;
   out[1] = h.y;
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free reduction (gb_reduce_noalloc).
+//
+// Some callers cannot let a library allocate device memory on their behalf:
+// applications that hand out all device memory from their own pool or under
+// a fixed budget, and latency-critical loops in which a cudaMalloc, or the
+// device-wide synchronisation of cudaFree, is not acceptable.  For them this
+// variant of gb_reduce keeps its block partial sums and its result in a
+// file-scope __device__ array of fixed size instead of library scratch, so
+// no call allocates anything.
+//
+// Limits and sharing:
+//  * One block per 2048 grid points and at most 8192 blocks: grids of up to
+//    16,777,216 points (256^3).  Larger grids are rejected with an error
+//    before any work is launched.
+//  * The array (8193 x 16 bytes) lives in every GPU that loads the library
+//    until the process exits.  Every call uses the same array and leaves its
+//    last contents behind; each call writes every slot it reads, so nothing
+//    needs clearing, but two calls that overlap on the GPU (e.g. from
+//    different streams or processes sharing the context) race on it.
+//  * The host code needs the array's device address, which the first call on
+//    a device obtains with cudaGetSymbolAddress while that device is current.
+//    Make that first call before any stream capture.
+//  * The library stream must exist (gb_init / cuda_enable called first).
+namespace {
+
+constexpr int kNoallocThreads = 256;
+constexpr int kNoallocPerThread = 8;
+constexpr long kNoallocBlockElems = (long) kNoallocThreads * kNoallocPerThread;
+constexpr long kNoallocMaxBlocks = 8192;
+
+__device__ __align__(256) double2 g_noalloc_scratch[kNoallocMaxBlocks + 1];
+
+double2 *g_noalloc_dev_ptr = nullptr;
+int g_noalloc_device = -1;
+
+// One element's contribution to the reductions of gb_reduce.
+template <typename TA, typename TB>
+__device__ __forceinline__ void noalloc_term(int op, const void *av, const void *bv, size_t g, size_t ij, size_t k,
+                                             long arow, long brow, long nx, long ny, long nz, double step, double &sx,
+                                             double &sy) {
+  switch (op) {
+    case GB_RED_SUM: {
+      const C2<TA> a = ((const C2<TA> *) av)[g];
+      sx += (double) a.x;
+      sy += (double) a.y;
+    } break;
+    case GB_RED_NORM2: {
+      const C2<TA> a = ((const C2<TA> *) av)[g];
+      sx += (double) a.x * (double) a.x + (double) a.y * (double) a.y;
+    } break;
+    case GB_RED_CONJ_PRODUCT: {
+      const C2<TA> a = ((const C2<TA> *) av)[g];
+      const C2<TB> b = ((const C2<TB> *) bv)[g];
+      const double ar = a.x, ai = a.y, br = b.x, bi = b.y;
+      sx += ar * br + ai * bi;
+      sy += ar * bi - ai * br;
+    } break;
+    case GB_RED_EXPECT_COMPLEX: {
+      const C2<TA> a = ((const C2<TA> *) av)[g];
+      const C2<TB> b = ((const C2<TB> *) bv)[g];
+      const double w = (double) a.x * (double) a.x + (double) a.y * (double) a.y;
+      sx += w * (double) b.x;
+      sy += w * (double) b.y;
+    } break;
+    case GB_RED_EXPECT_REAL: {
+      const C2<TA> a = ((const C2<TA> *) av)[g];
+      const double w = (double) a.x * (double) a.x + (double) a.y * (double) a.y;
+      sx += w * (double) ((const TB *) bv)[ij * brow + k];
+    } break;
+    case GB_RED_REAL_SUM: sx += (double) ((const TA *) av)[ij * arow + k]; break;
+    case GB_RED_KSQ_NORM2: {
+      const long j = (long) (ij % ny), i = (long) (ij / ny);
+      const double lx = 2.0 * M_PI / (step * (double) nx), ly = 2.0 * M_PI / (step * (double) ny),
+                   lz = 2.0 * M_PI / (step * (double) nz);
+      const double kx = (i <= nx / 2 ? (double) i : (double) (i - nx)) * lx;
+      const double ky = (j <= ny / 2 ? (double) j : (double) (j - ny)) * ly;
+      const double kz = ((long) k <= nz / 2 ? (double) k : (double) ((long) k - nz)) * lz;
+      const C2<TA> a = ((const C2<TA> *) av)[g];
+      sx += (kx * kx + ky * ky + kz * kz) * ((double) a.x * (double) a.x + (double) a.y * (double) a.y);
+    } break;
+  }
+}
+
+// Block b sums grid points [2048 b, 2048 (b + 1)) in a fixed order and
+// writes one partial into scratch[b].
+template <typename TA, typename TB>
+__global__ void __launch_bounds__(kNoallocThreads)
+    k_reduce_noalloc(int op, const void *av, const void *bv, long nxy, long nz, long arow, long brow, double2 *scratch,
+                     long nx, long ny, double step) {
+  __shared__ double sb[2 * kNoallocThreads / 32];
+  const size_t n = (size_t) nxy * nz;
+  const size_t base = (size_t) blockIdx.x * kNoallocBlockElems;
+  double sx = 0.0, sy = 0.0;
+#pragma unroll
+  for (int r = 0; r < kNoallocPerThread; r++) {
+    const size_t g = base + (size_t) r * kNoallocThreads + threadIdx.x;
+    if (g < n) {
+      const size_t ij = g / nz, k = g - ij * nz;
+      noalloc_term<TA, TB>(op, av, bv, g, ij, k, arow, brow, nx, ny, nz, step, sx, sy);
+    }
+  }
+  block_sum2<kNoallocThreads>(sx, sy, sb);
+  if (threadIdx.x == 0) scratch[blockIdx.x] = make_double2(sx, sy);
+}
+
+// Fixed-order sum of the nb partials into scratch[kNoallocMaxBlocks].
+__global__ void k_finish_noalloc(double2 *scratch, int nb) {
+  __shared__ double sb[2 * 1024 / 32];
+  double sx = 0.0, sy = 0.0;
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) {
+    sx += scratch[i].x;
+    sy += scratch[i].y;
+  }
+  block_sum2<1024>(sx, sy, sb);
+  if (threadIdx.x == 0) scratch[kNoallocMaxBlocks] = make_double2(sx, sy);
+}
+
+}  // namespace
+
+extern "C" int gb_reduce_noalloc(int op, const void *a, const void *b, const gb_geom *g, long arow, long brow, int bprec,
+                                 double *out) {
+  const long nxy = g->nx * g->ny;
+  const double npts = (double) nxy * (double) g->nz;
+  if (npts > (double) (kNoallocMaxBlocks * kNoallocBlockElems)) {
+    char msg[160];
+    snprintf(msg, sizeof(msg), "gb_reduce_noalloc: %.0f grid points exceed the %ld-point limit of its static scratch", npts,
+             kNoallocMaxBlocks * kNoallocBlockElems);
+    return gb__set_error(1020, msg);
+  }
+  cudaStream_t st = gb__stream();
+  if (!st) return gb__set_error(1021, "gb_reduce_noalloc: library not initialised (call gb_init or cuda_enable first)");
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return gb__set_error(1022, "gb_reduce_noalloc: cudaGetDevice failed");
+  if (!g_noalloc_dev_ptr || dev != g_noalloc_device) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return gb__set_error((int) e, "gb_reduce_noalloc: cudaGetSymbolAddress failed");
+    g_noalloc_dev_ptr = (double2 *) p;
+    g_noalloc_device = dev;
+  }
+  const int nb = (int) ((nxy * g->nz + kNoallocBlockElems - 1) / kNoallocBlockElems);
+  if (nb < 1) {
+    out[0] = out[1] = 0.0;
+    return 0;
+  }
+  const bool af = (g->prec == GB_FP32);
+  const bool bf = (bprec == GB_FP32);
+  double2 *sp = g_noalloc_dev_ptr;
+  if (af && bf) k_reduce_noalloc<float, float><<<nb, kNoallocThreads, 0, st>>>(op, a, b, nxy, g->nz, arow, brow, sp, g->nx, g->ny, g->step);
+  else if (af) k_reduce_noalloc<float, double><<<nb, kNoallocThreads, 0, st>>>(op, a, b, nxy, g->nz, arow, brow, sp, g->nx, g->ny, g->step);
+  else if (bf) k_reduce_noalloc<double, float><<<nb, kNoallocThreads, 0, st>>>(op, a, b, nxy, g->nz, arow, brow, sp, g->nx, g->ny, g->step);
+  else k_reduce_noalloc<double, double><<<nb, kNoallocThreads, 0, st>>>(op, a, b, nxy, g->nz, arow, brow, sp, g->nx, g->ny, g->step);
+  GB_CHECK_LAUNCH("reduce noalloc");
+  k_finish_noalloc<<<1, 1024, 0, st>>>(sp, nb);
+  GB_CHECK_LAUNCH("reduce noalloc finish");
+  double2 h;
+  const cudaError_t e = cudaMemcpyAsync(&h, sp + kNoallocMaxBlocks, sizeof(double2), cudaMemcpyDeviceToHost, st);
+  const cudaError_t s = (e == cudaSuccess) ? cudaStreamSynchronize(st) : e;
+  if (s != cudaSuccess) return gb__set_error((int) s, "gb_reduce_noalloc: result copy");
+  out[0] = h.x;
+  out[1] = h.y;
+  return 0;
 }
