@@ -93,7 +93,8 @@ float gb_event_elapsed_ms(int start_slot, int stop_slot);
 /* Per-pass timing of the FFT line passes with CUDA events on the library
  * stream (benchmark instrumentation).  Kinds are 5 * axis + program with
  * axis 0 x, 1 y, 2 z and program 0 forward FFT, 1 inverse FFT,
- * 2 forward + kinetic + inverse, 3 inverse + potential + forward, 4 other.
+ * 2 forward + kinetic + inverse, 3 inverse + potential + forward, 4 other;
+ * kinds 15 + axis are the Crank-Nicolson line sweeps.
  * report() fills ms[k] / count[k] for k < nkinds and returns the number of
  * timed passes. */
 int gb_pass_timing(int on);
@@ -128,6 +129,12 @@ int gb_split_step(void *psi, const gb_geom *g, const gb_kinetic *kin, const gb_p
 #define GB_K_GRADIENT_Y 3
 #define GB_K_GRADIENT_Z 4
 int gb_kspace_op(int op, void *dst, const void *src, const gb_geom *g);
+
+/* Self-test: the propagation kernels' FP64 phase sine/cosine against the
+ * CUDA library sincos on n host arguments; max_err[0..1] receives the
+ * largest absolute differences of sin and cos.  (Test hook; no counterpart
+ * in the reference.) */
+int gb_sincos_selftest(const double *x_host, long n, double *max_err);
 
 /* Pointwise kinetic factor on a k-space grid
  * (src/grid_wf_fft-cuda2.cu:23-99 and :108-138). */

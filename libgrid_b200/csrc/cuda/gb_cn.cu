@@ -124,7 +124,7 @@ __device__ __forceinline__ double2 cn_pot(double2 x, long ix, long iy, long iz, 
   }
   const double ar = cr * wr - ci * wi, ai = cr * wi + ci * wr;
   double s, c;
-  sincos(ai, &s, &c);
+  gb_sincos(ai, &s, &c);
   if (ar != 0.0) {
     const double m = exp(ar);
     s *= m;
@@ -678,7 +678,11 @@ extern "C" int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, co
         const size_t sm = (size_t) lpc * row * 16;
         cudaFuncSetAttribute(k_cn_fast<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
         const long nb = (a.outer + lpc - 1) / lpc;
-        k_cn_fast<true><<<(unsigned) nb, 32 * kSeg, sm, st>>>((double2 *) psi, a);
+        {
+          const int slot = gb__pass_begin(15 + axis);
+          k_cn_fast<true><<<(unsigned) nb, 32 * kSeg, sm, st>>>((double2 *) psi, a);
+          gb__pass_end(slot);
+        }
       } else {
         long cap = (long) (budget / (a.n * 16));
         if (cap > 32) cap = 32;
@@ -689,7 +693,11 @@ extern "C" int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, co
         cudaFuncSetAttribute(k_cn_fast<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
         if (a.outer > 65535) return gb__set_error(1012, "cn: outer extent above 65535");
         dim3 grid((unsigned) (a.inner / lpc), (unsigned) a.outer);
-        k_cn_fast<false><<<grid, 32 * kSeg, sm, st>>>((double2 *) psi, a);
+        {
+          const int slot = gb__pass_begin(15 + axis);
+          k_cn_fast<false><<<grid, 32 * kSeg, sm, st>>>((double2 *) psi, a);
+          gb__pass_end(slot);
+        }
       }
       GB_CHECK_LAUNCH("cn fast");
     } else {
@@ -699,7 +707,11 @@ extern "C" int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, co
       a.work = work;
       if (!contig) a.inner = a.inner;  // strided addressing in the kernel
       const long nb = (a.nlines + 127) / 128;
-      k_cn_general<<<(unsigned) nb, 128, 0, st>>>((double2 *) psi, a);
+      {
+        const int slot = gb__pass_begin(15 + axis);
+        k_cn_general<<<(unsigned) nb, 128, 0, st>>>((double2 *) psi, a);
+        gb__pass_end(slot);
+      }
       GB_CHECK_LAUNCH("cn general");
       if (a.post.kind != GB_POT_NONE || a.post.g != 0.0) GB_TRYC(gb_potential_multiply(psi, g, &a.post));
     }

@@ -51,26 +51,92 @@ template <typename T> __device__ __forceinline__ C2<T> to_c2(double re, double i
 #define GB_TWO_PI_LO 2.4492935982947063e-16
 #define GB_INV_TWO_PI 0.15915494309189533577
 
+// sin and cos of a phase argument in FP64 for |x| <= 1e7 (larger arguments
+// use the CUDA library routine).  Cody-Waite reduction by pi/2 (W. J. Cody,
+// W. Waite, "Software Manual for the Elementary Functions", 1980): n =
+// rint(x 2/pi), r = x - n (P1 + P2 + P3) with P1, P2 holding the leading 30
+// significant bits of pi/2 each (so n P1 and n P2 are exact for |n| < 2^23)
+// and P3 the rounded remainder, split here from the decimal expansion of pi.
+// On |r| <= pi/4 the Taylor series of sin and cos are cut after r^17/17! and
+// r^16/16! (truncation below 1e-17) and evaluated by Horner in r^2.  The
+// quadrant q = n mod 4 is applied without branches: q odd swaps sin and
+// cos, bit 1 of q (of q + 1 for the cosine) flips the sign.
+// The library fallback stays out of line, so the unrolled per-element loops
+// of the passes hold one copy of it.
+static __device__ __noinline__ double2 gb_sincos_lib(double x) {
+  double s, c;
+  sincos(x, &s, &c);
+  return double2{s, c};
+}
+
+__device__ __forceinline__ double gb_flip_sign(double v, int bit2) {
+  return __hiloint2double(__double2hiint(v) ^ (bit2 << 30), __double2loint(v));
+}
+
+// (sin x, cos x) for |x| <= 1e7.
+__device__ __forceinline__ double2 gb_sincos_reduced(double x) {
+  const double n = rint(x * 0.6366197723675814);
+  const int q = __double2int_rn(n);
+  double r = fma(-n, 1.570796325802803, x);
+  r = fma(-n, 9.920935791635221e-10, r);
+  r = fma(-n, 5.170182981794105e-19, r);
+  const double s2 = r * r;
+  double ps = 2.8114572543455206e-15;
+  ps = fma(ps, s2, -7.647163731819816e-13);
+  ps = fma(ps, s2, 1.6059043836821613e-10);
+  ps = fma(ps, s2, -2.505210838544172e-08);
+  ps = fma(ps, s2, 2.7557319223985893e-06);
+  ps = fma(ps, s2, -0.0001984126984126984);
+  ps = fma(ps, s2, 0.008333333333333333);
+  ps = fma(ps, s2, -0.16666666666666666);
+  double pc = 4.779477332387385e-14;
+  pc = fma(pc, s2, -1.1470745597729725e-11);
+  pc = fma(pc, s2, 2.08767569878681e-09);
+  pc = fma(pc, s2, -2.755731922398589e-07);
+  pc = fma(pc, s2, 2.48015873015873e-05);
+  pc = fma(pc, s2, -0.001388888888888889);
+  pc = fma(pc, s2, 0.041666666666666664);
+  pc = fma(pc, s2, -0.5);
+  const double sr = fma(r * s2, ps, r);
+  const double cr = fma(s2, pc, 1.0);
+  const bool swap = (q & 1) != 0;
+  const double s = swap ? cr : sr;
+  const double c = swap ? sr : cr;
+  return double2{gb_flip_sign(s, q & 2), gb_flip_sign(c, (q + 1) & 2)};
+}
+
+// (sin x, cos x) for any x.
+__device__ __forceinline__ double2 gb_sincos2(double x) {
+  if (!(fabs(x) <= 1.0e7)) return gb_sincos_lib(x);
+  return gb_sincos_reduced(x);
+}
+
+__device__ __forceinline__ void gb_sincos(double x, double *sp, double *cp) {
+  const double2 sc = gb_sincos2(x);
+  *sp = sc.x;
+  *cp = sc.y;
+}
+
 // exp(a + i b) as a complex number of type T, with both a and b evaluated in
 // FP64.  FP64 mode: exp and sincos in FP64.  FP32 mode: b is reduced into
-// [-pi, pi] in FP64, then sincosf/expf in FP32.
+// [-pi, pi] in FP64, then the hardware sine/cosine and the FP64 exp rounded
+// to FP32.
 template <typename T> __device__ __forceinline__ C2<T> cexp_phase(double a, double b, bool has_a) {
   if constexpr (sizeof(T) == 8) {
-    double s, c;
-    sincos(b, &s, &c);
+    const double2 sc = gb_sincos2(b);
     if (has_a) {
-      double m = exp(a);
-      return C2<T>{m * c, m * s};
+      const double m = exp(a);
+      return C2<T>{m * sc.y, m * sc.x};
     }
-    return C2<T>{c, s};
+    return C2<T>{sc.y, sc.x};
   } else {
-    double n = rint(b * GB_INV_TWO_PI);
+    const double n = rint(b * GB_INV_TWO_PI);
     double r = fma(-n, GB_TWO_PI_HI, b);
     r = fma(-n, GB_TWO_PI_LO, r);
     float s, c;
-    sincosf((float) r, &s, &c);
+    __sincosf((float) r, &s, &c);
     if (has_a) {
-      float m = (float) exp(a);
+      const float m = (float) exp(a);
       return C2<T>{m * c, m * s};
     }
     return C2<T>{c, s};

@@ -2,6 +2,7 @@
 // standalone pointwise kinetic and potential factors, and the deterministic
 // partial-sum finisher.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "gb_fft_impl.cuh"
@@ -221,6 +222,43 @@ extern "C" int gb_fft_ksq_sum(const void *psi, void *work, const gb_geom *g, dou
   if (fft_geom_ok(g)) return gb_last_error();
   if (g->prec == GB_FP32) return gb__ksq_sum_t<float>(psi, work, g, out);
   return gb__ksq_sum_t<double>(psi, work, g, out);
+}
+
+// Self-test of the phase sine/cosine: gb_sincos against the CUDA library
+// sincos, element by element.
+__global__ void k_sincos_check(const double *x, long n, double *err) {
+  const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double s0, c0, s1, c1;
+  sincos(x[i], &s0, &c0);
+  gb_sincos(x[i], &s1, &c1);
+  err[2 * i] = fabs(s1 - s0);
+  err[2 * i + 1] = fabs(c1 - c0);
+}
+
+extern "C" int gb_sincos_selftest(const double *x_host, long n, double *max_err) {
+  if (n <= 0) return gb__set_error(1020, "sincos self-test: empty input");
+  double *d = nullptr;
+  if (cudaMalloc(&d, (size_t) n * 3 * sizeof(double)) != cudaSuccess) return gb__set_error(2, "sincos self-test");
+  cudaStream_t st = gb__stream();
+  cudaMemcpyAsync(d, x_host, (size_t) n * sizeof(double), cudaMemcpyHostToDevice, st);
+  k_sincos_check<<<(unsigned) ((n + 255) / 256), 256, 0, st>>>(d, n, d + n);
+  double *h = (double *) malloc((size_t) n * 2 * sizeof(double));
+  cudaMemcpyAsync(h, d + n, (size_t) n * 2 * sizeof(double), cudaMemcpyDeviceToHost, st);
+  const cudaError_t e = cudaStreamSynchronize(st);
+  cudaFree(d);
+  if (e != cudaSuccess) {
+    free(h);
+    return gb__set_error((int) e, "sincos self-test");
+  }
+  max_err[0] = max_err[1] = 0.0;
+  for (long i = 0; i < n; i++) {
+    if (h[2 * i] > max_err[0]) max_err[0] = h[2 * i];
+    if (h[2 * i + 1] > max_err[1]) max_err[1] = h[2 * i + 1];
+  }
+  free(h);
+  gb__count_launch();
+  return 0;
 }
 
 extern "C" int gb_kspace_op(int op, void *dst, const void *src, const gb_geom *g) {

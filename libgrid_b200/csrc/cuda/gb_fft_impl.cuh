@@ -137,14 +137,27 @@ template <int R0, int... Rest> __host__ __device__ constexpr int first_radix(IL<
 
 __host__ __device__ constexpr int ilog2c(int v) { return v <= 1 ? 0 : 1 + ilog2c(v / 2); }
 
-// Shared-memory views.
+// Shared-memory views.  sync() orders the exchange between radix stages
+// among the threads that share a line: strided tiles interleave their lines
+// across the whole CTA; a contiguous line of TL threads lives inside one
+// warp when TL <= 32 (warp barrier), else in TL / 32 consecutive warps
+// (named barrier 1 + line, as id 0 is the CTA barrier).
 template <typename T2, int BZ> struct SmStrided {
   T2 *p;
   __device__ __forceinline__ T2 &operator()(int pos) const { return p[pos * BZ]; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
 };
-template <typename T2, int SH> struct SmContig {
+template <typename T2, int SH, int TL> struct SmContig {
   T2 *p;
   __device__ __forceinline__ T2 &operator()(int pos) const { return p[pos + (pos >> SH)]; }
+  __device__ __forceinline__ void sync() const {
+    if constexpr (TL <= 32) {
+      __syncwarp();
+    } else {
+      static_assert(TL % 32 == 0 && 256 / TL <= 15, "named barriers per line");
+      asm volatile("bar.sync %0, %1;" ::"r"(1 + (int) (threadIdx.x / TL)), "r"(TL) : "memory");
+    }
+  }
 };
 
 // One Stockham stage; v holds positions t + TL*m on entry and exit.
@@ -179,10 +192,10 @@ __device__ __forceinline__ void fft_stage(T2 (&v)[P], int t, const SM &sm, const
     }
   }
   if constexpr (!LAST) {
-    __syncthreads();
+    sm.sync();
 #pragma unroll
     for (int m = 0; m < P; m++) v[m] = sm(t + TL * m);
-    __syncthreads();
+    sm.sync();
   }
 }
 
@@ -269,6 +282,31 @@ __device__ __forceinline__ C2<T> pot_factor_apply(C2<T> x, long i, long j, long 
   return cmul(x, cexp_phase<T>(ar, ai, ar != 0.0));
 }
 
+// Potential factor on a register line when V is real or absent and there
+// is no absorbing region: the exponent c (cons + V + g |psi|^2) is then
+// purely imaginary when Re c = 0 (real time: a phase) or purely real when
+// Im c = 0 (imaginary time: a decay), and only sincos or exp is needed.
+// Same values as pot_factor_apply for these cases.
+template <typename T, int P, int TL, bool HAS_V, bool PHASE>
+__device__ __forceinline__ void pot_line_simple(C2<T> (&v)[P], int t, const T *vp, unsigned vs, double cons,
+                                                double g, double cc) {
+#pragma unroll
+  for (int m = 0; m < P; m++) {
+    const int p = t + TL * m;
+    double w = cons;
+    if constexpr (HAS_V) w += (double) vp[(unsigned) p * vs];
+    const double xr = (double) v[m].x, xi = (double) v[m].y;
+    w = fma(g, fma(xr, xr, xi * xi), w);
+    const double arg = cc * w;
+    if constexpr (PHASE) {
+      v[m] = cmul(v[m], cexp_phase<T>(0.0, arg, false));
+    } else {
+      const T f = (T) exp(arg);
+      v[m] = C2<T>{v[m].x * f, v[m].y * f};
+    }
+  }
+}
+
 template <int Op, int... Rest> struct OpsHead {
   static constexpr int value = Op;
 };
@@ -304,20 +342,25 @@ template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N,
       decode(a, o, 0, q, i, j, k);
       const int ax = a.axis;
       const int b0 = (ax == 0) ? 1 : 0, b1 = (ax == 2) ? 1 : 2;
-      const int idx[3] = {i, j, k};
+      const int ix0 = (ax == 0) ? j : i, ix1 = (ax == 2) ? j : k;
       const T2 *fa = (const T2 *) a.kfac[ax];
-      const T2 f0 = ((const T2 *) a.kfac[b0])[idx[b0]];
-      const T2 f1 = ((const T2 *) a.kfac[b1])[idx[b1]];
+      const T2 f0 = ((const T2 *) a.kfac[b0])[ix0];
+      const T2 f1 = ((const T2 *) a.kfac[b1])[ix1];
       T2 lf = cmul(f0, f1);
       lf = cscale(lf, (T) a.kscale);
       double k2line = 0.0;
-      if (a.cutoff) k2line = a.ksq[b0][idx[b0]] + a.ksq[b1][idx[b1]];
+      if (a.cutoff) k2line = a.ksq[b0][ix0] + a.ksq[b1][ix1];
+      if (a.cutoff) {
 #pragma unroll
-      for (int m = 0; m < P; m++) {
-        const int p = t + TL * m;
-        T2 f = cmul(lf, fa[p]);
-        if (a.cutoff && (k2line + a.ksq[ax][p] >= a.kmax2)) f = T2{(T) 0, (T) 0};
-        v[m] = cmul(v[m], f);
+        for (int m = 0; m < P; m++) {
+          const int p = t + TL * m;
+          T2 f = cmul(lf, fa[p]);
+          if (k2line + a.ksq[ax][p] >= a.kmax2) f = T2{(T) 0, (T) 0};
+          v[m] = cmul(v[m], f);
+        }
+      } else {
+#pragma unroll
+        for (int m = 0; m < P; m++) v[m] = cmul(v[m], cmul(lf, fa[t + TL * m]));
       }
     } else if constexpr (Op == OP_POT) {
       // decode the line once; along the pass axis the potential index
@@ -336,11 +379,25 @@ template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N,
         vbase = (unsigned) j0 * vrow + (unsigned) k0;
         vstride = ny * vrow;
       }
+      const gb_potential &pt = a.pot;
+      if (!pt.absorb && pt.kind != GB_POT_COMPLEX && (pt.c_re == 0.0 || pt.c_im == 0.0)) {
+        const bool phase = (pt.c_re == 0.0);
+        const double cc = phase ? pt.c_im : pt.c_re;
+        const T *vp = (const T *) pt.v + vbase;
+        if (pt.kind == GB_POT_REAL) {
+          if (phase) pot_line_simple<T, P, TL, true, true>(v, t, vp, vstride, pt.cons, pt.g, cc);
+          else pot_line_simple<T, P, TL, true, false>(v, t, vp, vstride, pt.cons, pt.g, cc);
+        } else {
+          if (phase) pot_line_simple<T, P, TL, false, true>(v, t, vp, vstride, pt.cons, pt.g, cc);
+          else pot_line_simple<T, P, TL, false, false>(v, t, vp, vstride, pt.cons, pt.g, cc);
+        }
+      } else {
 #pragma unroll
-      for (int m = 0; m < P; m++) {
-        const int p = t + TL * m;
-        const int i = (a.axis == 0) ? p : i0, j = (a.axis == 1) ? p : j0, k = (a.axis == 2) ? p : k0;
-        v[m] = pot_factor_apply<T>(v[m], i, j, k, vbase + (unsigned) p * vstride, a);
+        for (int m = 0; m < P; m++) {
+          const int p = t + TL * m;
+          const int i = (a.axis == 0) ? p : i0, j = (a.axis == 1) ? p : j0, k = (a.axis == 2) ? p : k0;
+          v[m] = pot_factor_apply<T>(v[m], i, j, k, vbase + (unsigned) p * vstride, a);
+        }
       }
     } else if constexpr (Op == OP_KSQ) {
       // sum |k|^2 |v|^2 with k from the unshifted frequency grid
@@ -348,8 +405,8 @@ template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N,
       decode(a, o, 0, q, i, j, k);
       const int ax = a.axis;
       const int b0 = (ax == 0) ? 1 : 0, b1 = (ax == 2) ? 1 : 2;
-      const int idx[3] = {i, j, k};
-      const double k2line = a.ksq[b0][idx[b0]] + a.ksq[b1][idx[b1]];
+      const int ix0 = (ax == 0) ? j : i, ix1 = (ax == 2) ? j : k;
+      const double k2line = a.ksq[b0][ix0] + a.ksq[b1][ix1];
 #pragma unroll
       for (int m = 0; m < P; m++) {
         const int p = t + TL * m;
@@ -406,9 +463,9 @@ __global__ void __launch_bounds__(ContigCfg<N>::THREADS, 2)
   T2 v[P];
 #pragma unroll
   for (int m = 0; m < P; m++) v[m] = ok ? s[t + TL * m] : T2{(T) 0, (T) 0};
-  SmContig<T2, Cfg::SH> sm{smem + l * Cfg::LINE};
+  SmContig<T2, Cfg::SH, TL> sm{smem + l * Cfg::LINE};
   double acc = 0.0;
-  Program<T, N, SmContig<T2, Cfg::SH>, Ops...>::run(v, t, sm, a, ok ? line : 0u, 0u, acc);
+  Program<T, N, SmContig<T2, Cfg::SH, TL>, Ops...>::run(v, t, sm, a, ok ? line : 0u, 0u, acc);
   if constexpr (has_ksq(OpL<Ops...>{})) {
     __shared__ double sbuf[(Cfg::THREADS + 31) / 32];
     double r = block_sum<Cfg::THREADS>(ok ? acc : 0.0, sbuf);

@@ -142,6 +142,29 @@ def test_gp_step_fft(b200, restate, shape, time):
     b200.free(vx)
 
 
+def test_long_run_gp_parity_and_norm(b200, restate):
+    """1000 FP64 GP steps: psi within 1e-11 relative L2 of the oracle and the
+    norm conserved to 1e-12 (real time)."""
+    shape, step, g = (32, 32, 32), 0.5, 0.0025
+    mass = 4.0 / workloads.GRID_AUTOAMU
+    psi0, v = workloads.gp_wells(shape, step, g, seed=13)
+    w = b200.wf(*shape, step, mass, PER, FFT2, values=psi0)
+    vx = b200.rgrid(*shape, step, values=v)
+    n0 = w.norm()
+    for _ in range(1000):
+        w.propagate_gp(vx, g, 1.0)
+    got = w.grid.get()
+    n1 = w.norm()
+    want = psi0.copy()
+    vr = workloads.padded(v)
+    for _ in range(1000):
+        want = restate.fft_step(want, step, mass, 1.0, vr=vr, g=g)
+    assert rel(got, want) < TOL_PSI
+    assert abs(n1 - n0) / n0 < 1e-12
+    b200.free(w)
+    b200.free(vx)
+
+
 def test_fp32_mode_error_bound(b200, restate):
     shape, step, g = (32, 32, 32), 0.5, 0.0025
     mass = 4.0 / workloads.GRID_AUTOAMU
@@ -420,3 +443,21 @@ def test_mixed_ops_vs_reference(b200, ref):
     assert rel(res[0][0], res[1][0]) < 1e-15
     assert rel(res[0][1], res[1][1]) < 1e-15
     assert abs(res[0][2] - res[1][2]) <= 1e-12 * abs(res[1][2])
+
+
+def test_phase_sincos_against_cuda(b200):
+    """The propagation kernels' FP64 phase sine/cosine (Cody-Waite reduction
+    + Taylor polynomials, library routine beyond 1e7) against the CUDA
+    library sincos."""
+    import ctypes as C
+
+    rng = np.random.default_rng(5)
+    x = np.concatenate([rng.uniform(-1e-3, 1e-3, 4000), rng.uniform(-4, 4, 4000), rng.uniform(-1e4, 1e4, 4000),
+                        rng.uniform(-1e7, 1e7, 2000), rng.uniform(-1e9, 1e9, 500),
+                        np.array([0.0, -0.0, np.pi / 4, -np.pi / 4, np.pi / 2, np.pi, 3e6 * np.pi])])
+    err = (C.c_double * 2)()
+    b200.lib.gb_sincos_selftest.argtypes = [C.c_void_p, C.c_long, C.POINTER(C.c_double)]
+    assert b200.lib.gb_sincos_selftest(x.ctypes.data, len(x), err) == 0
+    # a few ulp of 1 (arguments up to 1e7 keep the reduced argument accurate
+    # to ~1e-16)
+    assert err[0] < 1e-15 and err[1] < 1e-15, (err[0], err[1])
