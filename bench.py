@@ -45,6 +45,7 @@ if ROOT not in sys.path:
 
 METRIC = "GP 256^3 split-operator steps/s (FP64, resident in HBM)"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dram_traffic.json")
 FALLBACK_HBM = 6650.0
 BYTES_PER_POINT_STEP = 264
 BYTES_PER_POINT_PASS = 32
@@ -55,6 +56,16 @@ for _ax, _an in enumerate("xyz"):
         KIND_NAMES[5 * _ax + _p] = "%s_%s" % (_an, _pn)
     KIND_NAMES[15 + _ax] = "cn_%s" % _an
 NUM_KINDS = 18
+
+
+def measured_traffic(kind, n):
+    """DRAM bytes (read + write) per launch of a pass kind at n^3, from the
+    committed ncu capture summary (profiles/dram_traffic.json), or None."""
+    try:
+        with open(TRAFFIC_FILE) as f:
+            return float(json.load(f)["%s@%d" % (kind, n)]["dram_bytes"])
+    except Exception:
+        return None
 
 
 def hbm_peak():
@@ -324,7 +335,9 @@ def run_b200(args, world, rank, local):
     # dominant kernel = largest total time among pass kinds
     dom = max(per_kind.items(), key=lambda kv: kv[1]["ms_total"])
     dom_ms = dom[1]["ms_total"] / dom[1]["launches"]
-    dom_bytes = BYTES_PER_POINT_PASS * N
+    # the potential pass also reads the real V_ext row (8 B/pt in FP64)
+    dom_bytes = (BYTES_PER_POINT_PASS + (8 if dom[0].endswith("inv_pot_fwd") else 0)) * N
+    traffic = measured_traffic(dom[0], n)
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     step_gbs = BYTES_PER_POINT_STEP * N / (step_ms * 1e-3) / 1e9
     h2d = (N * 16 + n * n * 2 * (n // 2 + 1) * 8) / args.steps
@@ -369,7 +382,7 @@ def run_b200(args, world, rank, local):
             "unit": "GB/s",
             "frac": achieved / peak,
             "peak_source": peak_kind,
-            "traffic": None,
+            "traffic": traffic,
             "algorithmic_bytes_per_launch": dom_bytes,
             "mean_launch_ms": dom_ms,
         },
