@@ -79,3 +79,37 @@ def cn_wells(shape=(192, 192, 192), step=0.3, g=0.001, seed=3):
         sh[ax] = n
         win = win * s.reshape(sh)
     return (psi * win).astype(np.complex128), v
+
+
+def run_gp_steps(n: int = 256, steps: int = 3, prec: int = 0) -> float:
+    """Propagate the GP workload at n^3 for `steps` steps through the C API on
+    the current GPU and return the final norm (a small driver for profilers:
+    ``python -m libgrid_b200.workloads gp 256 3``)."""
+    import libgrid_b200 as gb
+    from libgrid_b200 import capi
+
+    api = gb.load()
+    api.lib.cuda_enable(b"\x01", 0, None)
+    shape, step, g = (n, n, n), 0.5, 0.0025
+    mass = 4.0 / GRID_AUTOAMU
+    psi0, v = gp_wells(shape, step, g, seed=2)
+    w = api.wf(*shape, step, mass, capi.WF_PERIODIC_BOUNDARY, capi.WF_2ND_ORDER_FFT, values=psi0)
+    if prec:
+        w.precision(prec)
+    vx = api.rgrid(*shape, step, values=v)
+    for _ in range(steps):
+        w.propagate_gp(vx, g, 1.0)
+    api.lib.gb_synchronize()
+    nrm = w.norm()
+    api.free(w)
+    api.free(vx)
+    return nrm
+
+
+if __name__ == "__main__":
+    import sys
+
+    if len(sys.argv) < 2 or sys.argv[1] != "gp":
+        sys.exit("usage: python -m libgrid_b200.workloads gp [n] [steps] [prec: 0 FP64, 1 FP32]")
+    a = [int(x) for x in sys.argv[2:]]
+    print("norm", run_gp_steps(*a))
