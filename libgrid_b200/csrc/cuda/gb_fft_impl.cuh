@@ -223,6 +223,8 @@ struct PassArgs {
   double scale;         // OP_SCALE
   gb_potential pot;
   double *partial;      // OP_KSQ: one partial sum per block
+  const void *vstage;   // this thread's prefetched V values in shared memory (element m at m * vstage_stride)
+  int vstage_stride;
 };
 
 // Decode (i, j, k) of axis position p for a line given by (o, q).  Grids
@@ -288,13 +290,12 @@ __device__ __forceinline__ C2<T> pot_factor_apply(C2<T> x, long i, long j, long 
 // Im c = 0 (imaginary time: a decay), and only sincos or exp is needed.
 // Same values as pot_factor_apply for these cases.
 template <typename T, int P, int TL, bool HAS_V, bool PHASE>
-__device__ __forceinline__ void pot_line_simple(C2<T> (&v)[P], int t, const T *vp, unsigned vs, double cons,
-                                                double g, double cc) {
+__device__ __forceinline__ void pot_line_simple(C2<T> (&v)[P], int t, const T *vp, unsigned vt, unsigned vm,
+                                                double cons, double g, double cc) {
 #pragma unroll
   for (int m = 0; m < P; m++) {
-    const int p = t + TL * m;
     double w = cons;
-    if constexpr (HAS_V) w += (double) vp[(unsigned) p * vs];
+    if constexpr (HAS_V) w += (double) vp[(unsigned) t * vt + (unsigned) m * vm];
     const double xr = (double) v[m].x, xi = (double) v[m].y;
     w = fma(g, fma(xr, xr, xi * xi), w);
     const double arg = cc * w;
@@ -306,6 +307,49 @@ __device__ __forceinline__ void pot_line_simple(C2<T> (&v)[P], int t, const T *v
     }
   }
 }
+
+// Start of a line's potential row and its stride along the pass axis
+// (potential arrays use the row length pot.vrow, e.g. the rgrid nz2).
+__device__ __forceinline__ void pot_row(const PassArgs &a, unsigned o, unsigned q, int &i0, int &j0, int &k0,
+                                        unsigned &vbase, unsigned &vstride) {
+  decode(a, o, 0, q, i0, j0, k0);
+  const unsigned vrow = (unsigned) a.pot.vrow, ny = (unsigned) a.ny;
+  if (a.axis == 2) {
+    vbase = ((unsigned) i0 * ny + (unsigned) j0) * vrow;
+    vstride = 1u;
+  } else if (a.axis == 1) {
+    vbase = (unsigned) i0 * ny * vrow + (unsigned) k0;
+    vstride = vrow;
+  } else {
+    vbase = (unsigned) j0 * vrow + (unsigned) k0;
+    vstride = ny * vrow;
+  }
+}
+
+__device__ __forceinline__ bool pot_is_simple(const gb_potential &pt) {
+  return !pt.absorb && pt.kind != GB_POT_COMPLEX && (pt.c_re == 0.0 || pt.c_im == 0.0);
+}
+
+// Issue asynchronous copies (cp.async) of the real potential values this
+// thread will need in the potential op into its own shared-memory slots
+// stage[m * stride], m < P, so the load latency overlaps the tile load and
+// the first transform.  Returns false (nothing issued) when the potential
+// op will not read a real V through the simple path.
+template <typename T, int P, int TL>
+__device__ __forceinline__ bool pot_prefetch(const PassArgs &a, unsigned o, unsigned q, int t, T *stage,
+                                             int stride) {
+  if (a.pot.kind != GB_POT_REAL || !pot_is_simple(a.pot)) return false;
+  int i0, j0, k0;
+  unsigned vbase, vstride;
+  pot_row(a, o, q, i0, j0, k0, vbase, vstride);
+  const T *g = (const T *) a.pot.v + vbase;
+#pragma unroll
+  for (int m = 0; m < P; m++) cp_async_elem<sizeof(T)>(stage + m * stride, g + (unsigned) (t + TL * m) * vstride);
+  cp_async_commit();
+  return true;
+}
+
+template <int... Ops> __host__ __device__ constexpr bool has_pot(OpL<Ops...>) { return ((Ops == OP_POT) || ...); }
 
 template <int Op, int... Rest> struct OpsHead {
   static constexpr int value = Op;
@@ -366,30 +410,29 @@ template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N,
       // decode the line once; along the pass axis the potential index
       // advances by a fixed stride
       int i0, j0, k0;
-      decode(a, o, 0, q, i0, j0, k0);
-      const unsigned vrow = (unsigned) a.pot.vrow, ny = (unsigned) a.ny;
       unsigned vbase, vstride;
-      if (a.axis == 2) {
-        vbase = ((unsigned) i0 * ny + (unsigned) j0) * vrow;
-        vstride = 1u;
-      } else if (a.axis == 1) {
-        vbase = (unsigned) i0 * ny * vrow + (unsigned) k0;
-        vstride = vrow;
-      } else {
-        vbase = (unsigned) j0 * vrow + (unsigned) k0;
-        vstride = ny * vrow;
-      }
+      pot_row(a, o, q, i0, j0, k0, vbase, vstride);
       const gb_potential &pt = a.pot;
-      if (!pt.absorb && pt.kind != GB_POT_COMPLEX && (pt.c_re == 0.0 || pt.c_im == 0.0)) {
+      if (pot_is_simple(pt)) {
         const bool phase = (pt.c_re == 0.0);
         const double cc = phase ? pt.c_im : pt.c_re;
+        // V from this thread's prefetched slots when the kernel staged it,
+        // else from the grid: element m of the thread sits at position
+        // t + TL m of the line
         const T *vp = (const T *) pt.v + vbase;
+        unsigned vt = vstride, vm = TL * vstride;
+        if (a.vstage) {
+          cp_async_wait_all();
+          vp = (const T *) a.vstage;
+          vt = 0;
+          vm = (unsigned) a.vstage_stride;
+        }
         if (pt.kind == GB_POT_REAL) {
-          if (phase) pot_line_simple<T, P, TL, true, true>(v, t, vp, vstride, pt.cons, pt.g, cc);
-          else pot_line_simple<T, P, TL, true, false>(v, t, vp, vstride, pt.cons, pt.g, cc);
+          if (phase) pot_line_simple<T, P, TL, true, true>(v, t, vp, vt, vm, pt.cons, pt.g, cc);
+          else pot_line_simple<T, P, TL, true, false>(v, t, vp, vt, vm, pt.cons, pt.g, cc);
         } else {
-          if (phase) pot_line_simple<T, P, TL, false, true>(v, t, vp, vstride, pt.cons, pt.g, cc);
-          else pot_line_simple<T, P, TL, false, false>(v, t, vp, vstride, pt.cons, pt.g, cc);
+          if (phase) pot_line_simple<T, P, TL, false, true>(v, t, vp, vt, vm, pt.cons, pt.g, cc);
+          else pot_line_simple<T, P, TL, false, false>(v, t, vp, vt, vm, pt.cons, pt.g, cc);
         }
       } else {
 #pragma unroll
@@ -460,12 +503,21 @@ __global__ void __launch_bounds__(ContigCfg<N>::THREADS, 2)
   const unsigned line = blockIdx.x * (unsigned) Cfg::L + (unsigned) l;
   const bool ok = line < (unsigned long) nlines;
   const T2 *s = src + (size_t) line * N;
+  PassArgs la = a;
+  if constexpr (has_pot(OpL<Ops...>{})) {
+    // potential values staged behind the exchange buffer
+    T *stage = (T *) (smraw + (size_t) Cfg::L * Cfg::LINE * sizeof(T2)) + threadIdx.x;
+    if (pot_prefetch<T, P, TL>(a, ok ? line : 0u, 0u, t, stage, Cfg::THREADS)) {
+      la.vstage = stage;
+      la.vstage_stride = Cfg::THREADS;
+    }
+  }
   T2 v[P];
 #pragma unroll
   for (int m = 0; m < P; m++) v[m] = ok ? s[t + TL * m] : T2{(T) 0, (T) 0};
   SmContig<T2, Cfg::SH, TL> sm{smem + l * Cfg::LINE};
   double acc = 0.0;
-  Program<T, N, SmContig<T2, Cfg::SH, TL>, Ops...>::run(v, t, sm, a, ok ? line : 0u, 0u, acc);
+  Program<T, N, SmContig<T2, Cfg::SH, TL>, Ops...>::run(v, t, sm, la, ok ? line : 0u, 0u, acc);
   if constexpr (has_ksq(OpL<Ops...>{})) {
     __shared__ double sbuf[(Cfg::THREADS + 31) / 32];
     double r = block_sum<Cfg::THREADS>(ok ? acc : 0.0, sbuf);
@@ -504,12 +556,20 @@ __global__ void __launch_bounds__((N / Sched<N>::P) * BZ, 2)
   // grid has fewer than 2^31 points, so the in-tile offsets fit 32 bits
   const size_t off = (size_t) o * (size_t) N * (size_t) inner + q;
   const T2 *s = src + off;
+  PassArgs la = a;
+  if constexpr (has_pot(OpL<Ops...>{})) {
+    T *stage = (T *) (smraw + (size_t) N * BZ * sizeof(T2)) + threadIdx.x;
+    if (pot_prefetch<T, P, TL>(a, o, q, t, stage, THREADS)) {
+      la.vstage = stage;
+      la.vstage_stride = THREADS;
+    }
+  }
   T2 v[P];
 #pragma unroll
   for (int m = 0; m < P; m++) v[m] = s[(unsigned) (t + TL * m) * in32];
   SmStrided<T2, BZ> sm{smem + c};
   double acc = 0.0;
-  Program<T, N, SmStrided<T2, BZ>, Ops...>::run(v, t, sm, a, o, q, acc);
+  Program<T, N, SmStrided<T2, BZ>, Ops...>::run(v, t, sm, la, o, q, acc);
   if constexpr (has_ksq(OpL<Ops...>{})) {
     __shared__ double sbuf[(THREADS + 31) / 32];
     double r = block_sum<THREADS>(acc, sbuf);
@@ -525,10 +585,12 @@ __global__ void __launch_bounds__((N / Sched<N>::P) * BZ, 2)
 template <typename T, int N, int... Ops>
 int launch_pass_n(const void *src, void *dst, const PassArgs &a, long outer, long inner, long *nblocks) {
   using T2 = C2<T>;
+  // per-thread staging of the potential values (P reals per thread)
+  constexpr size_t STAGE = has_pot(OpL<Ops...>{}) ? (size_t) Sched<N>::P * sizeof(T) : 0;
   cudaStream_t st = gb__stream();
   if (inner == 1) {
     using Cfg = ContigCfg<N>;
-    const size_t sm = (size_t) Cfg::L * Cfg::LINE * sizeof(T2);
+    const size_t sm = (size_t) Cfg::L * Cfg::LINE * sizeof(T2) + STAGE * Cfg::THREADS;
     auto kern = k_pass_contig<T, N, Ops...>;
     static bool attr_set = false;
     if (!attr_set) {
@@ -541,7 +603,7 @@ int launch_pass_n(const void *src, void *dst, const PassArgs &a, long outer, lon
   } else {
     constexpr int BZ = StridedCfg<N>::BZ;
     if (inner % BZ == 0 && outer <= 65535) {
-      const size_t sm = (size_t) N * BZ * sizeof(T2);
+      const size_t sm = (size_t) N * BZ * sizeof(T2) + STAGE * (N / Sched<N>::P) * BZ;
       auto kern = k_pass_strided<T, N, BZ, Ops...>;
       static bool attr_set = false;
       if (!attr_set) {
@@ -552,7 +614,7 @@ int launch_pass_n(const void *src, void *dst, const PassArgs &a, long outer, lon
       if (nblocks) *nblocks = (long) grid.x * grid.y;
       kern<<<grid, (N / Sched<N>::P) * BZ, sm, st>>>((const T2 *) src, (T2 *) dst, inner, a);
     } else if (outer <= 65535) {
-      const size_t sm = (size_t) N * sizeof(T2);
+      const size_t sm = (size_t) N * sizeof(T2) + STAGE * (N / Sched<N>::P);
       auto kern = k_pass_strided<T, N, 1, Ops...>;
       static bool attr_set = false;
       if (!attr_set) {
