@@ -172,7 +172,28 @@ __device__ __forceinline__ void fft_stage(T2 (&v)[P], int t, const SM &sm, const
     T2 w[R];
 #pragma unroll
     for (int r = 0; r < R; r++) w[r] = v[u + r * B];
-    if constexpr (!FIRST) {
+    if constexpr (!FIRST && R == 16) {
+      // w^(k r) with r = 4a + b is w^(4 k a) w^(k b): six table values
+      // (b, a = 1..3) instead of fifteen keep the register footprint of the
+      // stage small; each product is applied as two multiplications
+      constexpr int STRIDE = N / (NS * R);
+      T2 tb[4], ta[4];
+#pragma unroll
+      for (int e = 1; e < 4; e++) {
+        tb[e] = tw[k * e * STRIDE];
+        ta[e] = tw[k * 4 * e * STRIDE];
+        if constexpr (S > 0) {
+          tb[e].y = -tb[e].y;
+          ta[e].y = -ta[e].y;
+        }
+      }
+#pragma unroll
+      for (int r = 1; r < R; r++) {
+        const int a4 = r >> 2, b4 = r & 3;
+        if (b4) w[r] = cmul(w[r], tb[b4]);
+        if (a4) w[r] = cmul(w[r], ta[a4]);
+      }
+    } else if constexpr (!FIRST) {
       constexpr int STRIDE = N / (NS * R);
 #pragma unroll
       for (int r = 1; r < R; r++) {

@@ -123,7 +123,8 @@ def test_split_step_cfft_cutoff(b200, restate):
     assert rel(got, want) < TOL_PSI
 
 
-@pytest.mark.parametrize("shape,time", [((32, 32, 32), 1.0), ((16, 32, 64), -1.0j), ((1, 64, 64), 0.5)])
+@pytest.mark.parametrize("shape,time", [((32, 32, 32), 1.0), ((16, 32, 64), -1.0j), ((1, 64, 64), 0.5),
+                                        ((32, 64, 256), 1.0), ((256, 16, 32), -1.0j)])
 def test_gp_step_fft(b200, restate, shape, time):
     step, g = 0.5, 0.0025
     mass = 4.0 / workloads.GRID_AUTOAMU
