@@ -512,7 +512,7 @@ template <int N> struct ContigCfg {
 
 // Contiguous lines (inner == 1): L lines of N per block.
 template <typename T, int N, int... Ops>
-__global__ void __launch_bounds__(ContigCfg<N>::THREADS, 2)
+__global__ void __launch_bounds__(ContigCfg<N>::THREADS,  sizeof(T) == 8 ? 2 : 3)
     k_pass_contig(const C2<T> *__restrict__ src, C2<T> *__restrict__ dst, long nlines, PassArgs a) {
   using T2 = C2<T>;
   using Cfg = ContigCfg<N>;
@@ -561,7 +561,7 @@ template <int N> struct StridedCfg {
 
 // Strided lines: block = (column block of BZ adjacent inner indices, outer).
 template <typename T, int N, int BZ, int... Ops>
-__global__ void __launch_bounds__((N / Sched<N>::P) * BZ, 2)
+__global__ void __launch_bounds__((N / Sched<N>::P) * BZ,  sizeof(T) == 8 ? 2 : 3)
     k_pass_strided(const C2<T> *__restrict__ src, C2<T> *__restrict__ dst, long inner, PassArgs a) {
   using T2 = C2<T>;
   constexpr int P = Sched<N>::P, TL = N / P;
