@@ -58,7 +58,7 @@ template <typename T> __device__ __forceinline__ C2<T> to_c2(double re, double i
 // significant bits of pi/2 each (so n P1 and n P2 are exact for |n| < 2^23)
 // and P3 the rounded remainder, split here from the decimal expansion of pi.
 // On |r| <= pi/4 the Taylor series of sin and cos are cut after r^17/17! and
-// r^16/16! (truncation below 1e-17) and evaluated by Horner in r^2.  The
+// r^16/16! (truncation below 1e-17) and evaluated in r^2 by Estrin's scheme.  The
 // quadrant q = n mod 4 is applied without branches: q odd swaps sin and
 // cos, bit 1 of q (of q + 1 for the cosine) flips the sign.
 // The library fallback stays out of line, so the unrolled per-element loops
@@ -80,23 +80,24 @@ __device__ __forceinline__ double2 gb_sincos_reduced(double x) {
   double r = fma(-n, 1.570796325802803, x);
   r = fma(-n, 9.920935791635221e-10, r);
   r = fma(-n, 5.170182981794105e-19, r);
+  // both series in s2 = r^2, evaluated by Estrin's scheme (pairs of terms,
+  // then powers s2^2 and s2^4 shared by sine and cosine) for a short
+  // dependency chain
   const double s2 = r * r;
-  double ps = 2.8114572543455206e-15;
-  ps = fma(ps, s2, -7.647163731819816e-13);
-  ps = fma(ps, s2, 1.6059043836821613e-10);
-  ps = fma(ps, s2, -2.505210838544172e-08);
-  ps = fma(ps, s2, 2.7557319223985893e-06);
-  ps = fma(ps, s2, -0.0001984126984126984);
-  ps = fma(ps, s2, 0.008333333333333333);
-  ps = fma(ps, s2, -0.16666666666666666);
-  double pc = 4.779477332387385e-14;
-  pc = fma(pc, s2, -1.1470745597729725e-11);
-  pc = fma(pc, s2, 2.08767569878681e-09);
-  pc = fma(pc, s2, -2.755731922398589e-07);
-  pc = fma(pc, s2, 2.48015873015873e-05);
-  pc = fma(pc, s2, -0.001388888888888889);
-  pc = fma(pc, s2, 0.041666666666666664);
-  pc = fma(pc, s2, -0.5);
+  const double s4 = s2 * s2;
+  const double s8 = s4 * s4;
+  // sin: r + r s2 (-1/3! + s2/5! - s2^2/7! + ... + s2^7/17!)
+  const double a01 = fma(0.008333333333333333, s2, -0.16666666666666666);
+  const double a23 = fma(2.7557319223985893e-06, s2, -0.0001984126984126984);
+  const double a45 = fma(1.6059043836821613e-10, s2, -2.505210838544172e-08);
+  const double a67 = fma(2.8114572543455206e-15, s2, -7.647163731819816e-13);
+  const double ps = fma(fma(a67, s4, a45), s8, fma(a23, s4, a01));
+  // cos: 1 + s2 (-1/2! + s2/4! - ... + s2^7/16!)
+  const double b01 = fma(0.041666666666666664, s2, -0.5);
+  const double b23 = fma(2.48015873015873e-05, s2, -0.001388888888888889);
+  const double b45 = fma(2.08767569878681e-09, s2, -2.755731922398589e-07);
+  const double b67 = fma(4.779477332387385e-14, s2, -1.1470745597729725e-11);
+  const double pc = fma(fma(b67, s4, b45), s8, fma(b23, s4, b01));
   const double sr = fma(r * s2, ps, r);
   const double cr = fma(s2, pc, 1.0);
   const bool swap = (q & 1) != 0;
