@@ -153,7 +153,7 @@ template <typename T> int gb__ksq_sum_t(const void *psi, void *work, const gb_ge
     src = work;
   }
   const View v = axis_view(g, ax[na - 1]);
-  const long nb = blocks_for(v.n, v.outer, v.inner);
+  const long nb = blocks_for<(int) sizeof(T)>(v.n, v.outer, v.inner);
   double *partial = (double *) gb__scratch(GB_SCR_PARTIAL, sizeof(double) * (size_t) nb);
   if (!partial) return gb_last_error();
   a.partial = partial;

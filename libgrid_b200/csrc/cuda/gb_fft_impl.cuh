@@ -501,21 +501,32 @@ template <int THREADS> __device__ __forceinline__ double block_sum(double v, dou
 
 // ---------------------------------------------------------------- kernels
 
-template <int N> struct ContigCfg {
+// CTA shapes, by line length and element size ES = sizeof(real).  Small
+// CTAs (128 threads; four resident per SM in FP64) let the load, transform
+// and store phases of neighbouring CTAs interleave; FP32 strided passes keep
+// 16 columns (256 threads) so each row segment stays 128 bytes.
+// Resident CTAs per SM are bounded below by MINB (the register cap: 128
+// per thread in FP64, 85 in FP32).
+template <int THREADS, int ES> constexpr int pass_min_blocks() {
+  return (ES == 8 ? 512 : 768) / THREADS > 0 ? (ES == 8 ? 512 : 768) / THREADS : 1;
+}
+
+template <int N, int ES = 8> struct ContigCfg {
   static constexpr int P = Sched<N>::P;
   static constexpr int TL = N / P;
-  static constexpr int L = (256 / TL) > 0 ? (256 / TL) : 1;
+  static constexpr int L = (128 / TL) > 0 ? (128 / TL) : 1;
   static constexpr int THREADS = TL * L;
   static constexpr int SH = ilog2c(first_radix(typename Sched<N>::R{}));
   static constexpr int LINE = N + (N >> SH);
+  static constexpr int MINB = pass_min_blocks<THREADS, ES>();
 };
 
 // Contiguous lines (inner == 1): L lines of N per block.
 template <typename T, int N, int... Ops>
-__global__ void __launch_bounds__(ContigCfg<N>::THREADS,  sizeof(T) == 8 ? 2 : 3)
+__global__ void __launch_bounds__(ContigCfg<N, sizeof(T)>::THREADS, ContigCfg<N, sizeof(T)>::MINB)
     k_pass_contig(const C2<T> *__restrict__ src, C2<T> *__restrict__ dst, long nlines, PassArgs a) {
   using T2 = C2<T>;
-  using Cfg = ContigCfg<N>;
+  using Cfg = ContigCfg<N, sizeof(T)>;
   constexpr int P = Cfg::P, TL = Cfg::TL;
   extern __shared__ __align__(16) unsigned char smraw[];
   T2 *smem = (T2 *) smraw;
@@ -552,16 +563,16 @@ __global__ void __launch_bounds__(ContigCfg<N>::THREADS,  sizeof(T) == 8 ? 2 : 3
   }
 }
 
-template <int N> struct StridedCfg {
+template <int N, int ES = 8> struct StridedCfg {
   static constexpr int P = Sched<N>::P;
   static constexpr int TL = N / P;
-  static constexpr int BZ = (N <= 256) ? 16 : ((N <= 512) ? 8 : 4);
+  static constexpr int BZ = ES == 8 ? ((N <= 512) ? 8 : 4) : ((N <= 256) ? 16 : ((N <= 512) ? 8 : 4));
   static constexpr int THREADS = TL * BZ;
 };
 
 // Strided lines: block = (column block of BZ adjacent inner indices, outer).
 template <typename T, int N, int BZ, int... Ops>
-__global__ void __launch_bounds__((N / Sched<N>::P) * BZ,  sizeof(T) == 8 ? 2 : 3)
+__global__ void __launch_bounds__((N / Sched<N>::P) * BZ, pass_min_blocks<(N / Sched<N>::P) * BZ, sizeof(T)>())
     k_pass_strided(const C2<T> *__restrict__ src, C2<T> *__restrict__ dst, long inner, PassArgs a) {
   using T2 = C2<T>;
   constexpr int P = Sched<N>::P, TL = N / P;
@@ -610,7 +621,7 @@ int launch_pass_n(const void *src, void *dst, const PassArgs &a, long outer, lon
   constexpr size_t STAGE = has_pot(OpL<Ops...>{}) ? (size_t) Sched<N>::P * sizeof(T) : 0;
   cudaStream_t st = gb__stream();
   if (inner == 1) {
-    using Cfg = ContigCfg<N>;
+    using Cfg = ContigCfg<N, sizeof(T)>;
     const size_t sm = (size_t) Cfg::L * Cfg::LINE * sizeof(T2) + STAGE * Cfg::THREADS;
     auto kern = k_pass_contig<T, N, Ops...>;
     static bool attr_set = false;
@@ -622,7 +633,7 @@ int launch_pass_n(const void *src, void *dst, const PassArgs &a, long outer, lon
     if (nblocks) *nblocks = nb;
     kern<<<(unsigned) nb, Cfg::THREADS, sm, st>>>((const T2 *) src, (T2 *) dst, outer, a);
   } else {
-    constexpr int BZ = StridedCfg<N>::BZ;
+    constexpr int BZ = StridedCfg<N, sizeof(T)>::BZ;
     if (inner % BZ == 0 && outer <= 65535) {
       const size_t sm = (size_t) N * BZ * sizeof(T2) + STAGE * (N / Sched<N>::P) * BZ;
       auto kern = k_pass_strided<T, N, BZ, Ops...>;
@@ -654,9 +665,9 @@ int launch_pass_n(const void *src, void *dst, const PassArgs &a, long outer, lon
 }
 
 // Number of blocks a pass will launch (for sizing OP_KSQ partials).
-template <int N> long pass_blocks(long outer, long inner) {
-  if (inner == 1) return (outer + ContigCfg<N>::L - 1) / ContigCfg<N>::L;
-  constexpr int BZ = StridedCfg<N>::BZ;
+template <int N, int ES> long pass_blocks(long outer, long inner) {
+  if (inner == 1) return (outer + ContigCfg<N, ES>::L - 1) / ContigCfg<N, ES>::L;
+  constexpr int BZ = StridedCfg<N, ES>::BZ;
   if (inner % BZ == 0) return (inner / BZ) * outer;
   return inner * outer;
 }
@@ -680,20 +691,20 @@ int launch_pass(long n, const void *src, void *dst, const PassArgs &a, long oute
   }
 }
 
-inline long blocks_for(long n, long outer, long inner) {
+template <int ES> long blocks_for(long n, long outer, long inner) {
   switch (n) {
-    case 2: return pass_blocks<2>(outer, inner);
-    case 4: return pass_blocks<4>(outer, inner);
-    case 8: return pass_blocks<8>(outer, inner);
-    case 16: return pass_blocks<16>(outer, inner);
-    case 32: return pass_blocks<32>(outer, inner);
-    case 64: return pass_blocks<64>(outer, inner);
-    case 128: return pass_blocks<128>(outer, inner);
-    case 256: return pass_blocks<256>(outer, inner);
-    case 512: return pass_blocks<512>(outer, inner);
-    case 1024: return pass_blocks<1024>(outer, inner);
-    case 2048: return pass_blocks<2048>(outer, inner);
-    case 4096: return pass_blocks<4096>(outer, inner);
+    case 2: return pass_blocks<2, ES>(outer, inner);
+    case 4: return pass_blocks<4, ES>(outer, inner);
+    case 8: return pass_blocks<8, ES>(outer, inner);
+    case 16: return pass_blocks<16, ES>(outer, inner);
+    case 32: return pass_blocks<32, ES>(outer, inner);
+    case 64: return pass_blocks<64, ES>(outer, inner);
+    case 128: return pass_blocks<128, ES>(outer, inner);
+    case 256: return pass_blocks<256, ES>(outer, inner);
+    case 512: return pass_blocks<512, ES>(outer, inner);
+    case 1024: return pass_blocks<1024, ES>(outer, inner);
+    case 2048: return pass_blocks<2048, ES>(outer, inner);
+    case 4096: return pass_blocks<4096, ES>(outer, inner);
     default: return 0;
   }
 }
