@@ -73,13 +73,8 @@ __device__ __forceinline__ double gb_flip_sign(double v, int bit2) {
   return __hiloint2double(__double2hiint(v) ^ (bit2 << 30), __double2loint(v));
 }
 
-// (sin x, cos x) for |x| <= 1e7.
-__device__ __forceinline__ double2 gb_sincos_reduced(double x) {
-  const double n = rint(x * 0.6366197723675814);
-  const int q = __double2int_rn(n);
-  double r = fma(-n, 1.570796325802803, x);
-  r = fma(-n, 9.920935791635221e-10, r);
-  r = fma(-n, 5.170182981794105e-19, r);
+// (sin r, cos r) for |r| <= pi/4 by the two series below.
+__device__ __forceinline__ double2 gb_sincos_series(double r) {
   // both series in s2 = r^2, evaluated by Estrin's scheme (pairs of terms,
   // then powers s2^2 and s2^4 shared by sine and cosine) for a short
   // dependency chain
@@ -98,16 +93,28 @@ __device__ __forceinline__ double2 gb_sincos_reduced(double x) {
   const double b45 = fma(2.08767569878681e-09, s2, -2.755731922398589e-07);
   const double b67 = fma(4.779477332387385e-14, s2, -1.1470745597729725e-11);
   const double pc = fma(fma(b67, s4, b45), s8, fma(b23, s4, b01));
-  const double sr = fma(r * s2, ps, r);
-  const double cr = fma(s2, pc, 1.0);
+  return double2{fma(r * s2, ps, r), fma(s2, pc, 1.0)};
+}
+
+// (sin x, cos x) for |x| <= 1e7.
+__device__ __forceinline__ double2 gb_sincos_reduced(double x) {
+  const double n = rint(x * 0.6366197723675814);
+  const int q = __double2int_rn(n);
+  double r = fma(-n, 1.570796325802803, x);
+  r = fma(-n, 9.920935791635221e-10, r);
+  r = fma(-n, 5.170182981794105e-19, r);
+  const double2 sc = gb_sincos_series(r);
   const bool swap = (q & 1) != 0;
-  const double s = swap ? cr : sr;
-  const double c = swap ? sr : cr;
+  const double s = swap ? sc.y : sc.x;
+  const double c = swap ? sc.x : sc.y;
   return double2{gb_flip_sign(s, q & 2), gb_flip_sign(c, (q + 1) & 2)};
 }
 
-// (sin x, cos x) for any x.
+// (sin x, cos x) for any x.  Below pi/4 (n = 0: r = x exactly, quadrant 0)
+// the series apply directly, with the same result as the reduced path; this
+// is the usual case for split-operator phases dt (V + g |psi|^2).
 __device__ __forceinline__ double2 gb_sincos2(double x) {
+  if (fabs(x) < 0.78539816339744828) return gb_sincos_series(x);
   if (!(fabs(x) <= 1.0e7)) return gb_sincos_lib(x);
   return gb_sincos_reduced(x);
 }
