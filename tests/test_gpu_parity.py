@@ -453,7 +453,7 @@ def test_phase_sincos_against_cuda(b200):
     import ctypes as C
 
     rng = np.random.default_rng(5)
-    x = np.concatenate([rng.uniform(-1e-3, 1e-3, 4000), rng.uniform(-4, 4, 4000), rng.uniform(-1e4, 1e4, 4000),
+    x = np.concatenate([rng.uniform(-1e-3, 1e-3, 4000), rng.uniform(-0.07, 0.07, 4000), rng.uniform(-4, 4, 4000), rng.uniform(-1e4, 1e4, 4000),
                         rng.uniform(-1e7, 1e7, 2000), rng.uniform(-1e9, 1e9, 500),
                         np.array([0.0, -0.0, np.pi / 4, -np.pi / 4, np.pi / 2, np.pi, 3e6 * np.pi])])
     err = (C.c_double * 2)()
