@@ -249,6 +249,35 @@ typedef struct {
 } gb_cn_params;
 int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, const gb_potential *pre, const gb_potential *post);
 
+/* ------------------------------------------------------------- batches */
+/*
+ * Many independent 2-D wave functions of uneven sizes advanced together by
+ * the second-order FFT split-operator step (the step gb_split_step makes for
+ * one grid), all instances in one persistent launch per call.  No reference
+ * counterpart: the reference steps one grid per grid_wf_propagate call.
+ * An instance is psi (device, complex, geometry g with g.nx == 1 and
+ * g.ny, g.nz in {64, 128, 256, 512}; one precision for the whole batch), its
+ * K(dt/2) factor and its V(dt) step with the meanings of gb_split_step; a
+ * potential of kind GB_POT_NONE with g == 0 and cons == 0 leaves the
+ * potential step out.  The batch keeps the device pointers: the grids must
+ * stay allocated while it exists.
+ */
+typedef struct {
+  void *psi;
+  gb_geom g;
+  gb_kinetic kin;
+  gb_potential pot;
+} gb_batch_item;
+typedef struct gb_batch gb_batch;
+gb_batch *gb_batch_create(const gb_batch_item *items, int n);
+/* `steps` steps of every instance, asynchronous on the library stream. */
+int gb_batch_step(gb_batch *b, int steps);
+/* CTA size the autotuner chose (0 before the first call of >= 5 steps). */
+int gb_batch_threads(const gb_batch *b);
+/* Status of the launch's bounded grid barrier (0 = no wait gave up). */
+int gb_batch_error_flag(gb_batch *b, int reset);
+void gb_batch_free(gb_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -331,6 +331,25 @@ void grid_wf_propagate_gp(wf *gwf, rgrid *vext, REAL g, REAL complex time);
 void grid_wf_precision(wf *gwf, char mode);
 char grid_wf_get_precision(wf *gwf);
 
+/*
+ * Batched propagation (no reference counterpart; the reference advances one
+ * wave function per grid_wf_propagate call).  grid_wf_batch_alloc groups n
+ * 2-D wave functions (nx == 1; ny, nz in {64, 128, 256, 512}; periodic
+ * boundaries, WF_2ND_ORDER_FFT; one device precision for all) with their
+ * complex potentials (an entry may be NULL: no potential step) and one time
+ * step; grid_wf_batch_propagate then makes `steps` steps of every wave
+ * function, the same step grid_wf_propagate(wfs[i], potentials[i], time)
+ * makes, all in one persistent GPU launch.  The wave functions and
+ * potentials must stay allocated while the batch exists; host-side changes
+ * to them are picked up on the next propagate call.
+ */
+typedef struct grid_wf_batch grid_wf_batch;
+grid_wf_batch *grid_wf_batch_alloc(wf **wfs, cgrid **potentials, INT n, REAL complex time);
+void grid_wf_batch_propagate(grid_wf_batch *b, INT steps);
+void grid_wf_batch_free(grid_wf_batch *b);
+/* CTA size the batch autotuner chose (0 until a call of >= 5 steps). */
+int grid_wf_batch_threads(grid_wf_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -130,11 +130,33 @@ class Api:
             w.grid.set(values)
         return w
 
+    def batch(self, wfs, potentials, time) -> "Batch":
+        """grid_wf_batch_alloc over WaveFunction objects and complex potential
+        Grids (entries may be None)."""
+        n = len(wfs)
+        PW, PC = C.POINTER(self.WF), C.POINTER(self.CGrid)
+        warr = (PW * n)(*[w.ptr for w in wfs])
+        parr = (PC * n)(*[(p.ptr if p is not None else PC()) for p in potentials]) if potentials else None
+        b = self.lib.grid_wf_batch_alloc(warr, parr, n, capi.Complex.of(time))
+        if not b:
+            raise RuntimeError("grid_wf_batch_alloc failed")
+        return Batch(self, b)
+
     def free(self, obj) -> None:
         if isinstance(obj, WaveFunction):
             self.lib.grid_wf_free(obj.ptr)
         elif isinstance(obj, Grid):
             (self.lib.rgrid_free if obj.real else self.lib.cgrid_free)(obj.ptr)
+        elif isinstance(obj, Batch):
+            self.lib.grid_wf_batch_free(obj.ptr)
+
+
+class Batch:
+    def __init__(self, api: Api, ptr):
+        self.api, self.ptr = api, ptr
+
+    def propagate(self, steps: int) -> None:
+        self.api.lib.grid_wf_batch_propagate(self.ptr, steps)
 
 
 class WaveFunction:

@@ -216,6 +216,10 @@ def bind(lib: C.CDLL, cuda_layout: bool, extensions: bool):
         f("grid_wf_propagate_gp", None, PW, PR, D, Cx)
         f("grid_wf_precision", None, PW, ch)
         f("grid_wf_get_precision", ch, PW)
+        f("grid_wf_batch_alloc", V, C.POINTER(PW), C.POINTER(PC), L, Cx)
+        f("grid_wf_batch_propagate", None, V, L)
+        f("grid_wf_batch_free", None, V)
+        f("grid_wf_batch_threads", C.c_int, V)
         f("gb_grid_sync_host", None, V)
         f("gb_grid_host_modified", None, V)
         f("gb_last_error", C.c_int)

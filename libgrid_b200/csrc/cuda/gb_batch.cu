@@ -1,0 +1,437 @@
+// Batched split-operator propagation of many independent 2-D wave functions
+// of uneven sizes (sm_100a).
+//
+// All instances advance through the same five line passes of a 2-D
+// second-order split-operator step (z: contiguous lines, y: strided lines):
+//   z FWD | y FWD.K.INV | z INV.V.FWD | y FWD.K.INV | z INV
+// One cooperative, persistent launch runs K steps: in every pass the CTAs
+// walk a flat list of tiles that spans all instances (a tile is a group of
+// z lines, or a block of y columns, of one instance; the line length of the
+// tile's instance selects the compiled transform), and a grid-wide barrier
+// separates the passes.  The barrier is this file's own (atomic arrival
+// counter + generation word) with a bounded wait: a CTA that waits too long
+// sets the batch's error flag and leaves, so the launch always ends.
+// A small autotuner picks the CTA size (128 or 256 threads) per batch by
+// timing both on the first steps of the first call; both sizes compute the
+// same values.
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "gb_fft_impl.cuh"
+#include "gb_internal_cuda.h"
+
+namespace gbfft {
+
+struct BatchInst {
+  PassArgs az;  // z (contiguous) passes
+  PassArgs ay;  // y (strided) passes
+  void *psi;
+  int nz, ny;
+};
+
+struct BatchTile {
+  int inst;
+  int tile;
+};
+
+struct BatchDev {
+  const BatchInst *inst;
+  const BatchTile *ctiles;
+  const BatchTile *stiles;
+  int nct, nst;
+  unsigned *bar;  // [0] arrivals, [1] generation
+  int *err;
+};
+
+#define GB_GRID_WAIT_LIMIT (1u << 24)
+
+// Grid-wide barrier of a cooperative launch (all CTAs resident).  Returns
+// false on every thread of a CTA whose wait gave up (error flag set).
+__device__ __forceinline__ bool batch_grid_barrier(unsigned *bar, int *err) {
+  __syncthreads();
+  int ok = 1;
+  if (threadIdx.x == 0) {
+    volatile unsigned *gen = bar + 1;
+    const unsigned g0 = *gen;
+    __threadfence();
+    if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      unsigned it = 0;
+      while (*gen == g0) {
+        if (++it > GB_GRID_WAIT_LIMIT) {
+          atomicExch(err, 1);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+  }
+  return !__syncthreads_or(!ok);
+}
+
+// One tile of contiguous (z) lines: L = THREADS / TL lines of length N.
+template <typename T, int N, int THREADS, int... Ops>
+__device__ __forceinline__ void batch_tile_contig(const BatchInst &I, int tile, unsigned char *smraw) {
+  using T2 = C2<T>;
+  using Cfg = ContigCfg<N, sizeof(T)>;
+  constexpr int P = Cfg::P, TL = Cfg::TL, L = THREADS / TL;
+  static_assert(THREADS % TL == 0, "CTA size must hold whole lines");
+  T2 *smem = (T2 *) smraw;
+  const int t = threadIdx.x % TL;
+  const int l = threadIdx.x / TL;
+  const unsigned line = (unsigned) tile * L + (unsigned) l;
+  T2 *psi = (T2 *) I.psi;
+  const T2 *s = psi + (size_t) line * N;
+  const PassArgs &a = I.az;
+  const T *vstage = nullptr;
+  if constexpr (has_pot(OpL<Ops...>{})) {
+    T *stage = (T *) (smraw + (size_t) L * Cfg::LINE * sizeof(T2)) + threadIdx.x;
+    if (pot_prefetch<T, P, TL>(a, line, 0u, t, stage, THREADS)) vstage = stage;
+  }
+  T2 v[P];
+#pragma unroll
+  for (int m = 0; m < P; m++) v[m] = s[t + TL * m];
+  SmContig<T2, Cfg::SH, TL> sm{smem + l * Cfg::LINE};
+  double acc = 0.0;
+  Program<T, N, SmContig<T2, Cfg::SH, TL>, Ops...>::run(v, t, sm, a, line, 0u, acc, vstage, THREADS);
+  T2 *d = psi + (size_t) line * N;
+#pragma unroll
+  for (int m = 0; m < P; m++) d[t + TL * m] = v[m];
+}
+
+// One tile of strided (y) lines of a 2-D instance (outer = 1): BZ = THREADS
+// / TL adjacent columns, each a line of length N with stride inner = nz.
+template <typename T, int N, int THREADS, int... Ops>
+__device__ __forceinline__ void batch_tile_strided(const BatchInst &I, int tile, unsigned char *smraw) {
+  using T2 = C2<T>;
+  constexpr int P = Sched<N>::P, TL = N / P, BZ = THREADS / TL;
+  static_assert(THREADS % TL == 0, "CTA size must hold whole lines");
+  T2 *smem = (T2 *) smraw;
+  const int c = threadIdx.x % BZ;
+  const int t = threadIdx.x / BZ;
+  const unsigned q = (unsigned) tile * BZ + (unsigned) c;
+  const unsigned in32 = (unsigned) I.nz;
+  T2 *psi = (T2 *) I.psi;
+  const T2 *s = psi + q;
+  const PassArgs &a = I.ay;
+  const T *vstage = nullptr;
+  if constexpr (has_pot(OpL<Ops...>{})) {
+    T *stage = (T *) (smraw + (size_t) N * BZ * sizeof(T2)) + threadIdx.x;
+    if (pot_prefetch<T, P, TL>(a, 0u, q, t, stage, THREADS)) vstage = stage;
+  }
+  T2 v[P];
+#pragma unroll
+  for (int m = 0; m < P; m++) v[m] = s[(unsigned) (t + TL * m) * in32];
+  SmStrided<T2, BZ> sm{smem + c};
+  double acc = 0.0;
+  Program<T, N, SmStrided<T2, BZ>, Ops...>::run(v, t, sm, a, 0u, q, acc, vstage, THREADS);
+  T2 *d = psi + q;
+#pragma unroll
+  for (int m = 0; m < P; m++) d[(unsigned) (t + TL * m) * in32] = v[m];
+}
+
+// Line lengths a batch takes on either axis.
+template <typename T, int THREADS, int... Ops>
+__device__ __forceinline__ void batch_contig(const BatchInst &I, int tile, unsigned char *sm) {
+  switch (I.nz) {
+    case 64: batch_tile_contig<T, 64, THREADS, Ops...>(I, tile, sm); break;
+    case 128: batch_tile_contig<T, 128, THREADS, Ops...>(I, tile, sm); break;
+    case 256: batch_tile_contig<T, 256, THREADS, Ops...>(I, tile, sm); break;
+    default: batch_tile_contig<T, 512, THREADS, Ops...>(I, tile, sm); break;
+  }
+}
+template <typename T, int THREADS, int... Ops>
+__device__ __forceinline__ void batch_strided(const BatchInst &I, int tile, unsigned char *sm) {
+  switch (I.ny) {
+    case 64: batch_tile_strided<T, 64, THREADS, Ops...>(I, tile, sm); break;
+    case 128: batch_tile_strided<T, 128, THREADS, Ops...>(I, tile, sm); break;
+    case 256: batch_tile_strided<T, 256, THREADS, Ops...>(I, tile, sm); break;
+    default: batch_tile_strided<T, 512, THREADS, Ops...>(I, tile, sm); break;
+  }
+}
+
+// `steps` full steps of every instance; one pass = one sweep of the pass's
+// tile list by all CTAs, then a grid barrier.
+template <typename T, int THREADS>
+__global__ void __launch_bounds__(THREADS, pass_min_blocks<THREADS, sizeof(T)>())
+    k_batch_steps(BatchDev d, int steps) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  for (int s = 0; s < steps; s++) {
+#pragma unroll 1
+    for (int ps = 0; ps < 5; ps++) {
+      if ((ps & 1) == 0) {
+        for (int k = blockIdx.x; k < d.nct; k += gridDim.x) {
+          const BatchTile bt = d.ctiles[k];
+          const BatchInst &I = d.inst[bt.inst];
+          if (ps == 0) batch_contig<T, THREADS, OP_FWD>(I, bt.tile, smraw);
+          else if (ps == 2) batch_contig<T, THREADS, OP_INV, OP_POT, OP_FWD>(I, bt.tile, smraw);
+          else batch_contig<T, THREADS, OP_INV>(I, bt.tile, smraw);
+        }
+      } else {
+        for (int k = blockIdx.x; k < d.nst; k += gridDim.x) {
+          const BatchTile bt = d.stiles[k];
+          batch_strided<T, THREADS, OP_FWD, OP_KIN, OP_INV>(d.inst[bt.inst], bt.tile, smraw);
+        }
+      }
+      if (!batch_grid_barrier(d.bar, d.err)) return;
+    }
+  }
+}
+
+// Dynamic shared memory of a CTA of THREADS threads: the largest exchange
+// buffer over the line lengths plus the per-thread potential slots.
+template <typename T, int THREADS> constexpr size_t batch_smem() {
+  using T2 = C2<T>;
+  size_t m = 0;
+  const int ns[4] = {64, 128, 256, 512};
+  const int ps[4] = {Sched<64>::P, Sched<128>::P, Sched<256>::P, Sched<512>::P};
+  const int lines[4] = {ContigCfg<64>::LINE, ContigCfg<128>::LINE, ContigCfg<256>::LINE, ContigCfg<512>::LINE};
+  for (int i = 0; i < 4; i++) {
+    const int tl = ns[i] / ps[i];
+    const size_t c = (size_t) (THREADS / tl) * lines[i] * sizeof(T2);
+    const size_t st = (size_t) ns[i] * (THREADS / tl) * sizeof(T2);
+    const size_t a = (c > st ? c : st) + (size_t) THREADS * ps[i] * sizeof(T);
+    if (a > m) m = a;
+  }
+  return m;
+}
+
+}  // namespace gbfft
+
+// ------------------------------------------------------------------ host
+
+using namespace gbfft;
+
+struct gb_batch {
+  int n, prec;
+  BatchInst *d_inst;
+  BatchTile *d_tiles[2][2];  // [variant 128 / 256][contiguous / strided]
+  int ntiles[2][2];
+  unsigned char *d_kin;
+  unsigned *d_bar;
+  int *d_err;
+  int grid[2];
+  int threads;  // chosen CTA size, 0 until tuned
+};
+
+static bool batch_len_ok(long v) { return v == 64 || v == 128 || v == 256 || v == 512; }
+
+// Threads per line (N / P) of each line length.
+static long batch_tl(long n) {
+  switch (n) {
+    case 64: return 64 / Sched<64>::P;
+    case 128: return 128 / Sched<128>::P;
+    case 256: return 256 / Sched<256>::P;
+    default: return 512 / Sched<512>::P;
+  }
+}
+
+template <typename T, int THREADS> static int batch_grid() {
+  auto k = k_batch_steps<T, THREADS>;
+  constexpr size_t sm = batch_smem<T, THREADS>();
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
+  int dev = 0, nsm = 0, per = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k, THREADS, sm);
+  return nsm * per;
+}
+
+template <typename T, int THREADS> static int batch_launch(gb_batch *b, int steps, int v) {
+  BatchDev d;
+  d.inst = b->d_inst;
+  d.ctiles = b->d_tiles[v][0];
+  d.stiles = b->d_tiles[v][1];
+  d.nct = b->ntiles[v][0];
+  d.nst = b->ntiles[v][1];
+  d.bar = b->d_bar;
+  d.err = b->d_err;
+  void *args[] = {&d, &steps};
+  constexpr size_t sm = batch_smem<T, THREADS>();
+  const cudaError_t e = cudaLaunchCooperativeKernel((const void *) k_batch_steps<T, THREADS>, dim3(b->grid[v]),
+                                                    dim3(THREADS), args, sm, gb__stream());
+  gb__count_launch();
+  if (e != cudaSuccess) return gb__set_error((int) e, "batch launch");
+  return 0;
+}
+
+static int batch_run(gb_batch *b, int steps, int v) {
+  if (steps <= 0) return 0;
+  if (b->prec == GB_FP32) return v ? batch_launch<float, 256>(b, steps, 1) : batch_launch<float, 128>(b, steps, 0);
+  return v ? batch_launch<double, 256>(b, steps, 1) : batch_launch<double, 128>(b, steps, 0);
+}
+
+// Kinetic tables of one geometry into caller-owned buffers (gb_fft.cu).
+int gb__kin_tables_at(void *fac, double *ksq, const gb_geom *g, const gb_kinetic *kin);
+
+extern "C" gb_batch *gb_batch_create(const gb_batch_item *items, int n) {
+  if (n <= 0 || !items) {
+    gb__set_error(1040, "batch: no instances");
+    return nullptr;
+  }
+  const int prec = items[0].g.prec;
+  for (int i = 0; i < n; i++) {
+    const gb_geom &g = items[i].g;
+    if (g.nx != 1 || !batch_len_ok(g.ny) || !batch_len_ok(g.nz) || g.prec != prec || !items[i].psi) {
+      gb__set_error(1041, "batch: instances must be 2-D (1, ny, nz) with ny, nz in {64, 128, 256, 512} and one precision");
+      return nullptr;
+    }
+  }
+  const size_t esz = prec == GB_FP32 ? 8 : 16;
+  gb_batch *b = (gb_batch *) calloc(1, sizeof(gb_batch));
+  b->n = n;
+  b->prec = prec;
+  // kinetic tables: per instance (1 + ny + nz) factors and k^2 values
+  std::vector<size_t> koff(n);
+  size_t kbytes = 0;
+  for (int i = 0; i < n; i++) {
+    koff[i] = kbytes;
+    const size_t tot = 1 + (size_t) items[i].g.ny + (size_t) items[i].g.nz;
+    kbytes += (tot * (esz + 8) + 255) & ~(size_t) 255;
+  }
+  if (cudaMalloc(&b->d_kin, kbytes) != cudaSuccess || cudaMalloc(&b->d_inst, sizeof(BatchInst) * n) != cudaSuccess ||
+      cudaMalloc(&b->d_bar, 2 * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&b->d_err, sizeof(int)) != cudaSuccess) {
+    cudaGetLastError();
+    gb__set_error(2, "batch: cudaMalloc");
+    gb_batch_free(b);
+    return nullptr;
+  }
+  cudaStream_t st = gb__stream();
+  cudaMemsetAsync(b->d_bar, 0, 2 * sizeof(unsigned), st);
+  cudaMemsetAsync(b->d_err, 0, sizeof(int), st);
+  std::vector<BatchInst> hi(n);
+  for (int i = 0; i < n; i++) {
+    const gb_batch_item &it = items[i];
+    const long tot = 1 + it.g.ny + it.g.nz;
+    unsigned char *fac = b->d_kin + koff[i];
+    double *ksq = (double *) (fac + (size_t) tot * esz);
+    if (gb__kin_tables_at(fac, ksq, &it.g, &it.kin)) {
+      gb_batch_free(b);
+      return nullptr;
+    }
+    PassArgs a;
+    memset(&a, 0, sizeof(a));
+    a.nx = 1;
+    a.ny = it.g.ny;
+    a.nz = it.g.nz;
+    a.scale = 1.0;
+    a.kscale = it.kin.scale;
+    a.cutoff = it.kin.cutoff;
+    a.kmax2 = it.kin.kmax2;
+    a.kfac[0] = fac;
+    a.kfac[1] = fac + esz;
+    a.kfac[2] = fac + esz * (size_t) (1 + it.g.ny);
+    a.ksq[0] = ksq;
+    a.ksq[1] = ksq + 1;
+    a.ksq[2] = ksq + 1 + it.g.ny;
+    a.pot = it.pot;
+    if (a.pot.kind == GB_POT_NONE && a.pot.g == 0.0 && a.pot.cons == 0.0) a.pot.c_re = a.pot.c_im = 0.0;
+    BatchInst &bi = hi[i];
+    bi.az = a;
+    bi.az.axis = 2;
+    bi.az.tw = gb__twiddles(it.g.nz, prec);
+    bi.ay = a;
+    bi.ay.axis = 1;
+    bi.ay.tw = gb__twiddles(it.g.ny, prec);
+    if (!bi.az.tw || !bi.ay.tw) {
+      gb_batch_free(b);
+      return nullptr;
+    }
+    bi.psi = it.psi;
+    bi.nz = (int) it.g.nz;
+    bi.ny = (int) it.g.ny;
+  }
+  cudaMemcpyAsync(b->d_inst, hi.data(), sizeof(BatchInst) * n, cudaMemcpyHostToDevice, st);
+  // tile lists for the two CTA sizes
+  const int threads[2] = {128, 256};
+  for (int v = 0; v < 2; v++) {
+    std::vector<BatchTile> ct, stl;
+    for (int i = 0; i < n; i++) {
+      const long nz = items[i].g.nz, ny = items[i].g.ny;
+      const long tlz = batch_tl(nz), tly = batch_tl(ny);
+      const long lz = threads[v] / tlz, bzy = threads[v] / tly;
+      for (long k = 0; k < ny / lz; k++) ct.push_back(BatchTile{i, (int) k});
+      for (long k = 0; k < nz / bzy; k++) stl.push_back(BatchTile{i, (int) k});
+    }
+    b->ntiles[v][0] = (int) ct.size();
+    b->ntiles[v][1] = (int) stl.size();
+    if (cudaMalloc(&b->d_tiles[v][0], sizeof(BatchTile) * ct.size()) != cudaSuccess ||
+        cudaMalloc(&b->d_tiles[v][1], sizeof(BatchTile) * stl.size()) != cudaSuccess) {
+      cudaGetLastError();
+      gb__set_error(2, "batch: cudaMalloc");
+      gb_batch_free(b);
+      return nullptr;
+    }
+    cudaMemcpy(b->d_tiles[v][0], ct.data(), sizeof(BatchTile) * ct.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(b->d_tiles[v][1], stl.data(), sizeof(BatchTile) * stl.size(), cudaMemcpyHostToDevice);
+  }
+  b->grid[0] = prec == GB_FP32 ? batch_grid<float, 128>() : batch_grid<double, 128>();
+  b->grid[1] = prec == GB_FP32 ? batch_grid<float, 256>() : batch_grid<double, 256>();
+  if (b->grid[0] <= 0 || b->grid[1] <= 0) {
+    gb__set_error(1042, "batch: kernel cannot be resident");
+    gb_batch_free(b);
+    return nullptr;
+  }
+  return b;
+}
+
+// Steps of every instance.  The first call with at least five steps times one
+// step with each CTA size (after one warm-up step each) and keeps the faster;
+// those four steps count as steps of the run.
+extern "C" int gb_batch_step(gb_batch *b, int steps) {
+  if (!b) return gb__set_error(1040, "batch: null");
+  if (steps <= 0) return 0;
+  if (!b->threads) {
+    if (steps < 5) return batch_run(b, steps, b->prec == GB_FP32 ? 1 : 0);
+    cudaEvent_t e[4];
+    for (int i = 0; i < 4; i++) cudaEventCreate(&e[i]);
+    cudaStream_t st = gb__stream();
+    GB_TRYC(batch_run(b, 1, 0));
+    cudaEventRecord(e[0], st);
+    GB_TRYC(batch_run(b, 1, 0));
+    cudaEventRecord(e[1], st);
+    GB_TRYC(batch_run(b, 1, 1));
+    cudaEventRecord(e[2], st);
+    GB_TRYC(batch_run(b, 1, 1));
+    cudaEventRecord(e[3], st);
+    cudaEventSynchronize(e[3]);
+    float t128 = 0.f, t256 = 0.f;
+    cudaEventElapsedTime(&t128, e[0], e[1]);
+    cudaEventElapsedTime(&t256, e[2], e[3]);
+    for (int i = 0; i < 4; i++) cudaEventDestroy(e[i]);
+    b->threads = (t256 < t128) ? 256 : 128;
+    steps -= 4;
+  }
+  return batch_run(b, steps, b->threads == 256 ? 1 : 0);
+}
+
+extern "C" int gb_batch_threads(const gb_batch *b) { return b ? b->threads : 0; }
+
+extern "C" int gb_batch_error_flag(gb_batch *b, int reset) {
+  if (!b || !b->d_err) return 0;
+  int h = 0;
+  cudaStreamSynchronize(gb__stream());
+  cudaMemcpy(&h, b->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (reset) cudaMemset(b->d_err, 0, sizeof(int));
+  return h;
+}
+
+extern "C" void gb_batch_free(gb_batch *b) {
+  if (!b) return;
+  cudaStreamSynchronize(gb__stream());
+  cudaFree(b->d_inst);
+  for (int v = 0; v < 2; v++)
+    for (int k = 0; k < 2; k++) cudaFree(b->d_tiles[v][k]);
+  cudaFree(b->d_kin);
+  cudaFree(b->d_bar);
+  cudaFree(b->d_err);
+  free(b);
+}

@@ -101,6 +101,24 @@ int gb__kin_tables(const gb_geom *g, const gb_kinetic *kin, int unshifted, GbKin
   return 0;
 }
 
+// The same tables for one geometry into caller-owned buffers: fac holds
+// nx + ny + nz factors in the storage precision, ksq as many k^2 values.
+int gb__kin_tables_at(void *fac, double *ksq, const gb_geom *g, const gb_kinetic *kin) {
+  const long tot = g->nx + g->ny + g->nz;
+  const double lx = 2.0 * M_PI / (g->step * (double) g->nx);
+  const double ly = 2.0 * M_PI / (g->step * (double) g->ny);
+  const double lz = 2.0 * M_PI / (g->step * (double) g->nz);
+  const unsigned nb = (unsigned) ((tot + 255) / 256);
+  if (g->prec == GB_FP32)
+    k_kin_tables<float><<<nb, 256, 0, gb__stream()>>>((float2 *) fac, ksq, g->nx, g->ny, g->nz, lx, ly, lz, kin->kx0,
+                                                       kin->ky0, kin->kz0, kin->tm_re, kin->tm_im);
+  else
+    k_kin_tables<double><<<nb, 256, 0, gb__stream()>>>((double2 *) fac, ksq, g->nx, g->ny, g->nz, lx, ly, lz,
+                                                        kin->kx0, kin->ky0, kin->kz0, kin->tm_re, kin->tm_im);
+  GB_CHECK_LAUNCH("kinetic tables");
+  return 0;
+}
+
 // ------------------------------------------------------ partial-sum finisher
 
 __global__ void k_sum_partials(const double *__restrict__ p, long n, double *out) {

@@ -244,8 +244,6 @@ struct PassArgs {
   double scale;         // OP_SCALE
   gb_potential pot;
   double *partial;      // OP_KSQ: one partial sum per block
-  const void *vstage;   // this thread's prefetched V values in shared memory (element m at m * vstage_stride)
-  int vstage_stride;
 };
 
 // Decode (i, j, k) of axis position p for a line given by (o, q).  Grids
@@ -382,12 +380,14 @@ template <typename T, int N, class SM, int... Ops> struct Program;
 template <typename T, int N, class SM> struct Program<T, N, SM> {
   // o, q identify the line; thread holds positions t + TL*m
   static __device__ __forceinline__ void run(C2<T> (&)[Sched<N>::P], int, const SM &, const PassArgs &, unsigned,
-                                             unsigned, double &) {}
+                                             unsigned, double &, const void *, int) {}
 };
 
 template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N, SM, Op, Rest...> {
+  // vstage: this thread's prefetched potential values in shared memory
+  // (element m at vstage[m * vstride]), or null to read the potential grid
   static __device__ __forceinline__ void run(C2<T> (&v)[Sched<N>::P], int t, const SM &sm, const PassArgs &a, unsigned o,
-                                             unsigned q, double &acc) {
+                                             unsigned q, double &acc, const void *vstage = nullptr, int vstride = 0) {
     using T2 = C2<T>;
     constexpr int P = Sched<N>::P;
     constexpr int TL = N / P;
@@ -442,11 +442,11 @@ template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N,
         // t + TL m of the line
         const T *vp = (const T *) pt.v + vbase;
         unsigned vt = vstride, vm = TL * vstride;
-        if (a.vstage) {
+        if (vstage) {
           cp_async_wait_all();
-          vp = (const T *) a.vstage;
+          vp = (const T *) vstage;
           vt = 0;
-          vm = (unsigned) a.vstage_stride;
+          vm = (unsigned) vstride;
         }
         if (pt.kind == GB_POT_REAL) {
           if (phase) pot_line_simple<T, P, TL, true, true>(v, t, vp, vt, vm, pt.cons, pt.g, cc);
@@ -477,7 +477,7 @@ template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N,
         acc += (k2line + a.ksq[ax][p]) * ((double) v[m].x * (double) v[m].x + (double) v[m].y * (double) v[m].y);
       }
     }
-    Program<T, N, SM, Rest...>::run(v, t, sm, a, o, q, acc);
+    Program<T, N, SM, Rest...>::run(v, t, sm, a, o, q, acc, vstage, vstride);
   }
 };
 
@@ -535,21 +535,19 @@ __global__ void __launch_bounds__(ContigCfg<N, sizeof(T)>::THREADS, ContigCfg<N,
   const unsigned line = blockIdx.x * (unsigned) Cfg::L + (unsigned) l;
   const bool ok = line < (unsigned long) nlines;
   const T2 *s = src + (size_t) line * N;
-  PassArgs la = a;
+  const T *vstage = nullptr;
   if constexpr (has_pot(OpL<Ops...>{})) {
     // potential values staged behind the exchange buffer
     T *stage = (T *) (smraw + (size_t) Cfg::L * Cfg::LINE * sizeof(T2)) + threadIdx.x;
-    if (pot_prefetch<T, P, TL>(a, ok ? line : 0u, 0u, t, stage, Cfg::THREADS)) {
-      la.vstage = stage;
-      la.vstage_stride = Cfg::THREADS;
-    }
+    if (pot_prefetch<T, P, TL>(a, ok ? line : 0u, 0u, t, stage, Cfg::THREADS)) vstage = stage;
   }
   T2 v[P];
 #pragma unroll
   for (int m = 0; m < P; m++) v[m] = ok ? s[t + TL * m] : T2{(T) 0, (T) 0};
   SmContig<T2, Cfg::SH, TL> sm{smem + l * Cfg::LINE};
   double acc = 0.0;
-  Program<T, N, SmContig<T2, Cfg::SH, TL>, Ops...>::run(v, t, sm, la, ok ? line : 0u, 0u, acc);
+  Program<T, N, SmContig<T2, Cfg::SH, TL>, Ops...>::run(v, t, sm, a, ok ? line : 0u, 0u, acc, vstage,
+                                                        Cfg::THREADS);
   if constexpr (has_ksq(OpL<Ops...>{})) {
     __shared__ double sbuf[(Cfg::THREADS + 31) / 32];
     double r = block_sum<Cfg::THREADS>(ok ? acc : 0.0, sbuf);
@@ -588,20 +586,17 @@ __global__ void __launch_bounds__((N / Sched<N>::P) * BZ, pass_min_blocks<(N / S
   // grid has fewer than 2^31 points, so the in-tile offsets fit 32 bits
   const size_t off = (size_t) o * (size_t) N * (size_t) inner + q;
   const T2 *s = src + off;
-  PassArgs la = a;
+  const T *vstage = nullptr;
   if constexpr (has_pot(OpL<Ops...>{})) {
     T *stage = (T *) (smraw + (size_t) N * BZ * sizeof(T2)) + threadIdx.x;
-    if (pot_prefetch<T, P, TL>(a, o, q, t, stage, THREADS)) {
-      la.vstage = stage;
-      la.vstage_stride = THREADS;
-    }
+    if (pot_prefetch<T, P, TL>(a, o, q, t, stage, THREADS)) vstage = stage;
   }
   T2 v[P];
 #pragma unroll
   for (int m = 0; m < P; m++) v[m] = s[(unsigned) (t + TL * m) * in32];
   SmStrided<T2, BZ> sm{smem + c};
   double acc = 0.0;
-  Program<T, N, SmStrided<T2, BZ>, Ops...>::run(v, t, sm, la, o, q, acc);
+  Program<T, N, SmStrided<T2, BZ>, Ops...>::run(v, t, sm, a, o, q, acc, vstage, THREADS);
   if constexpr (has_ksq(OpL<Ops...>{})) {
     __shared__ double sbuf[(THREADS + 31) / 32];
     double r = block_sum<THREADS>(acc, sbuf);

@@ -651,3 +651,110 @@ char grid_wf_get_precision(wf *gwf) { return (char) (psi_prec(gwf) == GB_FP32 ? 
 
 /* npts is kept for symmetry with the other translation units */
 size_t gb__wf_points(const wf *gwf) { return npts(gwf->grid); }
+
+/* ------------------------------------------------------------ batches */
+
+struct grid_wf_batch {
+  INT n;
+  wf **wfs;
+  cgrid **pots;
+  REAL complex time;
+  gb_batch *b;
+  void **psi; /* device pointers the batch was built for */
+  const void **vdev;
+};
+
+/* One instance of a batch: the step fused_fft_step makes for gwf. */
+static void batch_item(gb_batch_item *it, wf *gwf, cgrid *cpot, REAL complex time, void **psi, const void **vdev) {
+  cgrid *grid = gwf->grid;
+  const int p = psi_prec(gwf);
+  memset(it, 0, sizeof(*it));
+  it->g = wf_geom(gwf);
+  REAL complex half = 0.5 * time;
+  REAL complex tm = -I * half * HBAR / (gwf->mass * 2.0);
+  it->kin.tm_re = creal(tm);
+  it->kin.tm_im = cimag(tm);
+  it->kin.kx0 = grid->kx0;
+  it->kin.ky0 = grid->ky0;
+  it->kin.kz0 = grid->kz0;
+  it->kin.scale = grid->fft_norm;
+  it->kin.kmax2 = gwf->kmax * gwf->kmax;
+  it->kin.cutoff = 0;
+  *vdev = NULL;
+  if (cpot) {
+    REAL complex c = -I * time / HBAR;
+    it->pot.c_re = creal(c);
+    it->pot.c_im = cimag(c);
+    it->pot.cons = frame_cons(gwf);
+    it->pot.kind = GB_POT_COMPLEX;
+    *vdev = gbh_dev_read(cpot->value, p);
+    it->pot.v = *vdev;
+    it->pot.vrow = cpot->nz;
+  }
+  *psi = gbh_dev_rw(grid->value, p);
+  it->psi = *psi;
+}
+
+static gb_batch *batch_build(grid_wf_batch *bb) {
+  gb_batch_item *items = (gb_batch_item *) malloc(sizeof(gb_batch_item) * (size_t) bb->n);
+  for (INT i = 0; i < bb->n; i++)
+    batch_item(&items[i], bb->wfs[i], bb->pots ? bb->pots[i] : NULL, bb->time, &bb->psi[i], &bb->vdev[i]);
+  gb_batch *b = gb_batch_create(items, (int) bb->n);
+  free(items);
+  return b;
+}
+
+grid_wf_batch *grid_wf_batch_alloc(wf **wfs, cgrid **potentials, INT n, REAL complex time) {
+  if (n <= 0 || !wfs) gbh_die("grid_wf_batch_alloc(): no wave functions");
+  const int p = psi_prec(wfs[0]);
+  for (INT i = 0; i < n; i++) {
+    wf *w = wfs[i];
+    if (w->propagator != WF_2ND_ORDER_FFT || w->boundary != WF_PERIODIC_BOUNDARY)
+      gbh_die("grid_wf_batch_alloc(): wave functions must use WF_2ND_ORDER_FFT with periodic boundaries");
+    if (w->ts_func) gbh_die("grid_wf_batch_alloc(): absorbing boundaries are not batched");
+    if (psi_prec(w) != p) gbh_die("grid_wf_batch_alloc(): all wave functions must have one precision");
+  }
+  grid_wf_batch *bb = (grid_wf_batch *) calloc(1, sizeof(grid_wf_batch));
+  bb->n = n;
+  bb->time = time;
+  bb->wfs = (wf **) malloc(sizeof(wf *) * (size_t) n);
+  memcpy(bb->wfs, wfs, sizeof(wf *) * (size_t) n);
+  if (potentials) {
+    bb->pots = (cgrid **) malloc(sizeof(cgrid *) * (size_t) n);
+    memcpy(bb->pots, potentials, sizeof(cgrid *) * (size_t) n);
+  }
+  bb->psi = (void **) calloc((size_t) n, sizeof(void *));
+  bb->vdev = (const void **) calloc((size_t) n, sizeof(void *));
+  bb->b = batch_build(bb);
+  if (!bb->b) gbh_check(gb_last_error() ? gb_last_error() : -1, "grid_wf_batch_alloc");
+  return bb;
+}
+
+void grid_wf_batch_propagate(grid_wf_batch *bb, INT steps) {
+  /* bring device copies up to date (host-side changes) and rebuild the
+   * batch if any device buffer moved */
+  int moved = 0;
+  for (INT i = 0; i < bb->n; i++) {
+    const int p = psi_prec(bb->wfs[i]);
+    if (gbh_dev_rw(bb->wfs[i]->grid->value, p) != bb->psi[i]) moved = 1;
+    if (bb->pots && bb->pots[i] && gbh_dev_read(bb->pots[i]->value, p) != bb->vdev[i]) moved = 1;
+  }
+  if (moved) {
+    gb_batch_free(bb->b);
+    bb->b = batch_build(bb);
+    if (!bb->b) gbh_check(gb_last_error() ? gb_last_error() : -1, "grid_wf_batch_propagate");
+  }
+  gbh_check(gb_batch_step(bb->b, (int) steps), "grid_wf_batch_propagate");
+}
+
+int grid_wf_batch_threads(grid_wf_batch *bb) { return bb ? gb_batch_threads(bb->b) : 0; }
+
+void grid_wf_batch_free(grid_wf_batch *bb) {
+  if (!bb) return;
+  gb_batch_free(bb->b);
+  free(bb->wfs);
+  free(bb->pots);
+  free(bb->psi);
+  free(bb->vdev);
+  free(bb);
+}

@@ -81,6 +81,32 @@ def cn_wells(shape=(192, 192, 192), step=0.3, g=0.001, seed=3):
     return (psi * win).astype(np.complex128), v
 
 
+def batch2d(seed: int = 7, sizes=(64, 128, 256, 512), per_size: int = 24, step: float = 0.2):
+    """The batched 2-D workload: per_size instances of each n x n size (order
+    shuffled with the seed), each with V = k r^2 / 2 (k ~ U(0.005, 0.02)) plus
+    1..6 Gaussian bumps (height ~ U(1e-3, 1e-2) Ha, width ~ U(1, 4) bohr,
+    centre ~ U(-L/4, L/4)^2) as a complex potential, and a Gaussian start
+    exp(-r^2/w^2 + i (k_y y + k_z z)) with w = 2 and k ~ U(-1, 1)^2.
+    Returns a list of (shape, psi0, v)."""
+    rng = np.random.default_rng(seed)
+    ns = [n for n in sizes for _ in range(per_size)]
+    rng.shuffle(ns)
+    out = []
+    for n in ns:
+        _, y, z = mesh(1, n, n, step)
+        r2 = y * y + z * z
+        v = 0.5 * rng.uniform(0.005, 0.02) * r2
+        L = n * step
+        for _ in range(int(rng.integers(1, 7))):
+            h, w = rng.uniform(1e-3, 1e-2), rng.uniform(1.0, 4.0)
+            cy, cz = rng.uniform(-L / 4, L / 4, 2)
+            v = v + h * np.exp(-((y - cy) ** 2 + (z - cz) ** 2) / w**2)
+        ky, kz = rng.uniform(-1.0, 1.0, 2)
+        psi = np.exp(-r2 / 4.0 + 1j * (ky * y + kz * z))
+        out.append(((1, n, n), psi.astype(np.complex128), v.astype(np.complex128)))
+    return out
+
+
 def run_gp_steps(n: int = 256, steps: int = 3, prec: int = 0) -> float:
     """Propagate the GP workload at n^3 for `steps` steps through the C API on
     the current GPU and return the final norm (a small driver for profilers:
