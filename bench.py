@@ -20,6 +20,10 @@ split-operator step of that wavefunction.
             complex128) over its mean CUDA-event duration in the timed region
   step_roofline  264 B/pt per step (4 transforms x 2 passes x 32 B + 8 B
             real V_ext) over the step time
+  batch2d   the batched uneven 2-D workload (96 instances of 64^2 .. 512^2,
+            complex potentials, FP64 and FP32): steps/s of all instances in
+            one persistent launch per call (grid_wf_batch_propagate) against
+            the same instances stepped one at a time (grid_wf_propagate)
 
 The grid (268 MB psi + 135 MB V_ext) exceeds the 126 MB L2, so no L2 flush
 is needed between steps.  Multi-GPU: independent replicas, one per GPU (the
@@ -229,6 +233,65 @@ def run_reference(args, world, rank):
     return 0
 
 
+def run_batch2d(api, lib, prec, steps, world):
+    """The batched 2-D workload (96 instances, n in {64, 128, 256, 512},
+    24 each, step 0.2, dt 0.05): `steps` steps of all instances through
+    grid_wf_batch_propagate (one persistent launch per call) against the
+    same instances stepped one at a time with grid_wf_propagate, both timed
+    with CUDA events on the library stream."""
+    from libgrid_b200 import capi, workloads
+
+    inst = workloads.batch2d(seed=7)
+    step, mass, dt = 0.2, 1.0, 0.05
+    wfs = [api.wf(*sh, step, mass, capi.WF_PERIODIC_BOUNDARY, capi.WF_2ND_ORDER_FFT, values=psi) for sh, psi, _ in inst]
+    pots = [api.cgrid(*sh, step, values=v) for sh, _, v in inst]
+    if prec:
+        for w in wfs:
+            w.precision(prec)
+    pts = sum(int(np.prod(sh)) for sh, _, _ in inst)
+    b = api.batch(wfs, pots, dt)
+    b.propagate(8)  # autotune (first call) + warm-up
+    lib.gb_synchronize()
+    barrier(world)
+    lib.gb_event_record(4)
+    b.propagate(steps)
+    lib.gb_event_record(5)
+    lib.gb_synchronize()
+    ms_b = allmax(world, lib.gb_event_elapsed_ms(4, 5))
+    threads = lib.grid_wf_batch_threads(b.ptr)
+    api.free(b)
+    seq_steps = max(2, steps // 10)
+    for w, p in zip(wfs, pots):
+        w.propagate(p, dt)
+    lib.gb_synchronize()
+    barrier(world)
+    lib.gb_event_record(6)
+    for w, p in zip(wfs, pots):
+        for _ in range(seq_steps):
+            w.propagate(p, dt)
+    lib.gb_event_record(7)
+    lib.gb_synchronize()
+    ms_s = allmax(world, lib.gb_event_elapsed_ms(6, 7))
+    for o in wfs + pots:
+        api.free(o)
+    esz = 8 if prec else 16
+    batched = world * steps / (ms_b * 1e-3)
+    seq = world * seq_steps / (ms_s * 1e-3)
+    return {
+        "instances": len(inst),
+        "points_per_step": pts,
+        "steps": steps,
+        "batched_steps_per_s": batched,
+        "sequential_steps_per_s": seq,
+        "speedup_vs_sequential": batched / seq,
+        "cta_threads_autotuned": threads,
+        "bytes_per_point_5pass": 5 * 2 * esz + esz,
+        "achieved_gbs_5pass": (5 * 2 * esz + esz) * pts * batched / world / 1e9,
+        "note": "a step = one 2nd-order split-operator step of every instance; sequential = the same instances "
+        "through grid_wf_propagate one at a time",
+    }
+
+
 def run_b200(args, world, rank, local):
     import libgrid_b200 as gb
     from libgrid_b200 import capi, workloads
@@ -326,6 +389,12 @@ def run_b200(args, world, rank, local):
     api.free(w)
     api.free(vx)
 
+    # ---------------------------------- batched uneven 2-D (one launch/call)
+    batch = {}
+    if not args.no_batch:
+        for prec, name in ((0, "fp64"), (capi.GRID_PREC_FP32, "fp32")):
+            batch[name] = run_batch2d(api, lib, prec, args.batch_steps, world)
+
     # ------------------------------------------------------------ report
     if rank != 0:
         return 0
@@ -389,6 +458,7 @@ def run_b200(args, world, rank, local):
         "step_roofline": {"bytes_per_point": BYTES_PER_POINT_STEP, "achieved": step_gbs, "frac": step_gbs / peak},
         "passes": per_kind,
         "gpu_launches": int(launches),
+        "batch2d": batch or None,
         "e2e": {
             "value": world * args.steps / e2e_s,
             "unit": "steps/s",
@@ -429,6 +499,8 @@ def main(argv=None):
     ap.add_argument("--size", type=int, default=256)
     ap.add_argument("--cpu-steps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--batch-steps", type=int, default=200)
     args = ap.parse_args(argv)
     world, rank, local = dist_setup()
     try:

@@ -347,7 +347,7 @@ typedef struct grid_wf_batch grid_wf_batch;
 grid_wf_batch *grid_wf_batch_alloc(wf **wfs, cgrid **potentials, INT n, REAL complex time);
 void grid_wf_batch_propagate(grid_wf_batch *b, INT steps);
 void grid_wf_batch_free(grid_wf_batch *b);
-/* CTA size the batch autotuner chose (0 until a call of >= 5 steps). */
+/* CTA size the batch autotuner chose (0 until a call of >= 7 steps). */
 int grid_wf_batch_threads(grid_wf_batch *b);
 
 #ifdef __cplusplus

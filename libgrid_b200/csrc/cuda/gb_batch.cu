@@ -11,8 +11,8 @@
 // separates the passes.  The barrier is this file's own (atomic arrival
 // counter + generation word) with a bounded wait: a CTA that waits too long
 // sets the batch's error flag and leaves, so the launch always ends.
-// A small autotuner picks the CTA size (128 or 256 threads) per batch by
-// timing both on the first steps of the first call; both sizes compute the
+// A small autotuner picks the CTA size (128, 256 or 512 threads) per batch
+// by timing each on the first steps of the first call; all sizes compute the
 // same values.
 #include <math.h>
 #include <stdlib.h>
@@ -213,12 +213,12 @@ using namespace gbfft;
 struct gb_batch {
   int n, prec;
   BatchInst *d_inst;
-  BatchTile *d_tiles[2][2];  // [variant 128 / 256][contiguous / strided]
-  int ntiles[2][2];
+  BatchTile *d_tiles[3][2];  // [variant 128 / 256 / 512][contiguous / strided]
+  int ntiles[3][2];
   unsigned char *d_kin;
   unsigned *d_bar;
   int *d_err;
-  int grid[2];
+  int grid[3];
   int threads;  // chosen CTA size, 0 until tuned
 };
 
@@ -263,10 +263,18 @@ template <typename T, int THREADS> static int batch_launch(gb_batch *b, int step
   return 0;
 }
 
+static const int kBatchThreads[3] = {128, 256, 512};
+
 static int batch_run(gb_batch *b, int steps, int v) {
   if (steps <= 0) return 0;
-  if (b->prec == GB_FP32) return v ? batch_launch<float, 256>(b, steps, 1) : batch_launch<float, 128>(b, steps, 0);
-  return v ? batch_launch<double, 256>(b, steps, 1) : batch_launch<double, 128>(b, steps, 0);
+  if (b->prec == GB_FP32) {
+    if (v == 0) return batch_launch<float, 128>(b, steps, 0);
+    if (v == 1) return batch_launch<float, 256>(b, steps, 1);
+    return batch_launch<float, 512>(b, steps, 2);
+  }
+  if (v == 0) return batch_launch<double, 128>(b, steps, 0);
+  if (v == 1) return batch_launch<double, 256>(b, steps, 1);
+  return batch_launch<double, 512>(b, steps, 2);
 }
 
 // Kinetic tables of one geometry into caller-owned buffers (gb_fft.cu).
@@ -350,14 +358,13 @@ extern "C" gb_batch *gb_batch_create(const gb_batch_item *items, int n) {
     bi.ny = (int) it.g.ny;
   }
   cudaMemcpyAsync(b->d_inst, hi.data(), sizeof(BatchInst) * n, cudaMemcpyHostToDevice, st);
-  // tile lists for the two CTA sizes
-  const int threads[2] = {128, 256};
-  for (int v = 0; v < 2; v++) {
+  // tile lists for the CTA sizes
+  for (int v = 0; v < 3; v++) {
     std::vector<BatchTile> ct, stl;
     for (int i = 0; i < n; i++) {
       const long nz = items[i].g.nz, ny = items[i].g.ny;
       const long tlz = batch_tl(nz), tly = batch_tl(ny);
-      const long lz = threads[v] / tlz, bzy = threads[v] / tly;
+      const long lz = kBatchThreads[v] / tlz, bzy = kBatchThreads[v] / tly;
       for (long k = 0; k < ny / lz; k++) ct.push_back(BatchTile{i, (int) k});
       for (long k = 0; k < nz / bzy; k++) stl.push_back(BatchTile{i, (int) k});
     }
@@ -375,7 +382,8 @@ extern "C" gb_batch *gb_batch_create(const gb_batch_item *items, int n) {
   }
   b->grid[0] = prec == GB_FP32 ? batch_grid<float, 128>() : batch_grid<double, 128>();
   b->grid[1] = prec == GB_FP32 ? batch_grid<float, 256>() : batch_grid<double, 256>();
-  if (b->grid[0] <= 0 || b->grid[1] <= 0) {
+  b->grid[2] = prec == GB_FP32 ? batch_grid<float, 512>() : batch_grid<double, 512>();
+  if (b->grid[0] <= 0 || b->grid[1] <= 0 || b->grid[2] <= 0) {
     gb__set_error(1042, "batch: kernel cannot be resident");
     gb_batch_free(b);
     return nullptr;
@@ -383,34 +391,39 @@ extern "C" gb_batch *gb_batch_create(const gb_batch_item *items, int n) {
   return b;
 }
 
-// Steps of every instance.  The first call with at least five steps times one
-// step with each CTA size (after one warm-up step each) and keeps the faster;
-// those four steps count as steps of the run.
+// Steps of every instance.  The first call with at least seven steps times
+// one step with each CTA size (after one warm-up step each) and keeps the
+// fastest; those six steps count as steps of the run.
 extern "C" int gb_batch_step(gb_batch *b, int steps) {
   if (!b) return gb__set_error(1040, "batch: null");
   if (steps <= 0) return 0;
   if (!b->threads) {
-    if (steps < 5) return batch_run(b, steps, b->prec == GB_FP32 ? 1 : 0);
-    cudaEvent_t e[4];
-    for (int i = 0; i < 4; i++) cudaEventCreate(&e[i]);
+    if (steps < 7) return batch_run(b, steps, 1);
+    cudaEvent_t e[2];
+    cudaEventCreate(&e[0]);
+    cudaEventCreate(&e[1]);
     cudaStream_t st = gb__stream();
-    GB_TRYC(batch_run(b, 1, 0));
-    cudaEventRecord(e[0], st);
-    GB_TRYC(batch_run(b, 1, 0));
-    cudaEventRecord(e[1], st);
-    GB_TRYC(batch_run(b, 1, 1));
-    cudaEventRecord(e[2], st);
-    GB_TRYC(batch_run(b, 1, 1));
-    cudaEventRecord(e[3], st);
-    cudaEventSynchronize(e[3]);
-    float t128 = 0.f, t256 = 0.f;
-    cudaEventElapsedTime(&t128, e[0], e[1]);
-    cudaEventElapsedTime(&t256, e[2], e[3]);
-    for (int i = 0; i < 4; i++) cudaEventDestroy(e[i]);
-    b->threads = (t256 < t128) ? 256 : 128;
-    steps -= 4;
+    float best = 0.f;
+    int bv = 1;
+    for (int v = 0; v < 3; v++) {
+      GB_TRYC(batch_run(b, 1, v));
+      cudaEventRecord(e[0], st);
+      GB_TRYC(batch_run(b, 1, v));
+      cudaEventRecord(e[1], st);
+      cudaEventSynchronize(e[1]);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e[0], e[1]);
+      if (v == 0 || ms < best) {
+        best = ms;
+        bv = v;
+      }
+    }
+    cudaEventDestroy(e[0]);
+    cudaEventDestroy(e[1]);
+    b->threads = kBatchThreads[bv];
+    steps -= 6;
   }
-  return batch_run(b, steps, b->threads == 256 ? 1 : 0);
+  return batch_run(b, steps, b->threads == 128 ? 0 : (b->threads == 256 ? 1 : 2));
 }
 
 extern "C" int gb_batch_threads(const gb_batch *b) { return b ? b->threads : 0; }
@@ -428,7 +441,7 @@ extern "C" void gb_batch_free(gb_batch *b) {
   if (!b) return;
   cudaStreamSynchronize(gb__stream());
   cudaFree(b->d_inst);
-  for (int v = 0; v < 2; v++)
+  for (int v = 0; v < 3; v++)
     for (int k = 0; k < 2; k++) cudaFree(b->d_tiles[v][k]);
   cudaFree(b->d_kin);
   cudaFree(b->d_bar);
