@@ -385,9 +385,9 @@ template <typename T, int N, class SM> struct Program<T, N, SM> {
 
 template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N, SM, Op, Rest...> {
   // vstage: this thread's prefetched potential values in shared memory
-  // (element m at vstage[m * vstride]), or null to read the potential grid
+  // (element m at vstage[m * vsstride]), or null to read the potential grid
   static __device__ __forceinline__ void run(C2<T> (&v)[Sched<N>::P], int t, const SM &sm, const PassArgs &a, unsigned o,
-                                             unsigned q, double &acc, const void *vstage = nullptr, int vstride = 0) {
+                                             unsigned q, double &acc, const void *vstage = nullptr, int vsstride = 0) {
     using T2 = C2<T>;
     constexpr int P = Sched<N>::P;
     constexpr int TL = N / P;
@@ -446,7 +446,7 @@ template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N,
           cp_async_wait_all();
           vp = (const T *) vstage;
           vt = 0;
-          vm = (unsigned) vstride;
+          vm = (unsigned) vsstride;
         }
         if (pt.kind == GB_POT_REAL) {
           if (phase) pot_line_simple<T, P, TL, true, true>(v, t, vp, vt, vm, pt.cons, pt.g, cc);
@@ -477,7 +477,7 @@ template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N,
         acc += (k2line + a.ksq[ax][p]) * ((double) v[m].x * (double) v[m].x + (double) v[m].y * (double) v[m].y);
       }
     }
-    Program<T, N, SM, Rest...>::run(v, t, sm, a, o, q, acc, vstage, vstride);
+    Program<T, N, SM, Rest...>::run(v, t, sm, a, o, q, acc, vstage, vsstride);
   }
 };
 

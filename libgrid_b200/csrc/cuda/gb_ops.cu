@@ -164,59 +164,100 @@ template <int THREADS> __device__ __forceinline__ void block_sum2(double &x, dou
   }
 }
 
-template <typename TA, typename TB>
-__global__ void __launch_bounds__(kThreads) k_reduce(int op, const void *av, const void *bv, long nxy, long nz, long arow,
-                                                   long brow, double2 *partial, long nx, long ny, double step) {
-  __shared__ double sb[2 * kThreads / 32];
-  const size_t n = (size_t) nxy * nz;
-  double sx = 0.0, sy = 0.0;
-  for (size_t g = blockIdx.x * (size_t) blockDim.x + threadIdx.x; g < n; g += (size_t) gridDim.x * blockDim.x) {
-    const size_t ij = g / nz, k = g - ij * nz;
-    switch (op) {
-      case GB_RED_SUM: {
-        const C2<TA> a = ((const C2<TA> *) av)[g];
-        sx += (double) a.x;
-        sy += (double) a.y;
-      } break;
-      case GB_RED_NORM2: {
-        const C2<TA> a = ((const C2<TA> *) av)[g];
-        sx += (double) a.x * (double) a.x + (double) a.y * (double) a.y;
-      } break;
-      case GB_RED_CONJ_PRODUCT: {
-        const C2<TA> a = ((const C2<TA> *) av)[g];
-        const C2<TB> b = ((const C2<TB> *) bv)[g];
-        const double ar = a.x, ai = a.y, br = b.x, bi = b.y;
-        sx += ar * br + ai * bi;
-        sy += ar * bi - ai * br;
-      } break;
-      case GB_RED_EXPECT_COMPLEX: {
-        const C2<TA> a = ((const C2<TA> *) av)[g];
-        const C2<TB> b = ((const C2<TB> *) bv)[g];
-        const double w = (double) a.x * (double) a.x + (double) a.y * (double) a.y;
-        sx += w * (double) b.x;
-        sy += w * (double) b.y;
-      } break;
-      case GB_RED_EXPECT_REAL: {
-        const C2<TA> a = ((const C2<TA> *) av)[g];
-        const double w = (double) a.x * (double) a.x + (double) a.y * (double) a.y;
-        sx += w * (double) ((const TB *) bv)[ij * brow + k];
-      } break;
-      case GB_RED_REAL_SUM: sx += (double) ((const TA *) av)[ij * arow + k]; break;
-      case GB_RED_KSQ_NORM2: {
-        // src/cgrid_diff.c:838-871
-        const long j = (long) (ij % ny), i = (long) (ij / ny);
-        const double lx = 2.0 * M_PI / (step * (double) nx), ly = 2.0 * M_PI / (step * (double) ny),
-                     lz = 2.0 * M_PI / (step * (double) nz);
-        const double kx = (i <= nx / 2 ? (double) i : (double) (i - nx)) * lx;
-        const double ky = (j <= ny / 2 ? (double) j : (double) (j - ny)) * ly;
-        const double kz = ((long) k <= nz / 2 ? (double) k : (double) ((long) k - nz)) * lz;
-        const C2<TA> a = ((const C2<TA> *) av)[g];
-        sx += (kx * kx + ky * ky + kz * kz) * ((double) a.x * (double) a.x + (double) a.y * (double) a.y);
-      } break;
+// Contribution of element g (row ij, column k) to a reduction op.
+template <int OP, typename TA, typename TB> struct RedTerm {
+  static __device__ __forceinline__ double2 at(size_t g, const void *av, const void *bv, long nz, long arow, long brow,
+                                               long nx, long ny, double step) {
+    if constexpr (OP == GB_RED_SUM) {
+      const C2<TA> a = ((const C2<TA> *) av)[g];
+      return double2{(double) a.x, (double) a.y};
+    } else if constexpr (OP == GB_RED_NORM2) {
+      const C2<TA> a = ((const C2<TA> *) av)[g];
+      return double2{(double) a.x * (double) a.x + (double) a.y * (double) a.y, 0.0};
+    } else if constexpr (OP == GB_RED_CONJ_PRODUCT) {
+      const C2<TA> a = ((const C2<TA> *) av)[g];
+      const C2<TB> b = ((const C2<TB> *) bv)[g];
+      const double ar = a.x, ai = a.y, br = b.x, bi = b.y;
+      return double2{ar * br + ai * bi, ar * bi - ai * br};
+    } else if constexpr (OP == GB_RED_EXPECT_COMPLEX) {
+      const C2<TA> a = ((const C2<TA> *) av)[g];
+      const C2<TB> b = ((const C2<TB> *) bv)[g];
+      const double w = (double) a.x * (double) a.x + (double) a.y * (double) a.y;
+      return double2{w * (double) b.x, w * (double) b.y};
+    } else if constexpr (OP == GB_RED_EXPECT_REAL) {
+      const size_t ij = g / (size_t) nz, k = g - ij * (size_t) nz;
+      const C2<TA> a = ((const C2<TA> *) av)[g];
+      const double w = (double) a.x * (double) a.x + (double) a.y * (double) a.y;
+      return double2{w * (double) ((const TB *) bv)[ij * brow + k], 0.0};
+    } else if constexpr (OP == GB_RED_REAL_SUM) {
+      const size_t ij = g / (size_t) nz, k = g - ij * (size_t) nz;
+      return double2{(double) ((const TA *) av)[ij * arow + k], 0.0};
+    } else {
+      // GB_RED_KSQ_NORM2 (src/cgrid_diff.c:838-871)
+      const size_t ij = g / (size_t) nz, k = g - ij * (size_t) nz;
+      const long j = (long) (ij % (size_t) ny), i = (long) (ij / (size_t) ny);
+      const double lx = 2.0 * M_PI / (step * (double) nx), ly = 2.0 * M_PI / (step * (double) ny),
+                   lz = 2.0 * M_PI / (step * (double) nz);
+      const double kx = (i <= nx / 2 ? (double) i : (double) (i - nx)) * lx;
+      const double ky = (j <= ny / 2 ? (double) j : (double) (j - ny)) * ly;
+      const double kz = ((long) k <= nz / 2 ? (double) k : (double) ((long) k - nz)) * lz;
+      const C2<TA> a = ((const C2<TA> *) av)[g];
+      return double2{(kx * kx + ky * ky + kz * kz) * ((double) a.x * (double) a.x + (double) a.y * (double) a.y), 0.0};
     }
   }
-  block_sum2<kThreads>(sx, sy, sb);
-  if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(sx, sy);
+};
+
+// Grid-stride sum with four independent terms per iteration (four loads in
+// flight per thread); the block count, each thread's order of terms and the
+// combination order are fixed, so the result is the same on every run.
+template <typename TA, typename TB, int OP>
+__global__ void __launch_bounds__(kThreads) k_reduce(const void *av, const void *bv, long nxy, long nz, long arow,
+                                                   long brow, double2 *partial, long nx, long ny, double step) {
+  __shared__ double sb[2 * kThreads / 32];
+  using R = RedTerm<OP, TA, TB>;
+  const size_t n = (size_t) nxy * nz;
+  const size_t stride = (size_t) gridDim.x * blockDim.x;
+  size_t g = blockIdx.x * (size_t) blockDim.x + threadIdx.x;
+  double sx[4] = {0.0, 0.0, 0.0, 0.0}, sy[4] = {0.0, 0.0, 0.0, 0.0};
+  for (; g + 3 * stride < n; g += 4 * stride) {
+    double2 e[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) e[u] = R::at(g + u * stride, av, bv, nz, arow, brow, nx, ny, step);
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      sx[u] += e[u].x;
+      sy[u] += e[u].y;
+    }
+  }
+  for (; g < n; g += stride) {
+    const double2 e = R::at(g, av, bv, nz, arow, brow, nx, ny, step);
+    sx[0] += e.x;
+    sy[0] += e.y;
+  }
+  double tx = (sx[0] + sx[1]) + (sx[2] + sx[3]);
+  double ty = (sy[0] + sy[1]) + (sy[2] + sy[3]);
+  block_sum2<kThreads>(tx, ty, sb);
+  if (threadIdx.x == 0) partial[blockIdx.x] = make_double2(tx, ty);
+}
+
+template <typename TA, typename TB>
+static void launch_reduce(int op, int nb, cudaStream_t st, const void *a, const void *b, long nxy, long nz, long arow,
+                          long brow, double2 *partial, long nx, long ny, double step) {
+#define GB_RED_CASE(OPV)                                                                                       \
+  case OPV:                                                                                                    \
+    k_reduce<TA, TB, OPV><<<nb, kThreads, 0, st>>>(a, b, nxy, nz, arow, brow, partial, nx, ny, step); \
+    break;
+  switch (op) {
+    GB_RED_CASE(GB_RED_SUM)
+    GB_RED_CASE(GB_RED_NORM2)
+    GB_RED_CASE(GB_RED_CONJ_PRODUCT)
+    GB_RED_CASE(GB_RED_EXPECT_COMPLEX)
+    GB_RED_CASE(GB_RED_EXPECT_REAL)
+    GB_RED_CASE(GB_RED_REAL_SUM)
+    default:
+      GB_RED_CASE(GB_RED_KSQ_NORM2)
+  }
+#undef GB_RED_CASE
 }
 
 __global__ void k_finish2(const double2 *__restrict__ p, int n, double2 *out) {
@@ -325,10 +366,10 @@ extern "C" int gb_reduce(int op, const void *a, const void *b, const gb_geom *g,
   cudaStream_t st = gb__stream();
   const bool af = (g->prec == GB_FP32);
   const bool bf = (bprec == GB_FP32);
-  if (af && bf) k_reduce<float, float><<<nb, kThreads, 0, st>>>(op, a, b, nxy, g->nz, arow, brow, partial, g->nx, g->ny, g->step);
-  else if (af) k_reduce<float, double><<<nb, kThreads, 0, st>>>(op, a, b, nxy, g->nz, arow, brow, partial, g->nx, g->ny, g->step);
-  else if (bf) k_reduce<double, float><<<nb, kThreads, 0, st>>>(op, a, b, nxy, g->nz, arow, brow, partial, g->nx, g->ny, g->step);
-  else k_reduce<double, double><<<nb, kThreads, 0, st>>>(op, a, b, nxy, g->nz, arow, brow, partial, g->nx, g->ny, g->step);
+  if (af && bf) launch_reduce<float, float>(op, nb, st, a, b, nxy, g->nz, arow, brow, partial, g->nx, g->ny, g->step);
+  else if (af) launch_reduce<float, double>(op, nb, st, a, b, nxy, g->nz, arow, brow, partial, g->nx, g->ny, g->step);
+  else if (bf) launch_reduce<double, float>(op, nb, st, a, b, nxy, g->nz, arow, brow, partial, g->nx, g->ny, g->step);
+  else launch_reduce<double, double>(op, nb, st, a, b, nxy, g->nz, arow, brow, partial, g->nx, g->ny, g->step);
   GB_CHECK_LAUNCH("reduce");
   k_finish2<<<1, 1024, 0, st>>>(partial, nb, res);
   GB_CHECK_LAUNCH("reduce finish");
