@@ -177,6 +177,12 @@ class WaveFunction:
     def propagate_gp(self, vext: Grid | None, g: float, time) -> None:
         self.api.lib.grid_wf_propagate_gp(self.ptr, vext.ptr if vext else None, g, Complex.of(time))
 
+    def propagate_n(self, potential: Grid | None, time, nsteps: int) -> None:
+        self.api.lib.grid_wf_propagate_n(self.ptr, potential.ptr if potential else None, Complex.of(time), nsteps)
+
+    def propagate_gp_n(self, vext: Grid | None, g: float, time, nsteps: int) -> None:
+        self.api.lib.grid_wf_propagate_gp_n(self.ptr, vext.ptr if vext else None, g, Complex.of(time), nsteps)
+
     def norm(self) -> float:
         return self.api.lib.grid_wf_norm(self.ptr)
 

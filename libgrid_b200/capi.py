@@ -214,6 +214,8 @@ def bind(lib: C.CDLL, cuda_layout: bool, extensions: bool):
         f("cuda_remove_block", C.c_int, V, ch)
     if extensions:
         f("grid_wf_propagate_gp", None, PW, PR, D, Cx)
+        f("grid_wf_propagate_n", None, PW, PC, Cx, L)
+        f("grid_wf_propagate_gp_n", None, PW, PR, D, Cx, L)
         f("grid_wf_precision", None, PW, ch)
         f("grid_wf_get_precision", ch, PW)
         f("grid_wf_batch_alloc", V, C.POINTER(PW), C.POINTER(PC), L, Cx)

@@ -277,9 +277,6 @@ static int batch_run(gb_batch *b, int steps, int v) {
   return batch_launch<double, 512>(b, steps, 2);
 }
 
-// Kinetic tables of one geometry into caller-owned buffers (gb_fft.cu).
-int gb__kin_tables_at(void *fac, double *ksq, const gb_geom *g, const gb_kinetic *kin);
-
 extern "C" gb_batch *gb_batch_create(const gb_batch_item *items, int n) {
   if (n <= 0 || !items) {
     gb__set_error(1040, "batch: no instances");

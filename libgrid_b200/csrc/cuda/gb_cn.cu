@@ -158,7 +158,7 @@ __device__ __forceinline__ double2 cn_rhs(long i, long n, int bc, double2 cp, do
 }
 
 // Segments per line in the fast kernel (= warps per CTA).
-constexpr int kSeg = 8;
+constexpr int kSeg = 16;
 
 // Contiguous tile rows are padded to an odd number of 16-byte elements so a
 // warp's lane-per-line accesses fall in distinct shared-memory banks.
@@ -180,7 +180,7 @@ template <bool CONTIG> __device__ __forceinline__ double2 &tile_at(double2 *sm, 
 // carry-in, one warp chains the 8 segment carries per line, and every
 // element then adds (carry-in) x (homogeneous response), whose tables
 // H_i = prod(-m_j) and G_i = prod(Q_j) over the segment are precomputed.
-template <bool CONTIG> __global__ void __launch_bounds__(32 * kSeg) k_cn_fast(double2 *__restrict__ psi, CnAxis a) {
+template <bool CONTIG> __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast(double2 *__restrict__ psi, CnAxis a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ double2 s_end[kSeg][32];

@@ -236,6 +236,12 @@ extern "C" int gb_split_step(void *psi, const gb_geom *g, const gb_kinetic *kin,
   return gb__split_step_t<double>(psi, g, kin, pot);
 }
 
+extern "C" int gb_split_steps(void *psi, const gb_geom *g, const gb_kinetic *kin, const gb_potential *pot, int nsteps) {
+  if (fft_geom_ok(g)) return gb_last_error();
+  if (g->prec == GB_FP32) return gb__split_steps_t<float>(psi, g, kin, pot, nsteps);
+  return gb__split_steps_t<double>(psi, g, kin, pot, nsteps);
+}
+
 extern "C" int gb_fft_ksq_sum(const void *psi, void *work, const gb_geom *g, double *out) {
   if (fft_geom_ok(g)) return gb_last_error();
   if (g->prec == GB_FP32) return gb__ksq_sum_t<float>(psi, work, g, out);

@@ -129,6 +129,65 @@ int gb__split_step_t(void *psi, const gb_geom *g, const gb_kinetic *kin, const g
   return 0;
 }
 
+// nsteps consecutive split-operator steps with the k-space state kept
+// between them: the trailing inverse transforms of one step and the leading
+// forward transforms of the next cancel, and the two K(dt/2) factors that
+// then meet on the outermost axis merge into one K(dt) pass.  Every FWD.K.INV
+// pass closes one round trip per axis, so each keeps the 1/N factor.  Steady
+// state: outermost FWD.K(dt).INV, middle INV, innermost INV.V.FWD, middle FWD.
+template <typename T>
+int gb__split_steps_t(void *psi, const gb_geom *g, const gb_kinetic *kin, const gb_potential *pot, int nsteps) {
+  using namespace gbfft;
+  int ax[3];
+  const int na = active_axes(g, ax);
+  if (nsteps <= 0) return 0;
+  if (na < 2 || nsteps == 1) {
+    for (int s = 0; s < nsteps; s++) GB_TRY(gb__split_step_t<T>(psi, g, kin, pot));
+    return 0;
+  }
+  PassArgs ah = base_args(g);
+  GbKinTables kt;
+  GB_TRY(gb__kin_tables(g, kin, 0, &kt));
+  for (int d = 0; d < 3; d++) {
+    ah.kfac[d] = kt.kfac[d];
+    ah.ksq[d] = kt.ksq[d];
+  }
+  ah.kscale = kin->scale;
+  ah.cutoff = kin->cutoff;
+  ah.kmax2 = kin->kmax2;
+  const bool has_pot = (pot != nullptr);
+  if (has_pot) ah.pot = *pot;
+  // K(dt): the same factor with twice the exponent, in its own tables
+  gb_kinetic kf = *kin;
+  kf.tm_re *= 2.0;
+  kf.tm_im *= 2.0;
+  const long tot = g->nx + g->ny + g->nz;
+  const size_t esz = sizeof(C2<T>);
+  unsigned char *fb = (unsigned char *) gb__scratch(GB_SCR_KIN2, (size_t) tot * (esz + 8));
+  if (!fb) return gb_last_error();
+  double *fsq = (double *) (fb + (size_t) tot * esz);
+  GB_TRY(gb__kin_tables_at(fb, fsq, g, &kf));
+  PassArgs af = ah;
+  af.kfac[0] = fb;
+  af.kfac[1] = fb + esz * (size_t) g->nx;
+  af.kfac[2] = fb + esz * (size_t) (g->nx + g->ny);
+  af.ksq[0] = fsq;
+  af.ksq[1] = fsq + g->nx;
+  af.ksq[2] = fsq + g->nx + g->ny;
+  const int last = ax[na - 1];
+  for (int s = 0; s < na - 1; s++) GB_TRY((pass<T>(g, ax[s], psi, psi, ah, OpL<OP_FWD>{})));
+  for (int st = 0; st < nsteps; st++) {
+    GB_TRY((pass<T>(g, last, psi, psi, st == 0 ? ah : af, OpL<OP_FWD, OP_KIN, OP_INV>{})));
+    for (int s = na - 2; s >= 1; s--) GB_TRY((pass<T>(g, ax[s], psi, psi, ah, OpL<OP_INV>{})));
+    if (has_pot) GB_TRY((pass<T>(g, ax[0], psi, psi, ah, OpL<OP_INV, OP_POT, OP_FWD>{})));
+    else GB_TRY((pass<T>(g, ax[0], psi, psi, ah, OpL<OP_INV, OP_FWD>{})));
+    for (int s = 1; s < na - 1; s++) GB_TRY((pass<T>(g, ax[s], psi, psi, ah, OpL<OP_FWD>{})));
+  }
+  GB_TRY((pass<T>(g, last, psi, psi, ah, OpL<OP_FWD, OP_KIN, OP_INV>{})));
+  for (int s = na - 2; s >= 0; s--) GB_TRY((pass<T>(g, ax[s], psi, psi, ah, OpL<OP_INV>{})));
+  return 0;
+}
+
 template <typename T> int gb__ksq_sum_t(const void *psi, void *work, const gb_geom *g, double *out) {
   using namespace gbfft;
   int ax[3];

@@ -6,4 +6,5 @@
 
 template int gb__fft3d_t<float>(void *, const gb_geom *, int, double);
 template int gb__split_step_t<float>(void *, const gb_geom *, const gb_kinetic *, const gb_potential *);
+template int gb__split_steps_t<float>(void *, const gb_geom *, const gb_kinetic *, const gb_potential *, int);
 template int gb__ksq_sum_t<float>(const void *, void *, const gb_geom *, double *);

@@ -13,6 +13,7 @@ enum {
   GB_SCR_CN = 3,       // line-solver coefficient tables
   GB_SCR_WORK = 4,     // temporary full grids
   GB_SCR_STAGE = 5,    // precision-conversion staging
+  GB_SCR_KIN2 = 6,     // kinetic factor tables of the merged K(dt) pass
   GB_SCR_COUNT = 8
 };
 
@@ -29,10 +30,15 @@ struct GbKinTables {
   const double *ksq[3];
 };
 int gb__kin_tables(const gb_geom *g, const gb_kinetic *kin, int unshifted, GbKinTables *out);
+// The same tables into caller-owned buffers (fac: nx + ny + nz factors in the
+// storage precision, then as many k^2 values in ksq).
+int gb__kin_tables_at(void *fac, double *ksq, const gb_geom *g, const gb_kinetic *kin);
 
 // Precision-specific drivers (gb_fft_f64.cu / gb_fft_f32.cu).
 template <typename T> int gb__fft3d_t(void *data, const gb_geom *g, int sign, double scale);
 template <typename T> int gb__split_step_t(void *psi, const gb_geom *g, const gb_kinetic *kin, const gb_potential *pot);
+template <typename T>
+int gb__split_steps_t(void *psi, const gb_geom *g, const gb_kinetic *kin, const gb_potential *pot, int nsteps);
 template <typename T> int gb__ksq_sum_t(const void *psi, void *work, const gb_geom *g, double *out);
 
 // Deterministic sum of n partials into out (FP64), on the library stream.
