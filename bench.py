@@ -20,6 +20,8 @@ split-operator step of that wavefunction.
             complex128) over its mean CUDA-event duration in the timed region
   step_roofline  264 B/pt per step (4 transforms x 2 passes x 32 B + 8 B
             real V_ext) over the step time
+  multi_step the same step through grid_wf_propagate_gp_n (all timed steps
+            in one call, k-space state kept between steps: 136 B/pt)
   batch2d   the batched uneven 2-D workload (96 instances of 64^2 .. 512^2,
             complex potentials, FP64 and FP32): steps/s of all instances in
             one persistent launch per call (grid_wf_batch_propagate) against
@@ -389,6 +391,19 @@ def run_b200(args, world, rank, local):
     api.free(w)
     api.free(vx)
 
+    # ------------------- multi-step calls (k-space state kept between steps)
+    w, vx = make()
+    w.propagate_gp_n(vx, g, dt, 4)
+    lib.gb_synchronize()
+    barrier(world)
+    lib.gb_event_record(8)
+    w.propagate_gp_n(vx, g, dt, args.steps)
+    lib.gb_event_record(9)
+    lib.gb_synchronize()
+    ms_multi = allmax(world, lib.gb_event_elapsed_ms(8, 9))
+    api.free(w)
+    api.free(vx)
+
     # ---------------------------------- batched uneven 2-D (one launch/call)
     batch = {}
     if not args.no_batch:
@@ -458,6 +473,17 @@ def run_b200(args, world, rank, local):
         "step_roofline": {"bytes_per_point": BYTES_PER_POINT_STEP, "achieved": step_gbs, "frac": step_gbs / peak},
         "passes": per_kind,
         "gpu_launches": int(launches),
+        "multi_step": {
+            "value": world * args.steps / (ms_multi * 1e-3),
+            "unit": "steps/s",
+            "ms_per_step": ms_multi / args.steps,
+            "speedup_vs_single_step_calls": ms_max / ms_multi,
+            "bytes_per_point": 136,
+            "achieved_gbs": 136 * N * args.steps / (ms_multi * 1e-3) / 1e9,
+            "note": "grid_wf_propagate_gp_n: the same steps in one call with the k-space state kept between "
+            "steps (4 passes per step: 4 x 32 B + 8 B V_ext); a different schedule from the headline, "
+            "reported separately",
+        },
         "batch2d": batch or None,
         "e2e": {
             "value": world * args.steps / e2e_s,

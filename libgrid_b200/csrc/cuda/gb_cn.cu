@@ -667,8 +667,20 @@ extern "C" int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, co
       if (!tab) return gb_last_error();
       a.tab = tab;
       a.cp = make_double2(cp.real(), cp.imag());
-      // tile budget: two CTAs (tile + ~8.7 KB static) per SM
-      const size_t budget = 100 * 1024;
+      // tile budget: two CTAs per SM, each with its tile, its static
+      // shared memory and the per-CTA reservation
+      static size_t budget = 0;
+      if (!budget) {
+        int dev = 0, smpm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&smpm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        cudaFuncAttributes fa0, fa1;
+        cudaFuncGetAttributes(&fa0, k_cn_fast<true>);
+        cudaFuncGetAttributes(&fa1, k_cn_fast<false>);
+        const size_t st_max = fa0.sharedSizeBytes > fa1.sharedSizeBytes ? fa0.sharedSizeBytes : fa1.sharedSizeBytes;
+        const long b = (long) smpm / 2 - 1024 - (long) st_max;
+        budget = b > 16 * 1024 ? (size_t) b : 16 * 1024;
+      }
       if (contig) {
         const long row = contig_row(a.n);
         long lpc = (long) (budget / (row * 16));
