@@ -108,6 +108,12 @@ int gb_upload_f64_as_f32(void *dev32, const void *host64, size_t n);
 int gb_download_f32_as_f64(void *host64, const void *dev32, size_t n);
 /* Status word of the bounded device-side waits (0 = none timed out). */
 int gb_cn_error_flag(void);
+/* Same for the pipelined FFT line passes; reset != 0 clears it. */
+int gb_pass_error_flag(int reset);
+/* Pipelined (persistent, TMA-prefetching) strided line passes: on = 1
+ * enables (the default), 0 disables, -1 only queries.  Returns the previous
+ * setting.  Both forms compute the same values.  (No reference counterpart.) */
+int gb_pass_pipeline(int on);
 
 /* ----------------------------------------------------------------- FFT */
 /* In-place 3-D complex FFT, unnormalised, then multiplied by scale

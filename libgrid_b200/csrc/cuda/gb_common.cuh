@@ -221,6 +221,15 @@ __device__ __forceinline__ void bulk_g2s(void *sdst, const void *gsrc, unsigned 
                "l"(gsrc), "r"(bytes), "r"(smem_u32(bar))
                : "memory");
 }
+// 3-D tiled tensor copy global -> shared through a tensor map (no
+// multicast); coordinates innermost first, completion signalled on bar.
+__device__ __forceinline__ void tma_load_3d(void *sdst, const void *tmap, int c0, int c1, int c2, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(smem_u32(sdst)),
+      "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(smem_u32(bar))
+      : "memory");
+}
 // shared -> global in the calling thread's bulk group
 __device__ __forceinline__ void bulk_s2g(void *gdst, const void *ssrc, unsigned bytes) {
   asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(gdst), "r"(smem_u32(ssrc)), "r"(bytes)

@@ -53,6 +53,8 @@ int pass(const gb_geom *g, int axis, const void *src, void *dst, PassArgs a, OpL
   a.axis = axis;
   a.tw = gb__twiddles(v.n, g->prec);
   if (!a.tw) return gb_last_error();
+  a.errflag = gb__pass_errflag();
+  if (!a.errflag) return gb_last_error();
   const int slot = gb__pass_begin(5 * axis + prog_id(ops));
   const int rc = launch_pass<T>(v.n, src, dst, a, v.outer, v.inner, ops);
   gb__pass_end(slot);

@@ -22,7 +22,13 @@
 // conflict-free.
 #pragma once
 
+#include <cuda.h>
+
 #include "gb_common.cuh"
+
+// Tensor maps for the pipelined strided passes and their error flag
+// (gb_runtime.cu).
+int gb__tmap_lines(CUtensorMap *out, const void *base, long outer, long n, long inner, int fp32, int bz, int rows);
 
 namespace gbfft {
 
@@ -244,6 +250,7 @@ struct PassArgs {
   double scale;         // OP_SCALE
   gb_potential pot;
   double *partial;      // OP_KSQ: one partial sum per block
+  int *errflag;         // pipelined passes: set when a bounded wait gives up
 };
 
 // Decode (i, j, k) of axis position p for a line given by (o, q).  Grids
@@ -369,6 +376,7 @@ __device__ __forceinline__ bool pot_prefetch(const PassArgs &a, unsigned o, unsi
 }
 
 template <int... Ops> __host__ __device__ constexpr bool has_pot(OpL<Ops...>) { return ((Ops == OP_POT) || ...); }
+template <int... Ops> __host__ __device__ constexpr bool has_kin(OpL<Ops...>) { return ((Ops == OP_KIN) || ...); }
 
 template <int Op, int... Rest> struct OpsHead {
   static constexpr int value = Op;
@@ -608,6 +616,124 @@ __global__ void __launch_bounds__((N / Sched<N>::P) * BZ, pass_min_blocks<(N / S
   }
 }
 
+// Pipelined strided passes: a persistent CTA walks over its tiles (BZ
+// columns x N rows of one outer index).  Each tile arrives in a landing
+// buffer through one tiled tensor copy (TMA, no multicast) per 256 rows,
+// completing on an mbarrier; as soon as every thread has its elements in
+// registers, the next tile's copy is issued, so the HBM reads of tile t + G
+// run under the transforms and stores of tile t.  The radix exchanges use a
+// separate buffer.  Waits are bounded: a CTA whose wait gives up sets the
+// pass error flag, waits (bounded) for its copy in flight and leaves.
+int pipe_enabled();
+
+template <int N> __host__ __device__ constexpr int pipe_rows() { return N < 256 ? N : 256; }
+
+template <typename T, int N, int BZ, int... Ops>
+__global__ void __launch_bounds__((N / Sched<N>::P) * BZ, sizeof(T) == 8 ? 3 : 3)
+    k_pass_strided_pipe(C2<T> *__restrict__ dst, unsigned inner, unsigned ncb, unsigned ntiles, PassArgs a,
+                        const __grid_constant__ CUtensorMap tmap) {
+  using T2 = C2<T>;
+  constexpr int P = Sched<N>::P, TL = N / P;
+  constexpr int ROWS = pipe_rows<N>();
+  constexpr unsigned TILE_BYTES = (unsigned) (N * BZ * sizeof(T2));
+  extern __shared__ __align__(128) unsigned char smraw[];
+  __shared__ __align__(8) uint64_t bar;
+  // the dynamic buffer has 128 spare bytes: the landing buffer starts at the
+  // first 128-byte boundary in it, as the tensor copy requires
+  unsigned char *base = smraw + ((128u - (smem_u32(smraw) & 127u)) & 127u);
+  T2 *land = (T2 *) base;
+  T2 *xch = (T2 *) (base + TILE_BYTES);
+  const int tid = threadIdx.x;
+  const int c = tid % BZ, t = tid / BZ;
+  // a descriptor that is not 64-byte aligned is recorded (code 3) and the
+  // pass skipped
+  if (((size_t) &tmap & 63u) != 0) {
+    if (tid == 0 && a.errflag) atomicExch(a.errflag, 3);
+    return;
+  }
+  if (tid == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  unsigned tile = blockIdx.x;
+  if (tid == 0 && tile < ntiles) {
+    const unsigned o = tile / ncb, cb = tile - o * ncb;
+    mbar_arrive_expect_tx(&bar, TILE_BYTES);
+#pragma unroll
+    for (int h = 0; h < N / ROWS; h++) tma_load_3d(land + h * ROWS * BZ, &tmap, (int) (cb * 2 * BZ), h * ROWS, (int) o, &bar);
+  }
+  for (unsigned it = 0; tile < ntiles; tile += gridDim.x, it++) {
+    const bool ok = mbar_wait_bounded(&bar, it & 1u);
+    T2 v[P];
+#pragma unroll
+    for (int m = 0; m < P; m++) v[m] = land[(t + TL * m) * BZ + c];
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) {
+        if (a.errflag) atomicExch(a.errflag, 1);
+        mbar_wait_bounded(&bar, it & 1u);
+      }
+      return;
+    }
+    const unsigned next = tile + gridDim.x;
+    if (tid == 0 && next < ntiles) {
+      const unsigned o = next / ncb, cb = next - o * ncb;
+      mbar_arrive_expect_tx(&bar, TILE_BYTES);
+#pragma unroll
+      for (int h = 0; h < N / ROWS; h++)
+        tma_load_3d(land + h * ROWS * BZ, &tmap, (int) (cb * 2 * BZ), h * ROWS, (int) o, &bar);
+    }
+    const unsigned o = tile / ncb;
+    const unsigned q = (tile - o * ncb) * (unsigned) BZ + (unsigned) c;
+    SmStrided<T2, BZ> sm{xch + c};
+    double acc = 0.0;
+    Program<T, N, SmStrided<T2, BZ>, Ops...>::run(v, t, sm, a, o, q, acc);
+    T2 *d = dst + (size_t) o * (size_t) N * inner + q;
+#pragma unroll
+    for (int m = 0; m < P; m++) d[(unsigned) (t + TL * m) * inner] = v[m];
+  }
+}
+
+// Launch the pipelined form when it applies (strided lines of 64..256,
+// programs with the kinetic op and without a potential or a reduction);
+// *launched says whether it did.
+template <typename T, int N, int BZ, int... Ops>
+int launch_strided_pipe(const void *src, void *dst, const PassArgs &a, long outer, long inner, int *launched) {
+  *launched = 0;
+  // measured on B200: the prefetch pays off on the fused FWD.K.INV pass
+  // (two transforms per tile), while single-transform passes are faster in
+  // the plain form, which keeps more warps resident
+  if constexpr (N < 64 || N > 256 || has_ksq(OpL<Ops...>{}) || has_pot(OpL<Ops...>{}) || !has_kin(OpL<Ops...>{})) {
+    return 0;
+  } else {
+    using T2 = C2<T>;
+    if (!pipe_enabled() || !a.errflag || (size_t) src % 16 != 0 || inner % BZ != 0) return 0;
+    const long ncb = inner / BZ, ntiles = outer * ncb;
+    if (ntiles >= (1l << 31) || inner >= (1l << 30)) return 0;
+    constexpr size_t SM = 2 * (size_t) N * BZ * sizeof(T2) + 128;
+    constexpr int THREADS = (N / Sched<N>::P) * BZ;
+    auto kern = k_pass_strided_pipe<T, N, BZ, Ops...>;
+    static int rgrid = 0;
+    if (!rgrid) {
+      int dev = 0, nsm = 0, per = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+      cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) SM);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, THREADS, SM);
+      rgrid = (nsm > 0 && per > 0) ? nsm * per : -1;
+    }
+    if (rgrid < 0) return 0;
+    CUtensorMap tm;
+    if (gb__tmap_lines(&tm, src, outer, N, inner, sizeof(T) == 4, BZ, pipe_rows<N>())) return gb_last_error();
+    const long g = ntiles < rgrid ? ntiles : rgrid;
+    kern<<<(unsigned) g, THREADS, SM, gb__stream()>>>((T2 *) dst, (unsigned) inner, (unsigned) ncb,
+                                                       (unsigned) ntiles, a, tm);
+    *launched = 1;
+    GB_CHECK_LAUNCH("pipelined fft pass");
+    return 0;
+  }
+}
+
 // Launch one pass of program Ops along `axis` for line length N.
 template <typename T, int N, int... Ops>
 int launch_pass_n(const void *src, void *dst, const PassArgs &a, long outer, long inner, long *nblocks) {
@@ -629,6 +755,11 @@ int launch_pass_n(const void *src, void *dst, const PassArgs &a, long outer, lon
     kern<<<(unsigned) nb, Cfg::THREADS, sm, st>>>((const T2 *) src, (T2 *) dst, outer, a);
   } else {
     constexpr int BZ = StridedCfg<N, sizeof(T)>::BZ;
+    if (!nblocks) {
+      int launched = 0;
+      const int rc = launch_strided_pipe<T, N, BZ, Ops...>(src, dst, a, outer, inner, &launched);
+      if (rc || launched) return rc;
+    }
     if (inner % BZ == 0 && outer <= 65535) {
       const size_t sm = (size_t) N * BZ * sizeof(T2) + STAGE * (N / Sched<N>::P) * BZ;
       auto kern = k_pass_strided<T, N, BZ, Ops...>;

@@ -1,6 +1,7 @@
 // Internal declarations shared by the libgrid-b200 CUDA translation units.
 #pragma once
 
+#include <cuda.h>
 #include <stddef.h>
 
 #include "gb_cuda.h"
@@ -22,6 +23,12 @@ void *gb__scratch(int slot, size_t bytes);
 int gb__pass_begin(int kind);
 void gb__pass_end(int slot);
 const void *gb__twiddles(long n, int prec);
+// Tensor map (TMA descriptor) over the line view [outer][n][inner] of a
+// complex grid (fp32 = 0: double2 elements, 1: float2), read as reals with
+// the box 2*bz reals x rows lines x 1.  Cached per argument set.
+int gb__tmap_lines(CUtensorMap *out, const void *base, long outer, long n, long inner, int fp32, int bz, int rows);
+// Device flag set by a pipelined pass whose bounded wait gave up.
+int *gb__pass_errflag(void);
 
 // Kinetic factor tables for (g, kin): per-axis complex factors exp(tm k_a^2)
 // in the storage precision of g and per-axis k_a^2 in FP64.

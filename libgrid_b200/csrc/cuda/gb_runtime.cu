@@ -11,6 +11,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <cudaTypedefs.h>
+
 #include "gb_common.cuh"
 #include "gb_internal_cuda.h"
 
@@ -221,6 +223,86 @@ int gb__pass_begin(int kind) {
 
 void gb__pass_end(int slot) {
   if (slot >= 0) cudaEventRecord(g_pt_ev[2 * slot + 1], g_stream);
+}
+
+// Tensor maps (TMA descriptors) for the pipelined strided passes, cached by
+// argument set.  The encode entry point is taken from the driver through the
+// runtime, so nothing links libcuda directly.
+struct TmapKey {
+  const void *base;
+  long outer, n, inner;
+  int fp32, bz, rows;
+};
+static TmapKey g_tm_key[32];
+static CUtensorMap g_tm_val[32];
+static int g_tm_used = 0, g_tm_next = 0;
+static PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+
+int gb__tmap_lines(CUtensorMap *out, const void *base, long outer, long n, long inner, int fp32, int bz, int rows) {
+  for (int i = 0; i < g_tm_used; i++) {
+    const TmapKey &k = g_tm_key[i];
+    if (k.base == base && k.outer == outer && k.n == n && k.inner == inner && k.fp32 == fp32 && k.bz == bz &&
+        k.rows == rows) {
+      *out = g_tm_val[i];
+      return 0;
+    }
+  }
+  if (!g_encode) {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn ||
+        q != cudaDriverEntryPointSuccess)
+      return gb__set_error(1030, "tensor map: cuTensorMapEncodeTiled unavailable");
+    g_encode = (PFN_cuTensorMapEncodeTiled_v12000) fn;
+  }
+  const cuuint64_t esz = fp32 ? 4 : 8;
+  const cuuint64_t dims[3] = {(cuuint64_t) (2 * inner), (cuuint64_t) n, (cuuint64_t) outer};
+  const cuuint64_t strides[2] = {(cuuint64_t) (2 * inner) * esz, (cuuint64_t) (2 * inner) * esz * (cuuint64_t) n};
+  const cuuint32_t box[3] = {(cuuint32_t) (2 * bz), (cuuint32_t) rows, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  CUtensorMap m;
+  const CUresult r = g_encode(&m, fp32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3,
+                              (void *) base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return gb__set_error(1031, "tensor map: encode failed");
+  const int slot = g_tm_used < 32 ? g_tm_used++ : (g_tm_next++ & 31);
+  g_tm_key[slot] = TmapKey{base, outer, n, inner, fp32, bz, rows};
+  g_tm_val[slot] = m;
+  *out = m;
+  return 0;
+}
+
+// Error flag of the pipelined passes (one device int, allocated once).
+static int *g_pass_err = nullptr;
+int *gb__pass_errflag(void) {
+  if (!g_pass_err) {
+    if (cudaMalloc(&g_pass_err, sizeof(int)) != cudaSuccess) {
+      gb__set_error(2, "pass error flag");
+      return nullptr;
+    }
+    cudaMemsetAsync(g_pass_err, 0, sizeof(int), g_stream);
+  }
+  return g_pass_err;
+}
+
+extern "C" int gb_pass_error_flag(int reset) {
+  if (!g_pass_err) return 0;
+  int h = 0;
+  cudaStreamSynchronize(g_stream);
+  cudaMemcpy(&h, g_pass_err, sizeof(int), cudaMemcpyDeviceToHost);
+  if (reset) cudaMemset(g_pass_err, 0, sizeof(int));
+  return h;
+}
+
+static int g_pipe_on = 1;
+namespace gbfft {
+int pipe_enabled() { return g_pipe_on; }
+}  // namespace gbfft
+extern "C" int gb_pass_pipeline(int on) {
+  const int old = g_pipe_on;
+  if (on >= 0) g_pipe_on = on ? 1 : 0;
+  return old;
 }
 
 extern "C" int gb_pass_timing_report(double *ms, long *count, int nkinds) {
