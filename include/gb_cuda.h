@@ -261,6 +261,28 @@ typedef struct {
 } gb_cn_params;
 int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, const gb_potential *pre, const gb_potential *post);
 
+/* --------------------------------------------------------------- noise */
+/* Seeded noise added to a device grid (the reference's src/rand.c API and
+ * src/rand-cuda2.cu kernels), from a counter-based generator: the values
+ * depend only on (seed, call, element), so they are reproducible for a
+ * given seed and call sequence.  Real kinds act on a real grid with rows of
+ * `row` scalars; complex kinds on a complex grid (row unused).
+ *   R_UNIFORM     r += 2 s_re (u - 1/2)                 (src/rand.c:55-74)
+ *   R_NORMAL      r += s_re n                           (src/rand.c:84-122)
+ *   C_UNIFORM     z += 2 s_re (u - 1/2) + 2 i s_im (u' - 1/2) (src/rand.c:132-149)
+ *   C_UNIFORM_SP  z += s_re u exp(2 pi i u')            (src/rand.c:159-176)
+ *   C_NORMAL      z += s_re n + i s_im n'               (src/rand.c:186-214)
+ *   C_NORMAL_SP   z += s_re n exp(i pi u)               (src/rand.c:224-250)
+ * with u, u' uniform in (0, 1) and n, n' standard normal. */
+#define GB_RAND_R_UNIFORM 1
+#define GB_RAND_R_NORMAL 2
+#define GB_RAND_C_UNIFORM 3
+#define GB_RAND_C_UNIFORM_SP 4
+#define GB_RAND_C_NORMAL 5
+#define GB_RAND_C_NORMAL_SP 6
+int gb_random(int kind, void *data, const gb_geom *g, long row, double scale_re, double scale_im,
+              unsigned long long seed, unsigned long long call);
+
 /* ------------------------------------------------------------- batches */
 /*
  * Many independent 2-D wave functions of uneven sizes advanced together by

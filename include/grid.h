@@ -179,6 +179,17 @@ void cgrid_shift_origin(cgrid *grid, REAL x0, REAL y0, REAL z0);
 void cgrid_set_momentum(cgrid *grid, REAL kx0, REAL ky0, REAL kz0);
 void cgrid_set_rotation(cgrid *grid, REAL omega);
 /* src/cgrid.c:360,383 -- binary format nx, ny, nz (INT), step (REAL), values */
+/* Seeded noise (src/rand.c:34-250; GPU src/rand-cuda2.cu:54-300).  Values
+ * come from a counter-based generator seeded by grid_random_seed (by the
+ * time of day when never seeded, as in the reference); they follow the
+ * reference's distributions, not its drand48 / cuRAND sequences. */
+void grid_random_seed(INT nx, INT ny, INT nz, INT seed);
+void rgrid_random_uniform(rgrid *grid, REAL scale);
+void rgrid_random_normal(rgrid *grid, REAL scale);
+void cgrid_random_uniform(cgrid *grid, REAL complex scale);
+void cgrid_random_uniform_sp(cgrid *grid, REAL scale);
+void cgrid_random_normal(cgrid *grid, REAL complex scale);
+void cgrid_random_normal_sp(cgrid *grid, REAL scale);
 void cgrid_write(cgrid *grid, FILE *out);
 cgrid *cgrid_read(cgrid *grid, FILE *in);
 /* src/cgrid.c:615 */

@@ -148,6 +148,13 @@ def bind(lib: C.CDLL, cuda_layout: bool, extensions: bool):
     f("cgrid_set_momentum", None, PC, D, D, D)
     f("cgrid_set_origin", None, PC, D, D, D)
     f("cgrid_set_rotation", None, PC, D)
+    f("grid_random_seed", None, L, L, L, L)
+    f("rgrid_random_uniform", None, PR, D)
+    f("rgrid_random_normal", None, PR, D)
+    f("cgrid_random_uniform", None, PC, Cx)
+    f("cgrid_random_uniform_sp", None, PC, D)
+    f("cgrid_random_normal", None, PC, Cx)
+    f("cgrid_random_normal_sp", None, PC, D)
     f("cgrid_fft", None, PC)
     f("cgrid_inverse_fft", None, PC)
     f("cgrid_inverse_fft_norm", None, PC)
