@@ -90,4 +90,5 @@ def test_seed_reproducibility(b200):
     assert not np.array_equal(outs[0], outs[2])
     # two calls are two independent streams: the sum has twice the variance
     n = np.prod(SHAPE)
-    _close(outs[0].var(), 2.0 / 3, 2.0 / 3 * np.sqrt(0.8 / n))
+    # (triangular distribution: excess kurtosis -0.6)
+    _close(outs[0].var(), 2.0 / 3, 2.0 / 3 * np.sqrt(1.4 / n))
