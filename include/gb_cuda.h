@@ -306,7 +306,8 @@ typedef struct gb_batch gb_batch;
 gb_batch *gb_batch_create(const gb_batch_item *items, int n);
 /* `steps` steps of every instance, asynchronous on the library stream. */
 int gb_batch_step(gb_batch *b, int steps);
-/* CTA size the autotuner chose (0 before the first call of >= 7 steps). */
+/* Plan the autotuner chose: the persistent launch's CTA size (128, 256,
+ * 512), -1 for the per-class graph, 0 before the first call of >= 9 steps. */
 int gb_batch_threads(const gb_batch *b);
 /* Status of the launch's bounded grid barrier (0 = no wait gave up). */
 int gb_batch_error_flag(gb_batch *b, int reset);

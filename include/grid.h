@@ -368,7 +368,8 @@ typedef struct grid_wf_batch grid_wf_batch;
 grid_wf_batch *grid_wf_batch_alloc(wf **wfs, cgrid **potentials, INT n, REAL complex time);
 void grid_wf_batch_propagate(grid_wf_batch *b, INT steps);
 void grid_wf_batch_free(grid_wf_batch *b);
-/* CTA size the batch autotuner chose (0 until a call of >= 7 steps). */
+/* Plan the batch autotuner chose: persistent CTA size (128, 256, 512), -1
+ * for the per-class CUDA graph, 0 until a call of >= 9 steps. */
 int grid_wf_batch_threads(grid_wf_batch *b);
 
 #ifdef __cplusplus

@@ -11,9 +11,11 @@
 // separates the passes.  The barrier is this file's own (atomic arrival
 // counter + generation word) with a bounded wait: a CTA that waits too long
 // sets the batch's error flag and leaves, so the launch always ends.
-// A small autotuner picks the CTA size (128, 256 or 512 threads) per batch
-// by timing each on the first steps of the first call; all sizes compute the
-// same values.
+// A second plan steps each shape class with the specialised pass kernels
+// (instance as a grid dimension), one stream per class, one step captured as
+// a CUDA graph.  A small autotuner picks the plan (persistent with 128, 256
+// or 512-thread CTAs, or per-class graph) per batch by timing each on the
+// first steps of the first call; all plans compute the same values.
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
@@ -206,6 +208,88 @@ template <typename T, int THREADS> constexpr size_t batch_smem() {
 
 }  // namespace gbfft
 
+namespace gbfft {
+
+// Per-shape-class kernels: every instance of a class has the same (ny, nz),
+// so a pass of the class is one launch of the specialised pass kernel with
+// the instance as the second grid dimension, in the CTA shapes of the
+// single-grid passes.
+template <typename T, int N, int... Ops>
+__global__ void __launch_bounds__(ContigCfg<N, sizeof(T)>::THREADS, ContigCfg<N, sizeof(T)>::MINB)
+    k_bclass_contig(const BatchInst *inst) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  batch_tile_contig<T, N, ContigCfg<N, sizeof(T)>::THREADS, Ops...>(inst[blockIdx.y], blockIdx.x, smraw);
+}
+
+template <typename T, int N, int... Ops>
+__global__ void __launch_bounds__(StridedCfg<N, sizeof(T)>::THREADS,
+                                  pass_min_blocks<StridedCfg<N, sizeof(T)>::THREADS, sizeof(T)>())
+    k_bclass_strided(const BatchInst *inst) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  batch_tile_strided<T, N, StridedCfg<N, sizeof(T)>::THREADS, Ops...>(inst[blockIdx.y], blockIdx.x, smraw);
+}
+
+template <typename T, int N, int... Ops>
+int launch_bclass_contig(const BatchInst *d, int ninst, long lines, cudaStream_t st) {
+  using T2 = C2<T>;
+  using Cfg = ContigCfg<N, sizeof(T)>;
+  constexpr size_t STAGE = has_pot(OpL<Ops...>{}) ? (size_t) Cfg::P * sizeof(T) : 0;
+  constexpr size_t SM = (size_t) Cfg::L * Cfg::LINE * sizeof(T2) + STAGE * Cfg::THREADS;
+  auto k = k_bclass_contig<T, N, Ops...>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) SM);
+    attr = true;
+  }
+  k<<<dim3((unsigned) (lines / Cfg::L), (unsigned) ninst), Cfg::THREADS, SM, st>>>(d);
+  GB_CHECK_LAUNCH("batch class pass");
+  return 0;
+}
+
+template <typename T, int N, int... Ops>
+int launch_bclass_strided(const BatchInst *d, int ninst, long inner, cudaStream_t st) {
+  using T2 = C2<T>;
+  using Cfg = StridedCfg<N, sizeof(T)>;
+  constexpr size_t SM = (size_t) N * Cfg::BZ * sizeof(T2);
+  auto k = k_bclass_strided<T, N, Ops...>;
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) SM);
+    attr = true;
+  }
+  k<<<dim3((unsigned) (inner / Cfg::BZ), (unsigned) ninst), Cfg::THREADS, SM, st>>>(d);
+  GB_CHECK_LAUNCH("batch class pass");
+  return 0;
+}
+
+// Pass ps (0..4 of the 2-D step) of one shape class.
+template <typename T, int N>
+int bclass_contig_pass(int ps, const BatchInst *d, int ninst, long ny, cudaStream_t st) {
+  if (ps == 0) return launch_bclass_contig<T, N, OP_FWD>(d, ninst, ny, st);
+  if (ps == 2) return launch_bclass_contig<T, N, OP_INV, OP_POT, OP_FWD>(d, ninst, ny, st);
+  return launch_bclass_contig<T, N, OP_INV>(d, ninst, ny, st);
+}
+
+template <typename T>
+int bclass_pass(int ps, const BatchInst *d, int ninst, long ny, long nz, cudaStream_t st) {
+  if ((ps & 1) == 0) {
+    switch (nz) {
+      case 64: return bclass_contig_pass<T, 64>(ps, d, ninst, ny, st);
+      case 128: return bclass_contig_pass<T, 128>(ps, d, ninst, ny, st);
+      case 256: return bclass_contig_pass<T, 256>(ps, d, ninst, ny, st);
+      default: return bclass_contig_pass<T, 512>(ps, d, ninst, ny, st);
+    }
+  }
+  switch (ny) {
+    case 64: return launch_bclass_strided<T, 64, OP_FWD, OP_KIN, OP_INV>(d, ninst, nz, st);
+    case 128: return launch_bclass_strided<T, 128, OP_FWD, OP_KIN, OP_INV>(d, ninst, nz, st);
+    case 256: return launch_bclass_strided<T, 256, OP_FWD, OP_KIN, OP_INV>(d, ninst, nz, st);
+    default: return launch_bclass_strided<T, 512, OP_FWD, OP_KIN, OP_INV>(d, ninst, nz, st);
+  }
+}
+
+}  // namespace gbfft
+
 // ------------------------------------------------------------------ host
 
 using namespace gbfft;
@@ -219,7 +303,16 @@ struct gb_batch {
   unsigned *d_bar;
   int *d_err;
   int grid[3];
-  int threads;  // chosen CTA size, 0 until tuned
+  int threads;  // chosen plan: persistent CTA size, -1 for the class graph, 0 until tuned
+  // per-shape-class plan: instances ordered by class, one stream per class,
+  // one step captured as a graph
+  BatchInst *d_cinst;
+  int ncls;
+  int cls_off[16], cls_n[16];
+  long cls_ny[16], cls_nz[16];
+  cudaStream_t cls_st[16];
+  cudaEvent_t ev_fork, ev_join[16];
+  cudaGraphExec_t graph;
 };
 
 static bool batch_len_ok(long v) { return v == 64 || v == 128 || v == 256 || v == 512; }
@@ -355,6 +448,30 @@ extern "C" gb_batch *gb_batch_create(const gb_batch_item *items, int n) {
     bi.ny = (int) it.g.ny;
   }
   cudaMemcpyAsync(b->d_inst, hi.data(), sizeof(BatchInst) * n, cudaMemcpyHostToDevice, st);
+  // shape classes for the per-class plan
+  {
+    std::vector<BatchInst> ci;
+    for (int sy = 64; sy <= 512; sy *= 2)
+      for (int sz = 64; sz <= 512; sz *= 2) {
+        const int off = (int) ci.size();
+        for (int i = 0; i < n; i++)
+          if (hi[i].ny == sy && hi[i].nz == sz) ci.push_back(hi[i]);
+        if ((int) ci.size() > off) {
+          b->cls_off[b->ncls] = off;
+          b->cls_n[b->ncls] = (int) ci.size() - off;
+          b->cls_ny[b->ncls] = sy;
+          b->cls_nz[b->ncls] = sz;
+          b->ncls++;
+        }
+      }
+    if (cudaMalloc(&b->d_cinst, sizeof(BatchInst) * n) != cudaSuccess) {
+      cudaGetLastError();
+      gb__set_error(2, "batch: cudaMalloc");
+      gb_batch_free(b);
+      return nullptr;
+    }
+    cudaMemcpy(b->d_cinst, ci.data(), sizeof(BatchInst) * n, cudaMemcpyHostToDevice);
+  }
   // tile lists for the CTA sizes
   for (int v = 0; v < 3; v++) {
     std::vector<BatchTile> ct, stl;
@@ -388,24 +505,72 @@ extern "C" gb_batch *gb_batch_create(const gb_batch_item *items, int n) {
   return b;
 }
 
-// Steps of every instance.  The first call with at least seven steps times
-// one step with each CTA size (after one warm-up step each) and keeps the
-// fastest; those six steps count as steps of the run.
+// The per-class plan: one step of every class on its own stream (forked from
+// and joined back into the library stream), captured once as a graph.
+template <typename T> static int batch_capture(gb_batch *b) {
+  cudaStream_t main = gb__stream();
+  if (!b->cls_st[0]) {
+    for (int c = 0; c < b->ncls; c++) {
+      cudaStreamCreateWithFlags(&b->cls_st[c], cudaStreamNonBlocking);
+      cudaEventCreateWithFlags(&b->ev_join[c], cudaEventDisableTiming);
+    }
+    cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+  }
+  if (cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+    return gb__set_error(1043, "batch: stream capture");
+  int rc = 0;
+  cudaEventRecord(b->ev_fork, main);
+  for (int c = 0; c < b->ncls && !rc; c++) {
+    cudaStream_t sc = b->cls_st[c];
+    cudaStreamWaitEvent(sc, b->ev_fork, 0);
+    for (int ps = 0; ps < 5 && !rc; ps++)
+      rc = bclass_pass<T>(ps, b->d_cinst + b->cls_off[c], b->cls_n[c], b->cls_ny[c], b->cls_nz[c], sc);
+    cudaEventRecord(b->ev_join[c], sc);
+    cudaStreamWaitEvent(main, b->ev_join[c], 0);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(main, &g);
+  if (rc || e != cudaSuccess || !g) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return rc ? rc : gb__set_error((int) e, "batch: stream capture");
+  }
+  const cudaError_t ei = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (ei != cudaSuccess) return gb__set_error((int) ei, "batch: graph instantiate");
+  return 0;
+}
+
+static int batch_run_classes(gb_batch *b, int steps) {
+  if (!b->graph) GB_TRYC(b->prec == GB_FP32 ? batch_capture<float>(b) : batch_capture<double>(b));
+  for (int s = 0; s < steps; s++) {
+    const cudaError_t e = cudaGraphLaunch(b->graph, gb__stream());
+    if (e != cudaSuccess) return gb__set_error((int) e, "batch: graph launch");
+    for (int k = 0; k < 5 * b->ncls; k++) gb__count_launch();
+  }
+  return 0;
+}
+
+// Steps of every instance.  The first call with at least nine steps times
+// one step of each plan (the persistent launch with 128, 256 and 512-thread
+// CTAs, and the per-class graph), each after one warm-up step, and keeps
+// the fastest; those eight steps count as steps of the run.  Every plan
+// computes the same values.
 extern "C" int gb_batch_step(gb_batch *b, int steps) {
   if (!b) return gb__set_error(1040, "batch: null");
   if (steps <= 0) return 0;
   if (!b->threads) {
-    if (steps < 7) return batch_run(b, steps, 1);
+    if (steps < 9) return batch_run(b, steps, 1);
     cudaEvent_t e[2];
     cudaEventCreate(&e[0]);
     cudaEventCreate(&e[1]);
     cudaStream_t st = gb__stream();
     float best = 0.f;
     int bv = 1;
-    for (int v = 0; v < 3; v++) {
-      GB_TRYC(batch_run(b, 1, v));
+    for (int v = 0; v < 4; v++) {
+      GB_TRYC(v < 3 ? batch_run(b, 1, v) : batch_run_classes(b, 1));
       cudaEventRecord(e[0], st);
-      GB_TRYC(batch_run(b, 1, v));
+      GB_TRYC(v < 3 ? batch_run(b, 1, v) : batch_run_classes(b, 1));
       cudaEventRecord(e[1], st);
       cudaEventSynchronize(e[1]);
       float ms = 0.f;
@@ -417,9 +582,10 @@ extern "C" int gb_batch_step(gb_batch *b, int steps) {
     }
     cudaEventDestroy(e[0]);
     cudaEventDestroy(e[1]);
-    b->threads = kBatchThreads[bv];
-    steps -= 6;
+    b->threads = bv < 3 ? kBatchThreads[bv] : -1;
+    steps -= 8;
   }
+  if (b->threads < 0) return batch_run_classes(b, steps);
   return batch_run(b, steps, b->threads == 128 ? 0 : (b->threads == 256 ? 1 : 2));
 }
 
@@ -443,5 +609,12 @@ extern "C" void gb_batch_free(gb_batch *b) {
   cudaFree(b->d_kin);
   cudaFree(b->d_bar);
   cudaFree(b->d_err);
+  cudaFree(b->d_cinst);
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (int c = 0; c < b->ncls; c++) {
+    if (b->cls_st[c]) cudaStreamDestroy(b->cls_st[c]);
+    if (b->ev_join[c]) cudaEventDestroy(b->ev_join[c]);
+  }
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
   free(b);
 }
