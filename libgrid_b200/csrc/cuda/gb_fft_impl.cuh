@@ -134,7 +134,7 @@ template <> struct Sched<32> { static constexpr int P = 8; using R = IL<8, 4>; }
 template <> struct Sched<64> { static constexpr int P = 8; using R = IL<8, 8>; };
 template <> struct Sched<128> { static constexpr int P = 16; using R = IL<16, 8>; };
 template <> struct Sched<256> { static constexpr int P = 16; using R = IL<16, 16>; };
-template <> struct Sched<512> { static constexpr int P = 8; using R = IL<8, 8, 8>; };
+template <> struct Sched<512> { static constexpr int P = 16; using R = IL<16, 16, 2>; };
 template <> struct Sched<1024> { static constexpr int P = 16; using R = IL<16, 16, 4>; };
 template <> struct Sched<2048> { static constexpr int P = 16; using R = IL<16, 16, 8>; };
 template <> struct Sched<4096> { static constexpr int P = 16; using R = IL<16, 16, 16>; };
