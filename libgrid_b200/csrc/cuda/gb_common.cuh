@@ -96,8 +96,9 @@ __device__ __forceinline__ double2 gb_sincos_series(double r) {
   return double2{fma(r * s2, ps, r), fma(s2, pc, 1.0)};
 }
 
-// (sin x, cos x) for |x| <= 1e7.
-__device__ __forceinline__ double2 gb_sincos_reduced(double x) {
+// (sin x, cos x) for |x| <= 1e7; out of line (with the library fallback it
+// serves the rare large phases), so the unrolled element loops stay small.
+static __device__ __noinline__ double2 gb_sincos_reduced(double x) {
   const double n = rint(x * 0.6366197723675814);
   const int q = __double2int_rn(n);
   double r = fma(-n, 1.570796325802803, x);
