@@ -61,7 +61,10 @@ for _ax, _an in enumerate("xyz"):
     for _p, _pn in enumerate(["fwd", "inv", "fwd_kin_inv", "inv_pot_fwd", "other"]):
         KIND_NAMES[5 * _ax + _p] = "%s_%s" % (_an, _pn)
     KIND_NAMES[15 + _ax] = "cn_%s" % _an
-NUM_KINDS = 18
+# plane-chained passes (z then y, y then z, plane by plane in one launch)
+KIND_NAMES[18] = "zy_fwd_chain"
+KIND_NAMES[20] = "yz_inv_chain"
+NUM_KINDS = 21
 
 
 def measured_traffic(kind, n):

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "gb_fft_impl.cuh"
+#include "gb_plane.cuh"
 #include "gb_internal_cuda.h"
 
 namespace gbfft {
@@ -61,6 +62,48 @@ int pass(const gb_geom *g, int axis, const void *src, void *dst, PassArgs a, OpL
   return rc;
 }
 
+// Plane-chained passes (gb_plane.cuh) for grids whose y and z lines are
+// 256 long.  The chain counters live in a scratch slot (stages x planes + 1
+// ints).
+constexpr int kPlaneN = 256;
+int plane_enabled();
+
+template <typename T> bool plane_ok(const gb_geom *g) {
+  return plane_enabled() && g->nx >= 2 && g->ny == kPlaneN && g->nz == kPlaneN;
+}
+
+// Timing kinds of the chains: 18 [z FWD, y FWD], 20 [y INV, z INV].
+template <typename T, class... Stages>
+int plane_chain(const gb_geom *g, void *psi, const PassArgs &a, int kind, Stages...) {
+  ChainArgs c;
+  memset(&c, 0, sizeof(c));
+  c.ay = a;
+  c.az = a;
+  c.ay.axis = 1;
+  c.az.axis = 2;
+  c.ay.tw = c.az.tw = gb__twiddles(kPlaneN, g->prec);
+  if (!c.ay.tw) return gb_last_error();
+  c.ay.errflag = c.az.errflag = gb__pass_errflag();
+  if (!c.ay.errflag) return gb_last_error();
+  int *cnt = (int *) gb__scratch(GB_SCR_CHAIN, sizeof(int) * (size_t) (3 * g->nx + 1));
+  if (!cnt) return gb_last_error();
+  const int slot = gb__pass_begin(kind);
+  const int rc = launch_chain<T, kPlaneN, Stages...>(psi, g->nx, c, cnt);
+  gb__pass_end(slot);
+  return rc;
+}
+
+// The middle of the step, y INV | z INV.V.FWD | y FWD, stays three line
+// passes: chained, its z stage (two transforms and the phase) is too heavy
+// in registers and arithmetic for the chain to gain.
+template <typename T> int plane_mid(const gb_geom *g, void *psi, const PassArgs &a, bool has_pot) {
+  int rc = pass<T>(g, 1, psi, psi, a, OpL<OP_INV>{});
+  if (!rc) rc = has_pot ? pass<T>(g, 2, psi, psi, a, OpL<OP_INV, OP_POT, OP_FWD>{})
+                        : pass<T>(g, 2, psi, psi, a, OpL<OP_INV, OP_FWD>{});
+  if (!rc) rc = pass<T>(g, 1, psi, psi, a, OpL<OP_FWD>{});
+  return rc;
+}
+
 #define GB_TRY(x)               \
   do {                          \
     int rc_ = (x);              \
@@ -114,6 +157,14 @@ int gb__split_step_t(void *psi, const gb_geom *g, const gb_kinetic *kin, const g
     if (has_pot)
       return pass<T>(g, ax[0], psi, psi, a, OpL<OP_FWD, OP_KIN, OP_INV, OP_POT, OP_FWD, OP_KIN, OP_INV>{});
     return pass<T>(g, ax[0], psi, psi, a, OpL<OP_FWD, OP_KIN, OP_INV, OP_FWD, OP_KIN, OP_INV>{});
+  }
+  if (na == 3 && plane_ok<T>(g)) {
+    // seven launches: [z FWD, y FWD] | x FWD.K.INV | y INV | z INV.V.FWD | y FWD | x FWD.K.INV | [y INV, z INV]
+    GB_TRY((plane_chain<T>(g, psi, a, 18, Stage<2, OP_FWD>{}, Stage<1, OP_FWD>{})));
+    GB_TRY((pass<T>(g, 0, psi, psi, a, OpL<OP_FWD, OP_KIN, OP_INV>{})));
+    GB_TRY(plane_mid<T>(g, psi, a, has_pot));
+    GB_TRY((pass<T>(g, 0, psi, psi, a, OpL<OP_FWD, OP_KIN, OP_INV>{})));
+    return plane_chain<T>(g, psi, a, 20, Stage<1, OP_INV>{}, Stage<2, OP_INV>{});
   }
   const int last = ax[na - 1];
   // forward along all but the outermost axis
@@ -176,6 +227,17 @@ int gb__split_steps_t(void *psi, const gb_geom *g, const gb_kinetic *kin, const 
   af.ksq[0] = fsq;
   af.ksq[1] = fsq + g->nx;
   af.ksq[2] = fsq + g->nx + g->ny;
+  if (na == 3 && plane_ok<T>(g)) {
+    // steady state as before (x FWD.K(dt).INV | y INV | z INV.V.FWD | y FWD), with the
+    // leading and trailing transform pairs chained
+    GB_TRY((plane_chain<T>(g, psi, ah, 18, Stage<2, OP_FWD>{}, Stage<1, OP_FWD>{})));
+    for (int st = 0; st < nsteps; st++) {
+      GB_TRY((pass<T>(g, 0, psi, psi, st == 0 ? ah : af, OpL<OP_FWD, OP_KIN, OP_INV>{})));
+      GB_TRY(plane_mid<T>(g, psi, ah, has_pot));
+    }
+    GB_TRY((pass<T>(g, 0, psi, psi, ah, OpL<OP_FWD, OP_KIN, OP_INV>{})));
+    return plane_chain<T>(g, psi, ah, 20, Stage<1, OP_INV>{}, Stage<2, OP_INV>{});
+  }
   const int last = ax[na - 1];
   for (int s = 0; s < na - 1; s++) GB_TRY((pass<T>(g, ax[s], psi, psi, ah, OpL<OP_FWD>{})));
   for (int st = 0; st < nsteps; st++) {

@@ -15,6 +15,7 @@ enum {
   GB_SCR_WORK = 4,     // temporary full grids
   GB_SCR_STAGE = 5,    // precision-conversion staging
   GB_SCR_KIN2 = 6,     // kinetic factor tables of the merged K(dt) pass
+  GB_SCR_CHAIN = 7,    // tile counters and ticket of the plane-chained passes
   GB_SCR_COUNT = 8
 };
 

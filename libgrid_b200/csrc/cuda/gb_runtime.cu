@@ -305,6 +305,16 @@ extern "C" int gb_pass_pipeline(int on) {
   return old;
 }
 
+static int g_plane_on = 1;
+namespace gbfft {
+int plane_enabled() { return g_plane_on; }
+}  // namespace gbfft
+extern "C" int gb_plane_passes(int on) {
+  const int old = g_plane_on;
+  if (on >= 0) g_plane_on = on ? 1 : 0;
+  return old;
+}
+
 extern "C" int gb_pass_timing_report(double *ms, long *count, int nkinds) {
   for (int k = 0; k < nkinds; k++) {
     ms[k] = 0.0;

@@ -1,0 +1,133 @@
+"""Plane-chained passes (the leading z FWD + y FWD and the trailing y INV +
+z INV of a split step, each one persistent launch working plane by plane
+with per-plane completion counters) against the nine-pass schedule and the
+oracle.  Both schedules run the same per-line arithmetic in the same order,
+so they agree to the last bit up to contraction differences (<= 1e-15
+relative L2; FP32 <= 1e-7)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import rel
+from libgrid_b200 import capi, workloads
+
+pytestmark = pytest.mark.gpu
+
+PER, FFT2 = capi.WF_PERIODIC_BOUNDARY, capi.WF_2ND_ORDER_FFT
+
+
+def _lib(b200):
+    lib = b200.lib
+    lib.gb_plane_passes.argtypes = [C.c_int]
+    lib.gb_plane_passes.restype = C.c_int
+    return lib
+
+
+def _run(b200, shape, prec, time, steps=3, multi=False, g=0.0025, kind="gp"):
+    step = 0.5
+    mass = 4.0 / workloads.GRID_AUTOAMU
+    psi0, v = workloads.gp_wells(shape, step, g, seed=37)
+    w = b200.wf(*shape, step, mass, PER, FFT2, values=psi0)
+    if prec:
+        w.precision(prec)
+    if kind == "gp":
+        pot = b200.rgrid(*shape, step, values=v)
+        if multi:
+            w.propagate_gp_n(pot, g, time, steps)
+        else:
+            for _ in range(steps):
+                w.propagate_gp(pot, g, time)
+    elif kind == "complex":
+        rng = np.random.default_rng(5)
+        vc = v + 0.01j * rng.standard_normal(shape)
+        pot = b200.cgrid(*shape, step, values=vc)
+        for _ in range(steps):
+            w.propagate(pot, time)
+        v = vc
+    else:
+        pot = None
+        if multi:
+            w.propagate_n(None, time, steps)
+        else:
+            for _ in range(steps):
+                w.propagate(None, time)
+    out = w.grid.get()
+    b200.free(w)
+    if pot is not None:
+        b200.free(pot)
+    return out, psi0, v
+
+
+def _both(b200, *args, **kw):
+    lib = _lib(b200)
+    old = lib.gb_plane_passes(0)
+    try:
+        nine, psi0, v = _run(b200, *args, **kw)
+        lib.gb_plane_passes(1)
+        plane, _, _ = _run(b200, *args, **kw)
+    finally:
+        lib.gb_plane_passes(old)
+    return plane, nine, psi0, v
+
+
+@pytest.mark.parametrize("shape", [(2, 256, 256), (16, 256, 256)])
+@pytest.mark.parametrize("time", [1.0, -1.0j])
+@pytest.mark.parametrize("prec", [0, capi.GRID_PREC_FP32])
+def test_plane_matches_nine_pass(b200, shape, time, prec):
+    plane, nine, _, _ = _both(b200, shape, prec, time)
+    assert rel(plane, nine) <= (1e-15 if not prec else 1e-7)
+
+
+@pytest.mark.parametrize("kind", ["free", "complex"])
+def test_plane_other_programs(b200, kind):
+    plane, nine, _, _ = _both(b200, (4, 256, 256), 0, 1.0, kind=kind)
+    assert rel(plane, nine) <= 1e-15
+
+
+@pytest.mark.parametrize("kind", ["gp", "free"])
+@pytest.mark.parametrize("prec", [0, capi.GRID_PREC_FP32])
+def test_plane_multistep(b200, kind, prec):
+    plane, nine, _, _ = _both(b200, (8, 256, 256), prec, 1.0, steps=7, multi=True, kind=kind)
+    assert rel(plane, nine) <= (1e-15 if not prec else 1e-7)
+
+
+def test_plane_against_oracle(b200, restate):
+    lib = _lib(b200)
+    old = lib.gb_plane_passes(1)
+    try:
+        got, psi0, v = _run(b200, (4, 256, 256), 0, 1.0, steps=2)
+    finally:
+        lib.gb_plane_passes(old)
+    want = psi0.copy()
+    vr = workloads.padded(v)
+    for _ in range(2):
+        want = restate.fft_step(want, 0.5, 4.0 / workloads.GRID_AUTOAMU, 1.0, vr=vr, g=0.0025)
+    assert rel(got, want) < 1e-11
+
+
+def test_plane_timing_kinds(b200):
+    """A chained step runs seven launches: the two chains (kinds 18 and 20),
+    the x FWD.K.INV pass twice and the middle y INV | z INV.V.FWD | y FWD;
+    the pass error flag stays clear."""
+    lib = _lib(b200)
+    lib.gb_pass_timing.argtypes = [C.c_int]
+    lib.gb_pass_timing_report.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_long), C.c_int]
+    lib.gb_pass_error_flag.argtypes = [C.c_int]
+    lib.gb_pass_error_flag.restype = C.c_int
+    old = lib.gb_plane_passes(1)
+    try:
+        lib.gb_pass_timing(1)
+        _run(b200, (4, 256, 256), 0, 1.0, steps=1)
+        ms = (C.c_double * 21)()
+        cnt = (C.c_long * 21)()
+        lib.gb_pass_timing_report(ms, cnt, 21)
+        lib.gb_pass_timing(0)
+    finally:
+        lib.gb_plane_passes(old)
+    counts = list(cnt)
+    assert counts[18] == 1 and counts[20] == 1
+    assert counts[2] == 2  # x FWD.K.INV
+    assert counts[6] == 1 and counts[13] == 1 and counts[5] == 1  # y INV, z INV.V.FWD, y FWD
+    assert sum(counts) == 7
+    assert lib.gb_pass_error_flag(1) == 0
