@@ -183,34 +183,6 @@ extern "C" cudaStream_t gb__stream(void);
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned) __cvta_generic_to_shared(p); }
 
-// Thread-block clusters: rank of this CTA, distributed shared memory
-// (mapa + ld.shared::cluster) and the cluster-wide barrier (all threads of
-// all CTAs of the cluster; release/acquire orders shared-memory writes
-// before the barrier against reads after it).
-__device__ __forceinline__ unsigned cluster_rank() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-  return r;
-}
-__device__ __forceinline__ unsigned cluster_map(const void *local, unsigned rank) {
-  unsigned r;
-  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(smem_u32(local)), "r"(rank));
-  return r;
-}
-__device__ __forceinline__ double2 dsmem_ld(unsigned addr, double2) {
-  double2 v;
-  asm volatile("ld.shared::cluster.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "r"(addr) : "memory");
-  return v;
-}
-__device__ __forceinline__ float2 dsmem_ld(unsigned addr, float2) {
-  float2 v;
-  asm volatile("ld.shared::cluster.v2.f32 {%0, %1}, [%2];" : "=f"(v.x), "=f"(v.y) : "r"(addr) : "memory");
-  return v;
-}
-__device__ __forceinline__ void cluster_sync_all() {
-  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
-}
-
 // Per-thread asynchronous global -> shared copy of one 4- or 8-byte element
 // (both addresses naturally aligned); completion is awaited by the issuing
 // thread with cp_async_wait_all().

@@ -92,6 +92,16 @@ def test_plane_multistep(b200, kind, prec):
     assert rel(plane, nine) <= (1e-15 if not prec else 1e-7)
 
 
+@pytest.mark.parametrize("prec", [0, capi.GRID_PREC_FP32])
+def test_plane_chains_full_size(b200, prec):
+    """The 256^3 workload: 256 planes per chain, two steps and a multi-step
+    call, bit for bit against the nine-pass schedule."""
+    plane, nine, _, _ = _both(b200, (256, 256, 256), prec, 1.0, steps=2)
+    assert rel(plane, nine) <= (1e-15 if not prec else 1e-7)
+    plane, nine, _, _ = _both(b200, (256, 256, 256), prec, -1.0j, steps=4, multi=True)
+    assert rel(plane, nine) <= (1e-15 if not prec else 1e-7)
+
+
 def test_plane_against_oracle(b200, restate):
     lib = _lib(b200)
     old = lib.gb_plane_passes(1)
