@@ -63,6 +63,7 @@ for _ax, _an in enumerate("xyz"):
     KIND_NAMES[15 + _ax] = "cn_%s" % _an
 # plane-chained passes (z then y, y then z, plane by plane in one launch)
 KIND_NAMES[18] = "zy_fwd_chain"
+KIND_NAMES[19] = "z_inv_pot_fwd_y_fwd_chain"
 KIND_NAMES[20] = "yz_inv_chain"
 NUM_KINDS = 21
 
@@ -432,8 +433,10 @@ def run_b200(args, world, rank, local):
     # dominant kernel = largest total time among pass kinds
     dom = max(per_kind.items(), key=lambda kv: kv[1]["ms_total"])
     dom_ms = dom[1]["ms_total"] / dom[1]["launches"]
-    # the potential pass also reads the real V_ext row (8 B/pt in FP64)
-    dom_bytes = (BYTES_PER_POINT_PASS + (8 if dom[0].endswith("inv_pot_fwd") else 0)) * N
+    # every pass and every chained launch reads and writes psi once (32 B/pt);
+    # the potential pass and the chain that carries it also read the real
+    # V_ext row (8 B/pt in FP64)
+    dom_bytes = (BYTES_PER_POINT_PASS + (8 if "pot" in dom[0] else 0)) * N
     traffic = measured_traffic(dom[0], n)
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     step_gbs = BYTES_PER_POINT_STEP * N / (step_ms * 1e-3) / 1e9

@@ -94,8 +94,9 @@ float gb_event_elapsed_ms(int start_slot, int stop_slot);
  * stream (benchmark instrumentation).  Kinds are 5 * axis + program with
  * axis 0 x, 1 y, 2 z and program 0 forward FFT, 1 inverse FFT,
  * 2 forward + kinetic + inverse, 3 inverse + potential + forward, 4 other;
- * kinds 15 + axis are the Crank-Nicolson line sweeps; kinds 18 and 20 the
- * plane-chained passes [z FWD, y FWD] and [y INV, z INV].
+ * kinds 15 + axis are the Crank-Nicolson line sweeps; kinds 18, 19 and 20
+ * the plane-chained passes [z FWD, y FWD], [z INV.V.FWD, y FWD] (FP64) and
+ * [y INV, z INV].
  * report() fills ms[k] / count[k] for k < nkinds and returns the number of
  * timed passes. */
 int gb_pass_timing(int on);
@@ -116,9 +117,10 @@ int gb_pass_error_flag(int reset);
  * setting.  Both forms compute the same values.  (No reference counterpart.) */
 int gb_pass_pipeline(int on);
 /* Plane-chained passes: the leading z FWD + y FWD and the trailing
- * y INV + z INV transforms of a split-operator step each run as one
- * persistent launch that works plane by plane, so the intermediate result
- * stays in L2 (grids with nx >= 2 and ny = nz = 256).  on = 1 enables (the
+ * y INV + z INV transforms of a split-operator step (in FP64 also the
+ * potential pass with the y FWD after it) each run as one persistent launch
+ * that works plane by plane, so the intermediate result stays in L2 (grids
+ * with nx >= 2 and ny = nz = 256).  on = 1 enables (the
  * default), 0 disables, -1 only queries; returns the previous setting.  Both
  * schedules compute the same values.  (No reference counterpart.) */
 int gb_plane_passes(int on);

@@ -72,7 +72,8 @@ template <typename T> bool plane_ok(const gb_geom *g) {
   return plane_enabled() && g->nx >= 2 && g->ny == kPlaneN && g->nz == kPlaneN;
 }
 
-// Timing kinds of the chains: 18 [z FWD, y FWD], 20 [y INV, z INV].
+// Timing kinds of the chains: 18 [z FWD, y FWD], 19 [z INV.V.FWD (or
+// INV.FWD), y FWD], 20 [y INV, z INV].
 template <typename T, class... Stages>
 int plane_chain(const gb_geom *g, void *psi, const PassArgs &a, int kind, Stages...) {
   ChainArgs c;
@@ -93,15 +94,21 @@ int plane_chain(const gb_geom *g, void *psi, const PassArgs &a, int kind, Stages
   return rc;
 }
 
-// The middle of the step, y INV | z INV.V.FWD | y FWD, stays three line
-// passes: chained, its z stage (two transforms and the phase) is too heavy
-// in registers and arithmetic for the chain to gain.
+// The middle of the step, y INV | z INV.V.FWD | y FWD.  In FP64 the last
+// two run as one chain (the potential stage at 3 CTAs per SM); in FP32 the
+// chain is slower than the two passes, and all three stay line passes.
 template <typename T> int plane_mid(const gb_geom *g, void *psi, const PassArgs &a, bool has_pot) {
   int rc = pass<T>(g, 1, psi, psi, a, OpL<OP_INV>{});
-  if (!rc) rc = has_pot ? pass<T>(g, 2, psi, psi, a, OpL<OP_INV, OP_POT, OP_FWD>{})
-                        : pass<T>(g, 2, psi, psi, a, OpL<OP_INV, OP_FWD>{});
-  if (!rc) rc = pass<T>(g, 1, psi, psi, a, OpL<OP_FWD>{});
-  return rc;
+  if (rc) return rc;
+  if constexpr (sizeof(T) == 8) {
+    return has_pot ? plane_chain<T>(g, psi, a, 19, Stage<2, OP_INV, OP_POT, OP_FWD>{}, Stage<1, OP_FWD>{})
+                   : plane_chain<T>(g, psi, a, 19, Stage<2, OP_INV, OP_FWD>{}, Stage<1, OP_FWD>{});
+  } else {
+    rc = has_pot ? pass<T>(g, 2, psi, psi, a, OpL<OP_INV, OP_POT, OP_FWD>{})
+                 : pass<T>(g, 2, psi, psi, a, OpL<OP_INV, OP_FWD>{});
+    if (!rc) rc = pass<T>(g, 1, psi, psi, a, OpL<OP_FWD>{});
+    return rc;
+  }
 }
 
 #define GB_TRY(x)               \
@@ -159,7 +166,8 @@ int gb__split_step_t(void *psi, const gb_geom *g, const gb_kinetic *kin, const g
     return pass<T>(g, ax[0], psi, psi, a, OpL<OP_FWD, OP_KIN, OP_INV, OP_FWD, OP_KIN, OP_INV>{});
   }
   if (na == 3 && plane_ok<T>(g)) {
-    // seven launches: [z FWD, y FWD] | x FWD.K.INV | y INV | z INV.V.FWD | y FWD | x FWD.K.INV | [y INV, z INV]
+    // [z FWD, y FWD] | x FWD.K.INV | y INV | [z INV.V.FWD, y FWD] (FP64; FP32: two passes) | x FWD.K.INV |
+    // [y INV, z INV]
     GB_TRY((plane_chain<T>(g, psi, a, 18, Stage<2, OP_FWD>{}, Stage<1, OP_FWD>{})));
     GB_TRY((pass<T>(g, 0, psi, psi, a, OpL<OP_FWD, OP_KIN, OP_INV>{})));
     GB_TRY(plane_mid<T>(g, psi, a, has_pot));
@@ -228,8 +236,8 @@ int gb__split_steps_t(void *psi, const gb_geom *g, const gb_kinetic *kin, const 
   af.ksq[1] = fsq + g->nx;
   af.ksq[2] = fsq + g->nx + g->ny;
   if (na == 3 && plane_ok<T>(g)) {
-    // steady state as before (x FWD.K(dt).INV | y INV | z INV.V.FWD | y FWD), with the
-    // leading and trailing transform pairs chained
+    // steady state x FWD.K(dt).INV | y INV | [z INV.V.FWD, y FWD] (FP64), with the leading
+    // and trailing transform pairs chained
     GB_TRY((plane_chain<T>(g, psi, ah, 18, Stage<2, OP_FWD>{}, Stage<1, OP_FWD>{})));
     for (int st = 0; st < nsteps; st++) {
       GB_TRY((pass<T>(g, 0, psi, psi, st == 0 ? ah : af, OpL<OP_FWD, OP_KIN, OP_INV>{})));

@@ -1,9 +1,9 @@
 // Plane-chained passes: one persistent launch runs a chain of line stages on
-// the y and z axes (z FWD then y FWD; y INV then z INV), plane by plane, so
-// a plane's intermediate result is read back from L2 by the next stage
-// instead of making a full HBM round trip: the chain reads and writes psi in
-// HBM once.  A split step runs
-//   [z FWD, y FWD] | x FWD.K.INV | y INV | z INV.V.FWD | y FWD | x FWD.K.INV | [y INV, z INV]
+// the y and z axes (z FWD then y FWD; y INV then z INV; in FP64 also
+// z INV.V.FWD then y FWD), plane by plane, so a plane's intermediate result
+// is read back from L2 by the next stage instead of making a full HBM round
+// trip: the chain reads and writes psi in HBM once.  An FP64 split step runs
+//   [z FWD, y FWD] | x FWD.K.INV | y INV | [z INV.V.FWD, y FWD] | x FWD.K.INV | [y INV, z INV]
 //
 // Work is a sequence of tickets drawn from a global counter.  Ticket group
 // g holds, for every stage s, the tiles of plane g - s * lag, so stage s of
@@ -105,8 +105,15 @@ __device__ __forceinline__ void chain_tile(Stage<AX, Ops...>, C2<T> *__restrict_
   }
 }
 
+// Resident CTAs per SM for the register bound: a chain whose stage carries
+// the potential op (two transforms and the phase) gets 3 in FP64, so it
+// does not spill.
+template <typename T, int N, class... Stages> constexpr int chain_minb() {
+  return (sizeof(T) == 8 && (stage_has_pot(Stages{}) || ...)) ? 3 : ChainCfg<T, N>::MINB;
+}
+
 template <typename T, int N, class... Stages>
-__global__ void __launch_bounds__(ChainCfg<T, N>::THREADS, ChainCfg<T, N>::MINB)
+__global__ void __launch_bounds__(ChainCfg<T, N>::THREADS, chain_minb<T, N, Stages...>())
     k_chain(C2<T> *__restrict__ psi, ChainArgs c) {
   using Cfg = ChainCfg<T, N>;
   constexpr int S = sizeof...(Stages);

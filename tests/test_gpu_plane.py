@@ -117,9 +117,9 @@ def test_plane_against_oracle(b200, restate):
 
 
 def test_plane_timing_kinds(b200):
-    """A chained step runs seven launches: the two chains (kinds 18 and 20),
-    the x FWD.K.INV pass twice and the middle y INV | z INV.V.FWD | y FWD;
-    the pass error flag stays clear."""
+    """A chained FP64 step runs six launches: the three chains (kinds 18, 19
+    and 20), the x FWD.K.INV pass twice and the y INV pass; the pass error
+    flag stays clear."""
     lib = _lib(b200)
     lib.gb_pass_timing.argtypes = [C.c_int]
     lib.gb_pass_timing_report.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_long), C.c_int]
@@ -136,8 +136,8 @@ def test_plane_timing_kinds(b200):
     finally:
         lib.gb_plane_passes(old)
     counts = list(cnt)
-    assert counts[18] == 1 and counts[20] == 1
+    assert counts[18] == 1 and counts[19] == 1 and counts[20] == 1
     assert counts[2] == 2  # x FWD.K.INV
-    assert counts[6] == 1 and counts[13] == 1 and counts[5] == 1  # y INV, z INV.V.FWD, y FWD
-    assert sum(counts) == 7
+    assert counts[6] == 1  # y INV
+    assert sum(counts) == 6
     assert lib.gb_pass_error_flag(1) == 0
