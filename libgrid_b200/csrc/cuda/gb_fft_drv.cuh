@@ -101,6 +101,10 @@ template <typename T> int plane_mid(const gb_geom *g, void *psi, const PassArgs 
   int rc = pass<T>(g, 1, psi, psi, a, OpL<OP_INV>{});
   if (rc) return rc;
   if constexpr (sizeof(T) == 8) {
+    // real-time steps with a real V_ext (the GP workload) get a chain built
+    // for that potential case alone
+    if (has_pot && a.pot.kind == GB_POT_REAL && !a.pot.absorb && a.pot.c_re == 0.0)
+      return plane_chain<T>(g, psi, a, 19, Stage<2, OP_INV, OP_POT_RP, OP_FWD>{}, Stage<1, OP_FWD>{});
     return has_pot ? plane_chain<T>(g, psi, a, 19, Stage<2, OP_INV, OP_POT, OP_FWD>{}, Stage<1, OP_FWD>{})
                    : plane_chain<T>(g, psi, a, 19, Stage<2, OP_INV, OP_FWD>{}, Stage<1, OP_FWD>{});
   } else {

@@ -32,7 +32,10 @@ int gb__tmap_lines(CUtensorMap *out, const void *base, long outer, long n, long 
 
 namespace gbfft {
 
-enum : int { OP_END = 0, OP_FWD = 1, OP_INV = 2, OP_KIN = 3, OP_POT = 4, OP_SCALE = 5, OP_KSQ = 6 };
+// OP_POT_RP is the potential op for one case only, a real V_ext in real
+// time without an absorbing region (a pure phase), so a kernel built for it
+// carries none of the other potential paths.
+enum : int { OP_END = 0, OP_FWD = 1, OP_INV = 2, OP_KIN = 3, OP_POT = 4, OP_SCALE = 5, OP_KSQ = 6, OP_POT_RP = 7 };
 
 template <int... Ops> struct OpL {};
 template <int... Rs> struct IL {};
@@ -375,7 +378,9 @@ __device__ __forceinline__ bool pot_prefetch(const PassArgs &a, unsigned o, unsi
   return true;
 }
 
-template <int... Ops> __host__ __device__ constexpr bool has_pot(OpL<Ops...>) { return ((Ops == OP_POT) || ...); }
+template <int... Ops> __host__ __device__ constexpr bool has_pot(OpL<Ops...>) {
+  return ((Ops == OP_POT || Ops == OP_POT_RP) || ...);
+}
 template <int... Ops> __host__ __device__ constexpr bool has_kin(OpL<Ops...>) { return ((Ops == OP_KIN) || ...); }
 
 template <int Op, int... Rest> struct OpsHead {
@@ -471,6 +476,21 @@ template <typename T, int N, class SM, int Op, int... Rest> struct Program<T, N,
           v[m] = pot_factor_apply<T>(v[m], i, j, k, vbase + (unsigned) p * vstride, a);
         }
       }
+    } else if constexpr (Op == OP_POT_RP) {
+      // real V_ext, real time, no absorber (the caller checked): the phase
+      // loop of the simple path only
+      int i0, j0, k0;
+      unsigned vbase, vstride;
+      pot_row(a, o, q, i0, j0, k0, vbase, vstride);
+      const T *vp = (const T *) a.pot.v + vbase;
+      unsigned vt = vstride, vm = TL * vstride;
+      if (vstage) {
+        cp_async_wait_all();
+        vp = (const T *) vstage;
+        vt = 0;
+        vm = (unsigned) vsstride;
+      }
+      pot_line_simple<T, P, TL, true, true>(v, t, vp, vt, vm, a.pot.cons, a.pot.g, a.pot.c_im);
     } else if constexpr (Op == OP_KSQ) {
       // sum |k|^2 |v|^2 with k from the unshifted frequency grid
       int i, j, k;

@@ -47,7 +47,7 @@ struct ChainArgs {
 };
 
 template <int AX, int... Ops> __host__ __device__ constexpr bool stage_has_pot(Stage<AX, Ops...>) {
-  return ((Ops == OP_POT) || ...);
+  return ((Ops == OP_POT || Ops == OP_POT_RP) || ...);
 }
 
 __device__ __forceinline__ int ld_acquire(const int *p) {
@@ -78,7 +78,7 @@ __device__ __forceinline__ void chain_tile(Stage<AX, Ops...>, C2<T> *__restrict_
     const int l = threadIdx.x / TL, t = threadIdx.x % TL;
     const unsigned line = p * (unsigned) N + tile * (unsigned) W + (unsigned) l;
     const T *vstage = nullptr;
-    if constexpr (((Ops == OP_POT) || ...)) {
+    if constexpr (((Ops == OP_POT || Ops == OP_POT_RP) || ...)) {
       if (pot_prefetch<T, P, TL>(c.az, line, 0u, t, stage, THREADS)) vstage = stage;
     }
     T2 *s = psi + (size_t) line * N;
@@ -92,7 +92,7 @@ __device__ __forceinline__ void chain_tile(Stage<AX, Ops...>, C2<T> *__restrict_
     const int cc = threadIdx.x % W, t = threadIdx.x / W;
     const unsigned q = tile * (unsigned) W + (unsigned) cc;
     const T *vstage = nullptr;
-    if constexpr (((Ops == OP_POT) || ...)) {
+    if constexpr (((Ops == OP_POT || Ops == OP_POT_RP) || ...)) {
       if (pot_prefetch<T, P, TL>(c.ay, p, q, t, stage, THREADS)) vstage = stage;
     }
     T2 *s = psi + (size_t) p * N * N + q;
