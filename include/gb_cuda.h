@@ -15,6 +15,7 @@
 #define LIBGRID_B200_GB_CUDA_H
 
 #include <stddef.h>
+#include <stdint.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -322,6 +323,48 @@ int gb_batch_threads(const gb_batch *b);
 /* Status of the launch's bounded grid barrier (0 = no wait gave up). */
 int gb_batch_error_flag(gb_batch *b, int reset);
 void gb_batch_free(gb_batch *b);
+
+/* ------------------------------------------ learned warm start (U-Net) */
+/*
+ * Kernels of the 3-D convolutional U-Net that turns an external potential
+ * into a starting guess for imaginary-time ground-state relaxation.  No
+ * reference counterpart: the reference's imaginary-time loop is composed by
+ * its callers from grid_wf_propagate / grid_wf_normalize / grid_wf_energy
+ * (src/grid_wf.c:379-556, 681-700, 215-221) and starts from whatever guess
+ * the caller maps in; these kernels only produce that guess.
+ *
+ * Activations are FP32 [C][D][H][W] (one sample per call), weights bf16
+ * [Cout][Cin][27] (3x3x3 taps, zero padding, tap t = 9(dz+1)+3(dy+1)+(dx+1)),
+ * accumulation FP32.  Gradient buffers accumulate (+=); gb_unet_adam clears
+ * them.  All calls are asynchronous on the library stream.
+ */
+/* y = conv(x, w) + b, optionally ReLU'd.  4*cin*27*4 B must fit 48 KB. */
+int gb_unet_conv3_fwd(const float *x, const uint16_t *w, const float *b, float *y, int cin, int cout, int d, int h,
+                      int wd, int relu);
+/* gx = conv^T(gy, w) (overwrites gx).  4*cout*27*4 B must fit 48 KB. */
+int gb_unet_conv3_bwd_data(const float *gy, const uint16_t *w, float *gx, int cin, int cout, int d, int h, int wd);
+/* gw += dL/dw, gb += dL/db (gb may be NULL). */
+int gb_unet_conv3_bwd_weight(const float *x, const float *gy, float *gw, float *gb, int cin, int cout, int d, int h,
+                             int wd);
+/* gy[i] = 0 where y[i] <= 0 (y is the ReLU output). */
+int gb_unet_relu_bwd(float *gy, const float *y, long n);
+/* 2x2x2 average pooling and its gradient (gx += ...); d, h, wd = input
+ * extents (even). */
+int gb_unet_pool2_fwd(const float *x, float *y, int c, int d, int h, int wd);
+int gb_unet_pool2_bwd(const float *gy, float *gx, int c, int d, int h, int wd);
+/* Nearest-neighbour 2x upsampling and its gradient; d, h, wd = input extents. */
+int gb_unet_up2_fwd(const float *x, float *y, int c, int d, int h, int wd);
+int gb_unet_up2_bwd(const float *gy, float *gx, int c, int d, int h, int wd);
+/* grad = scale * (pred - tgt). */
+int gb_unet_mse_grad(const float *pred, const float *tgt, float *grad, long n, float scale);
+/* Adam step on FP32 master weights w; refreshes the bf16 copy wb (may be
+ * NULL) and clears g.  c1 = 1/(1-b1^t), c2 = 1/(1-b2^t). */
+int gb_unet_adam(float *w, uint16_t *wb, float *m, float *v, float *g, long n, float lr, float b1, float b2, float eps,
+                 float c1, float c2);
+/* wb = bf16(w), round to nearest even. */
+int gb_unet_to_bf16(const float *w, uint16_t *wb, long n);
+/* p[0..n) = v. */
+int gb_unet_fill(float *p, long n, float v);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,374 @@
+// Kernels of the learned warm start for imaginary-time ground states: a 3-D
+// convolutional U-Net that maps an external potential (and the coupling g) to
+// a guess of the ground-state amplitude.  Nothing here exists in the
+// reference; the network only replaces the Gaussian initial guess of the
+// caller-composed imaginary-time loop (propagate(-i dt) -> normalize -> energy
+// every M steps).  The plain imaginary-time propagation still decides the
+// converged state.
+//
+// Layout: activations FP32 [C][D][H][W], one sample per call; weights bf16
+// [Cout][Cin][27] (3x3x3 taps, zero padding), FP32 master weights and FP32
+// gradient accumulators [Cout][Cin][27] owned by the caller.  All
+// accumulation is FP32 in a fixed order, so every kernel is deterministic.
+// Weight gradients accumulate (+=) so that a minibatch is a sequence of
+// backward calls followed by one gb_unet_adam, which clears them.
+//
+// These are SIMT kernels (one thread per output voxel and a group of output
+// channels, the block's weight slice staged in shared memory as FP32).
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "gb_common.cuh"
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kCoGroup = 4;                      // output channels per thread (forward)
+constexpr int kCiGroup = 4;                      // input channels per thread (data gradient)
+constexpr size_t kMaxStage = 48 * 1024;          // static shared-memory budget for a weight slice
+
+__global__ void __launch_bounds__(kThreads) k_conv3_fwd(const float *__restrict__ x, const __nv_bfloat16 *__restrict__ w,
+                                                        const float *__restrict__ b, float *__restrict__ y, int cin,
+                                                        int cout, int d, int h, int wd, int relu) {
+  extern __shared__ float ws[];  // [kCoGroup][cin][27]
+  const int co0 = blockIdx.y * kCoGroup;
+  const int nco = min(kCoGroup, cout - co0);
+  for (int i = threadIdx.x; i < nco * cin * 27; i += blockDim.x)
+    ws[i] = __bfloat162float(w[(size_t) co0 * cin * 27 + i]);
+  __syncthreads();
+  const long vol = (long) d * h * wd;
+  const long p = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= vol) return;
+  const int ix = (int) (p % wd), iy = (int) ((p / wd) % h), iz = (int) (p / ((long) wd * h));
+  float acc[kCoGroup];
+#pragma unroll
+  for (int j = 0; j < kCoGroup; j++) acc[j] = 0.f;
+  for (int ci = 0; ci < cin; ci++) {
+    const float *xc = x + (size_t) ci * vol;
+    const float *wc = ws + ci * 27;
+    for (int dz = -1; dz <= 1; dz++) {
+      const int z = iz + dz;
+      if (z < 0 || z >= d) continue;
+      for (int dy = -1; dy <= 1; dy++) {
+        const int yy = iy + dy;
+        if (yy < 0 || yy >= h) continue;
+        for (int dx = -1; dx <= 1; dx++) {
+          const int xx = ix + dx;
+          if (xx < 0 || xx >= wd) continue;
+          const float v = xc[((long) z * h + yy) * wd + xx];
+          const int t = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+#pragma unroll
+          for (int j = 0; j < kCoGroup; j++)
+            if (j < nco) acc[j] = fmaf(v, wc[(size_t) j * cin * 27 + t], acc[j]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kCoGroup; j++) {
+    if (j >= nco) break;
+    float r = acc[j] + b[co0 + j];
+    if (relu) r = fmaxf(r, 0.f);
+    y[(size_t) (co0 + j) * vol + p] = r;
+  }
+}
+
+// gx[ci][q] = sum_co sum_t gy[co][q - off(t)] * w[co][ci][t]
+__global__ void __launch_bounds__(kThreads) k_conv3_bwd_data(const float *__restrict__ gy,
+                                                             const __nv_bfloat16 *__restrict__ w, float *__restrict__ gx,
+                                                             int cin, int cout, int d, int h, int wd) {
+  extern __shared__ float ws[];  // [kCiGroup][cout][27]
+  const int ci0 = blockIdx.y * kCiGroup;
+  const int nci = min(kCiGroup, cin - ci0);
+  for (int i = threadIdx.x; i < nci * cout * 27; i += blockDim.x) {
+    const int j = i / (cout * 27), r = i % (cout * 27), co = r / 27, t = r % 27;
+    ws[i] = __bfloat162float(w[((size_t) co * cin + ci0 + j) * 27 + t]);
+  }
+  __syncthreads();
+  const long vol = (long) d * h * wd;
+  const long q = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= vol) return;
+  const int ix = (int) (q % wd), iy = (int) ((q / wd) % h), iz = (int) (q / ((long) wd * h));
+  float acc[kCiGroup];
+#pragma unroll
+  for (int j = 0; j < kCiGroup; j++) acc[j] = 0.f;
+  for (int co = 0; co < cout; co++) {
+    const float *gc = gy + (size_t) co * vol;
+    const float *wc = ws + co * 27;
+    for (int dz = -1; dz <= 1; dz++) {
+      const int z = iz - dz;
+      if (z < 0 || z >= d) continue;
+      for (int dy = -1; dy <= 1; dy++) {
+        const int yy = iy - dy;
+        if (yy < 0 || yy >= h) continue;
+        for (int dx = -1; dx <= 1; dx++) {
+          const int xx = ix - dx;
+          if (xx < 0 || xx >= wd) continue;
+          const float v = gc[((long) z * h + yy) * wd + xx];
+          const int t = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+#pragma unroll
+          for (int j = 0; j < kCiGroup; j++)
+            if (j < nci) acc[j] = fmaf(v, wc[(size_t) j * cout * 27 + t], acc[j]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kCiGroup; j++) {
+    if (j >= nci) break;
+    gx[(size_t) (ci0 + j) * vol + q] = acc[j];
+  }
+}
+
+// gw[co][ci][t] += sum_p gy[co][p] * x[ci][p + off(t)]; one block per (ci, co).
+__global__ void __launch_bounds__(kThreads) k_conv3_bwd_weight(const float *__restrict__ x, const float *__restrict__ gy,
+                                                               float *__restrict__ gw, int cin, int d, int h, int wd) {
+  __shared__ float red[kThreads / 32][27];
+  const int ci = blockIdx.x, co = blockIdx.y;
+  const long vol = (long) d * h * wd;
+  const float *xc = x + (size_t) ci * vol;
+  const float *gc = gy + (size_t) co * vol;
+  float acc[27];
+#pragma unroll
+  for (int t = 0; t < 27; t++) acc[t] = 0.f;
+  for (long p = threadIdx.x; p < vol; p += blockDim.x) {
+    const float g = gc[p];
+    const int ix = (int) (p % wd), iy = (int) ((p / wd) % h), iz = (int) (p / ((long) wd * h));
+#pragma unroll
+    for (int t = 0; t < 27; t++) {
+      const int z = iz + t / 9 - 1, yy = iy + (t / 3) % 3 - 1, xx = ix + t % 3 - 1;
+      const bool in = z >= 0 && z < d && yy >= 0 && yy < h && xx >= 0 && xx < wd;
+      const float v = in ? xc[((long) z * h + yy) * wd + xx] : 0.f;
+      acc[t] = fmaf(g, v, acc[t]);
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int t = 0; t < 27; t++) {
+    float v = acc[t];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) red[warp][t] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 27) {
+    float s = 0.f;
+    for (int k = 0; k < kThreads / 32; k++) s += red[k][threadIdx.x];
+    gw[((size_t) co * cin + ci) * 27 + threadIdx.x] += s;
+  }
+}
+
+// gb[co] += sum_p gy[co][p]; one block per output channel.
+__global__ void __launch_bounds__(kThreads) k_bias_grad(const float *__restrict__ gy, float *__restrict__ gb, long vol) {
+  __shared__ float red[kThreads / 32];
+  const float *gc = gy + (size_t) blockIdx.x * vol;
+  float s = 0.f;
+  for (long p = threadIdx.x; p < vol; p += blockDim.x) s += gc[p];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.f;
+    for (int k = 0; k < kThreads / 32; k++) t += red[k];
+    gb[blockIdx.x] += t;
+  }
+}
+
+__global__ void k_relu_bwd(float *__restrict__ gy, const float *__restrict__ y, long n) {
+  const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && !(y[i] > 0.f)) gy[i] = 0.f;
+}
+
+// Average over 2x2x2 blocks; d, h, wd are the input extents (even).  The
+// gradient accumulates (gx +=): a pooled activation is also the skip input of
+// the decoder, whose gradient is written first.
+__global__ void k_pool2_fwd(const float *__restrict__ x, float *__restrict__ y, long n_out, int d, int h, int wd) {
+  const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_out) return;
+  const int ow = wd / 2, oh = h / 2, od = d / 2;
+  const int ox = (int) (i % ow), oy = (int) ((i / ow) % oh), oz = (int) ((i / ((long) ow * oh)) % od);
+  const long c = i / ((long) ow * oh * od);
+  const float *xc = x + (size_t) c * d * h * wd;
+  float s = 0.f;
+  for (int k = 0; k < 8; k++) s += xc[((long) (2 * oz + (k >> 2)) * h + 2 * oy + ((k >> 1) & 1)) * wd + 2 * ox + (k & 1)];
+  y[i] = 0.125f * s;
+}
+
+__global__ void k_pool2_bwd(const float *__restrict__ gy, float *__restrict__ gx, long n_in, int d, int h, int wd) {
+  const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_in) return;
+  const int ix = (int) (i % wd), iy = (int) ((i / wd) % h), iz = (int) ((i / ((long) wd * h)) % d);
+  const long c = i / ((long) wd * h * d);
+  const int ow = wd / 2, oh = h / 2, od = d / 2;
+  gx[i] += 0.125f * gy[(((size_t) c * od + iz / 2) * oh + iy / 2) * ow + ix / 2];
+}
+
+// Nearest-neighbour doubling; d, h, wd are the input extents.
+__global__ void k_up2_fwd(const float *__restrict__ x, float *__restrict__ y, long n_out, int d, int h, int wd) {
+  const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_out) return;
+  const int W = 2 * wd, H = 2 * h, D = 2 * d;
+  const int X = (int) (i % W), Y = (int) ((i / W) % H), Z = (int) ((i / ((long) W * H)) % D);
+  const long c = i / ((long) W * H * D);
+  y[i] = x[(((size_t) c * d + Z / 2) * h + Y / 2) * wd + X / 2];
+}
+
+__global__ void k_up2_bwd(const float *__restrict__ gy, float *__restrict__ gx, long n_in, int d, int h, int wd) {
+  const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_in) return;
+  const int ix = (int) (i % wd), iy = (int) ((i / wd) % h), iz = (int) ((i / ((long) wd * h)) % d);
+  const long c = i / ((long) wd * h * d);
+  const int W = 2 * wd, H = 2 * h, D = 2 * d;
+  const float *gc = gy + (size_t) c * D * H * W;
+  float s = 0.f;
+  for (int k = 0; k < 8; k++) s += gc[((long) (2 * iz + (k >> 2)) * H + 2 * iy + ((k >> 1) & 1)) * W + 2 * ix + (k & 1)];
+  gx[i] = s;
+}
+
+__global__ void k_mse_grad(const float *__restrict__ pred, const float *__restrict__ tgt, float *__restrict__ grad, long n,
+                           float scale) {
+  const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) grad[i] = scale * (pred[i] - tgt[i]);
+}
+
+// Adam on FP32 master weights; writes the bf16 copy and clears the gradient.
+// c1 = 1/(1-b1^t), c2 = 1/(1-b2^t).
+__global__ void k_adam(float *__restrict__ w, __nv_bfloat16 *__restrict__ wb, float *__restrict__ m, float *__restrict__ v,
+                       float *__restrict__ g, long n, float lr, float b1, float b2, float eps, float c1, float c2) {
+  const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float wi = w[i] - lr * (mi * c1) / (sqrtf(vi * c2) + eps);
+  w[i] = wi;
+  if (wb) wb[i] = __float2bfloat16_rn(wi);
+  g[i] = 0.f;
+}
+
+__global__ void k_to_bf16(const float *__restrict__ w, __nv_bfloat16 *__restrict__ wb, long n) {
+  const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) wb[i] = __float2bfloat16_rn(w[i]);
+}
+
+__global__ void k_fill(float *__restrict__ p, long n, float v) {
+  const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+inline unsigned blocks_for(long n) { return (unsigned) ((n + kThreads - 1) / kThreads); }
+
+inline int shape_ok(const char *where, long a, long b, long c, long d) {
+  if (a <= 0 || b <= 0 || c <= 0 || d <= 0) return gb__set_error(1101, where);
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int gb_unet_conv3_fwd(const float *x, const uint16_t *w, const float *b, float *y, int cin, int cout, int d,
+                                 int h, int wd, int relu) {
+  if (shape_ok("gb_unet_conv3_fwd: bad shape", cin, cout, (long) d * h, wd)) return 1101;
+  const size_t smem = (size_t) kCoGroup * cin * 27 * sizeof(float);
+  if (smem > kMaxStage) return gb__set_error(1102, "gb_unet_conv3_fwd: too many input channels for the weight stage");
+  const long vol = (long) d * h * wd;
+  dim3 grid(blocks_for(vol), (cout + kCoGroup - 1) / kCoGroup);
+  k_conv3_fwd<<<grid, kThreads, smem, gb__stream()>>>(x, (const __nv_bfloat16 *) w, b, y, cin, cout, d, h, wd, relu);
+  GB_CHECK_LAUNCH("gb_unet_conv3_fwd");
+  return 0;
+}
+
+extern "C" int gb_unet_conv3_bwd_data(const float *gy, const uint16_t *w, float *gx, int cin, int cout, int d, int h,
+                                      int wd) {
+  if (shape_ok("gb_unet_conv3_bwd_data: bad shape", cin, cout, (long) d * h, wd)) return 1101;
+  const size_t smem = (size_t) kCiGroup * cout * 27 * sizeof(float);
+  if (smem > kMaxStage) return gb__set_error(1102, "gb_unet_conv3_bwd_data: too many output channels for the weight stage");
+  const long vol = (long) d * h * wd;
+  dim3 grid(blocks_for(vol), (cin + kCiGroup - 1) / kCiGroup);
+  k_conv3_bwd_data<<<grid, kThreads, smem, gb__stream()>>>(gy, (const __nv_bfloat16 *) w, gx, cin, cout, d, h, wd);
+  GB_CHECK_LAUNCH("gb_unet_conv3_bwd_data");
+  return 0;
+}
+
+extern "C" int gb_unet_conv3_bwd_weight(const float *x, const float *gy, float *gw, float *gb, int cin, int cout, int d,
+                                        int h, int wd) {
+  if (shape_ok("gb_unet_conv3_bwd_weight: bad shape", cin, cout, (long) d * h, wd)) return 1101;
+  const long vol = (long) d * h * wd;
+  k_conv3_bwd_weight<<<dim3(cin, cout), kThreads, 0, gb__stream()>>>(x, gy, gw, cin, d, h, wd);
+  GB_CHECK_LAUNCH("gb_unet_conv3_bwd_weight");
+  if (gb) {
+    k_bias_grad<<<cout, kThreads, 0, gb__stream()>>>(gy, gb, vol);
+    GB_CHECK_LAUNCH("gb_unet_conv3_bwd_bias");
+  }
+  return 0;
+}
+
+extern "C" int gb_unet_relu_bwd(float *gy, const float *y, long n) {
+  if (n <= 0) return 0;
+  k_relu_bwd<<<blocks_for(n), kThreads, 0, gb__stream()>>>(gy, y, n);
+  GB_CHECK_LAUNCH("gb_unet_relu_bwd");
+  return 0;
+}
+
+extern "C" int gb_unet_pool2_fwd(const float *x, float *y, int c, int d, int h, int wd) {
+  if (shape_ok("gb_unet_pool2_fwd: bad shape", c, d, h, wd) || (d | h | wd) & 1)
+    return gb__set_error(1103, "gb_unet_pool2_fwd: extents must be positive and even");
+  const long n = (long) c * (d / 2) * (h / 2) * (wd / 2);
+  k_pool2_fwd<<<blocks_for(n), kThreads, 0, gb__stream()>>>(x, y, n, d, h, wd);
+  GB_CHECK_LAUNCH("gb_unet_pool2_fwd");
+  return 0;
+}
+
+extern "C" int gb_unet_pool2_bwd(const float *gy, float *gx, int c, int d, int h, int wd) {
+  if (shape_ok("gb_unet_pool2_bwd: bad shape", c, d, h, wd) || (d | h | wd) & 1)
+    return gb__set_error(1103, "gb_unet_pool2_bwd: extents must be positive and even");
+  const long n = (long) c * d * h * wd;
+  k_pool2_bwd<<<blocks_for(n), kThreads, 0, gb__stream()>>>(gy, gx, n, d, h, wd);
+  GB_CHECK_LAUNCH("gb_unet_pool2_bwd");
+  return 0;
+}
+
+extern "C" int gb_unet_up2_fwd(const float *x, float *y, int c, int d, int h, int wd) {
+  if (shape_ok("gb_unet_up2_fwd: bad shape", c, d, h, wd)) return 1101;
+  const long n = 8L * c * d * h * wd;
+  k_up2_fwd<<<blocks_for(n), kThreads, 0, gb__stream()>>>(x, y, n, d, h, wd);
+  GB_CHECK_LAUNCH("gb_unet_up2_fwd");
+  return 0;
+}
+
+extern "C" int gb_unet_up2_bwd(const float *gy, float *gx, int c, int d, int h, int wd) {
+  if (shape_ok("gb_unet_up2_bwd: bad shape", c, d, h, wd)) return 1101;
+  const long n = (long) c * d * h * wd;
+  k_up2_bwd<<<blocks_for(n), kThreads, 0, gb__stream()>>>(gy, gx, n, d, h, wd);
+  GB_CHECK_LAUNCH("gb_unet_up2_bwd");
+  return 0;
+}
+
+extern "C" int gb_unet_mse_grad(const float *pred, const float *tgt, float *grad, long n, float scale) {
+  if (n <= 0) return 0;
+  k_mse_grad<<<blocks_for(n), kThreads, 0, gb__stream()>>>(pred, tgt, grad, n, scale);
+  GB_CHECK_LAUNCH("gb_unet_mse_grad");
+  return 0;
+}
+
+extern "C" int gb_unet_adam(float *w, uint16_t *wb, float *m, float *v, float *g, long n, float lr, float b1, float b2,
+                            float eps, float c1, float c2) {
+  if (n <= 0) return 0;
+  k_adam<<<blocks_for(n), kThreads, 0, gb__stream()>>>(w, (__nv_bfloat16 *) wb, m, v, g, n, lr, b1, b2, eps, c1, c2);
+  GB_CHECK_LAUNCH("gb_unet_adam");
+  return 0;
+}
+
+extern "C" int gb_unet_to_bf16(const float *w, uint16_t *wb, long n) {
+  if (n <= 0) return 0;
+  k_to_bf16<<<blocks_for(n), kThreads, 0, gb__stream()>>>(w, (__nv_bfloat16 *) wb, n);
+  GB_CHECK_LAUNCH("gb_unet_to_bf16");
+  return 0;
+}
+
+extern "C" int gb_unet_fill(float *p, long n, float v) {
+  if (n <= 0) return 0;
+  k_fill<<<blocks_for(n), kThreads, 0, gb__stream()>>>(p, n, v);
+  GB_CHECK_LAUNCH("gb_unet_fill");
+  return 0;
+}

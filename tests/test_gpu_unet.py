@@ -1,0 +1,171 @@
+"""U-Net warm-start kernels (gb_unet_*) against the numpy oracle, the whole
+network's gradients against the oracle's reverse mode, and the warm start
+itself: ground states relaxed from the network's guess need fewer
+imaginary-time steps than from a Gaussian and reach the same energy."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from libgrid_b200 import warmstart as ws
+from oracle import unet_oracle as uo
+
+pytestmark = pytest.mark.gpu
+
+TOL = 2e-6  # FP32 accumulation against the float64 oracle, relative L2
+
+
+def _rel(a, b):
+    return float(np.linalg.norm((np.asarray(a, np.float64) - b).ravel()) / max(np.linalg.norm(np.ravel(b)), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def lib(b200):
+    b200.lib.cuda_enable(b"\x01", 0, None)
+    ws._bind(b200.lib)
+    return b200.lib
+
+
+class Dev:
+    def __init__(self, lib):
+        self.lib, self.ptrs = lib, []
+
+    def put(self, a):
+        a = np.ascontiguousarray(a)
+        p = self.lib.gb_device_alloc(max(a.nbytes, 4))
+        assert p
+        assert self.lib.gb_h2d(p, a.ctypes.data, a.nbytes) == 0
+        self.ptrs.append(p)
+        return p
+
+    def get(self, p, shape, dtype=np.float32):
+        out = np.empty(shape, dtype)
+        assert self.lib.gb_d2h(out.ctypes.data, p, out.nbytes) == 0
+        assert self.lib.gb_synchronize() == 0
+        return out
+
+    def free(self):
+        for p in self.ptrs:
+            self.lib.gb_device_free(p)
+
+
+@pytest.mark.parametrize("cin,cout,shape", [(5, 6, (6, 8, 10)), (24, 8, (8, 8, 8)), (96, 32, (4, 4, 4)), (3, 1, (5, 7, 3))])
+def test_conv_kernels_vs_oracle(lib, cin, cout, shape):
+    rng = np.random.default_rng(cin * 100 + cout)
+    d = Dev(lib)
+    x = rng.standard_normal((cin,) + shape).astype(np.float32)
+    w = (rng.standard_normal((cout, cin, 27)) * 0.2).astype(np.float32)
+    b = rng.standard_normal(cout).astype(np.float32)
+    gy = rng.standard_normal((cout,) + shape).astype(np.float32)
+    wr = uo.bf16_round(w)
+    dx, dw, db, dgy = d.put(x), d.put(uo.bf16_bits(w)), d.put(b), d.put(gy)
+    dy = d.put(np.zeros((cout,) + shape, np.float32))
+    for relu in (0, 1):
+        assert lib.gb_unet_conv3_fwd(dx, dw, db, dy, cin, cout, *shape, relu) == 0
+        assert _rel(d.get(dy, (cout,) + shape), uo.conv3_fwd(x, wr, b, relu)) < TOL
+    dgx = d.put(np.full((cin,) + shape, 7.0, np.float32))
+    assert lib.gb_unet_conv3_bwd_data(dgy, dw, dgx, cin, cout, *shape) == 0
+    assert _rel(d.get(dgx, (cin,) + shape), uo.conv3_bwd_data(gy, wr)) < TOL
+    gw0 = rng.standard_normal((cout, cin, 27)).astype(np.float32)
+    gb0 = rng.standard_normal(cout).astype(np.float32)
+    dgw, dgb = d.put(gw0), d.put(gb0)
+    assert lib.gb_unet_conv3_bwd_weight(dx, dgy, dgw, dgb, cin, cout, *shape) == 0
+    gw, gb = uo.conv3_bwd_weight(x, gy)
+    assert _rel(d.get(dgw, gw.shape), gw + gw0) < TOL
+    assert _rel(d.get(dgb, gb.shape), gb + gb0) < TOL
+    d.free()
+
+
+def test_pool_up_relu_adam_vs_oracle(lib):
+    rng = np.random.default_rng(3)
+    d = Dev(lib)
+    c, shape = 5, (6, 8, 4)
+    half = tuple(s // 2 for s in shape)
+    x = rng.standard_normal((c,) + shape).astype(np.float32)
+    dx = d.put(x)
+    dp = d.put(np.zeros((c,) + half, np.float32))
+    assert lib.gb_unet_pool2_fwd(dx, dp, c, *shape) == 0
+    assert _rel(d.get(dp, (c,) + half), uo.pool2_fwd(x)) < TOL
+    gy = rng.standard_normal((c,) + half).astype(np.float32)
+    g0 = rng.standard_normal((c,) + shape).astype(np.float32)
+    dgy, dg0 = d.put(gy), d.put(g0)
+    assert lib.gb_unet_pool2_bwd(dgy, dg0, c, *shape) == 0  # accumulates
+    assert _rel(d.get(dg0, (c,) + shape), g0 + uo.pool2_bwd(gy)) < TOL
+    xs = rng.standard_normal((c,) + half).astype(np.float32)
+    dxs, dup = d.put(xs), d.put(np.zeros((c,) + shape, np.float32))
+    assert lib.gb_unet_up2_fwd(dxs, dup, c, *half) == 0
+    assert np.array_equal(d.get(dup, (c,) + shape), uo.up2_fwd(xs).astype(np.float32))
+    gup = rng.standard_normal((c,) + shape).astype(np.float32)
+    dgup, dgs = d.put(gup), d.put(np.zeros((c,) + half, np.float32))
+    assert lib.gb_unet_up2_bwd(dgup, dgs, c, *half) == 0
+    assert _rel(d.get(dgs, (c,) + half), uo.up2_bwd(gup)) < TOL
+    y = rng.standard_normal(1000).astype(np.float32)
+    g = rng.standard_normal(1000).astype(np.float32)
+    dyy, dg = d.put(np.maximum(y, 0)), d.put(g)
+    assert lib.gb_unet_relu_bwd(dg, dyy, 1000) == 0
+    assert np.array_equal(d.get(dg, 1000), np.where(y > 0, g, 0).astype(np.float32))
+    # Adam
+    n = 777
+    w, m, v, gr = (rng.standard_normal(n).astype(np.float32) for _ in range(4))
+    v = np.abs(v)
+    dw, dm, dv, dgr = d.put(w), d.put(m), d.put(v), d.put(gr)
+    dwb = d.put(np.zeros(n, np.uint16))
+    lr, b1, b2, eps, c1, c2 = 1e-2, 0.9, 0.999, 1e-8, 1 / (1 - 0.9**3), 1 / (1 - 0.999**3)
+    assert lib.gb_unet_adam(dw, dwb, dm, dv, dgr, n, lr, b1, b2, eps, c1, c2) == 0
+    m1 = b1 * m.astype(np.float64) + (1 - b1) * gr
+    v1 = b2 * v.astype(np.float64) + (1 - b2) * gr.astype(np.float64) ** 2
+    w1 = w - lr * (m1 * c1) / (np.sqrt(v1 * c2) + eps)
+    got = d.get(dw, n)
+    assert _rel(got, w1) < 1e-6
+    assert np.array_equal(d.get(dwb, n, np.uint16), uo.bf16_bits(got))
+    assert not np.any(d.get(dgr, n))
+    d.free()
+
+
+def test_unet_gradients_vs_oracle(b200, lib):
+    n = 16
+    rng = np.random.default_rng(11)
+    net = ws.DeviceUNet(b200, n, cin=3, seed=4)
+    try:
+        p = net.get("p")
+        bias = rng.standard_normal(p.shape).astype(np.float32) * 0.05
+        for o, co, ci in net.layers.values():  # give the biases nonzero values
+            p[o + co * ci * 27 : o + co * ci * 27 + co] = bias[:co]
+        net.set_params(p)
+        x = rng.standard_normal((3, n, n, n)).astype(np.float32)
+        tgt = rng.standard_normal((n, n, n)).astype(np.float32) * 0.1
+        net.set_input(x)
+        net.forward()
+        net.loss_grad(net.set_target(tgt), 2.0 / n**3)
+        net.backward()
+        g = net.get("g")
+        pred = net.activation("out")[0]
+        params = {k: (uo.bf16_round(w), b.astype(np.float64)) for k, (w, b) in net.layer_arrays(p).items()}
+        want_pred, _ = uo.unet_forward(net.spec, params, x)
+        assert _rel(pred, want_pred[0]) < 1e-5
+        _, grads = uo.unet_loss_grads(net.spec, params, x, tgt[None])
+        got = net.layer_arrays(g)
+        for layer, (gw, gb) in grads.items():
+            assert _rel(got[layer][0], gw) < 1e-4, layer
+            assert _rel(got[layer][1], gb) < 1e-4, layer
+    finally:
+        net.free()
+
+
+def test_warm_start_cuts_imaginary_time_steps(b200, lib):
+    n, step = 32, 0.1
+    xs, ys, meta = ws.make_dataset(b200, range(1000, 1032), n, step)
+    assert all(m["steps"] < 20000 for m in meta)
+    net = ws.DeviceUNet(b200, n, cin=3, seed=0)
+    try:
+        loss = ws.train(net, xs, ys, epochs=40, batch=8, lr=2e-3)
+        assert loss < 0.05 * float((ys**2).mean())
+        rows = ws.evaluate(b200, net, range(5000, 5006), n, step)
+    finally:
+        net.free()
+    steps_g = np.mean([r["steps_gauss"] for r in rows])
+    steps_n = np.mean([r["steps_net"] for r in rows])
+    print("warm start: steps %.0f (Gaussian) -> %.0f (network); TF start %.0f; max |dE| %.2e"
+          % (steps_g, steps_n, np.mean([r["steps_tf"] for r in rows]), max(r["de"] for r in rows)))
+    assert steps_n < steps_g
+    assert max(r["de"] for r in rows) < 1e-6
