@@ -25,45 +25,70 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kCoGroup = 4;                      // output channels per thread (forward)
 constexpr int kCiGroup = 4;                      // input channels per thread (data gradient)
-constexpr size_t kMaxStage = 48 * 1024;          // static shared-memory budget for a weight slice
+constexpr int kSplit = 4;                        // channel-loop slices for small volumes
+constexpr long kSplitVolume = 4096;              // volumes up to 16^3 use the sliced kernels
+// Shared-memory budget for a weight slice: 48 KB less the slices' reduction buffer.
+constexpr size_t kMaxStage = 48 * 1024 - kSplit * 4 * (kThreads / kSplit) * sizeof(float);
 
+// S thread slices per voxel split the input-channel loop (ci = s, s + S, ...)
+// and are summed in slice order through shared memory, so small volumes (the
+// coarse levels: 4^3 to 16^3 voxels) still fill the SM.  S = 1 for large ones.
+template <int S>
 __global__ void __launch_bounds__(kThreads) k_conv3_fwd(const float *__restrict__ x, const __nv_bfloat16 *__restrict__ w,
                                                         const float *__restrict__ b, float *__restrict__ y, int cin,
                                                         int cout, int d, int h, int wd, int relu) {
-  extern __shared__ float ws[];  // [kCoGroup][cin][27]
+  constexpr int VB = kThreads / S;  // voxels per block
+  extern __shared__ float ws[];     // [kCoGroup][cin][27]
   const int co0 = blockIdx.y * kCoGroup;
   const int nco = min(kCoGroup, cout - co0);
   for (int i = threadIdx.x; i < nco * cin * 27; i += blockDim.x)
     ws[i] = __bfloat162float(w[(size_t) co0 * cin * 27 + i]);
   __syncthreads();
   const long vol = (long) d * h * wd;
-  const long p = (long) blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= vol) return;
-  const int ix = (int) (p % wd), iy = (int) ((p / wd) % h), iz = (int) (p / ((long) wd * h));
+  const int sl = threadIdx.x / VB, pl = threadIdx.x % VB;
+  const long p = (long) blockIdx.x * VB + pl;
+  const bool valid = p < vol;
   float acc[kCoGroup];
 #pragma unroll
   for (int j = 0; j < kCoGroup; j++) acc[j] = 0.f;
-  for (int ci = 0; ci < cin; ci++) {
-    const float *xc = x + (size_t) ci * vol;
-    const float *wc = ws + ci * 27;
-    for (int dz = -1; dz <= 1; dz++) {
-      const int z = iz + dz;
-      if (z < 0 || z >= d) continue;
-      for (int dy = -1; dy <= 1; dy++) {
-        const int yy = iy + dy;
-        if (yy < 0 || yy >= h) continue;
-        for (int dx = -1; dx <= 1; dx++) {
-          const int xx = ix + dx;
-          if (xx < 0 || xx >= wd) continue;
-          const float v = xc[((long) z * h + yy) * wd + xx];
-          const int t = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+  if (valid) {
+    const int ix = (int) (p % wd), iy = (int) ((p / wd) % h), iz = (int) (p / ((long) wd * h));
+    for (int ci = sl; ci < cin; ci += S) {
+      const float *xc = x + (size_t) ci * vol;
+      const float *wc = ws + ci * 27;
+      for (int dz = -1; dz <= 1; dz++) {
+        const int z = iz + dz;
+        if (z < 0 || z >= d) continue;
+        for (int dy = -1; dy <= 1; dy++) {
+          const int yy = iy + dy;
+          if (yy < 0 || yy >= h) continue;
+          for (int dx = -1; dx <= 1; dx++) {
+            const int xx = ix + dx;
+            if (xx < 0 || xx >= wd) continue;
+            const float v = xc[((long) z * h + yy) * wd + xx];
+            const int t = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
 #pragma unroll
-          for (int j = 0; j < kCoGroup; j++)
-            if (j < nco) acc[j] = fmaf(v, wc[(size_t) j * cin * 27 + t], acc[j]);
+            for (int j = 0; j < kCoGroup; j++)
+              if (j < nco) acc[j] = fmaf(v, wc[(size_t) j * cin * 27 + t], acc[j]);
+          }
         }
       }
     }
   }
+  if constexpr (S > 1) {
+    __shared__ float red[S][kCoGroup][VB];
+#pragma unroll
+    for (int j = 0; j < kCoGroup; j++) red[sl][j][pl] = acc[j];
+    __syncthreads();
+    if (sl != 0) return;
+#pragma unroll
+    for (int j = 0; j < kCoGroup; j++) {
+      float t = red[0][j][pl];
+      for (int k = 1; k < S; k++) t += red[k][j][pl];
+      acc[j] = t;
+    }
+  }
+  if (!valid) return;
 #pragma unroll
   for (int j = 0; j < kCoGroup; j++) {
     if (j >= nco) break;
@@ -73,10 +98,13 @@ __global__ void __launch_bounds__(kThreads) k_conv3_fwd(const float *__restrict_
   }
 }
 
-// gx[ci][q] = sum_co sum_t gy[co][q - off(t)] * w[co][ci][t]
+// gx[ci][q] = sum_co sum_t gy[co][q - off(t)] * w[co][ci][t]; S slices split
+// the output-channel loop as in the forward kernel.
+template <int S>
 __global__ void __launch_bounds__(kThreads) k_conv3_bwd_data(const float *__restrict__ gy,
                                                              const __nv_bfloat16 *__restrict__ w, float *__restrict__ gx,
                                                              int cin, int cout, int d, int h, int wd) {
+  constexpr int VB = kThreads / S;
   extern __shared__ float ws[];  // [kCiGroup][cout][27]
   const int ci0 = blockIdx.y * kCiGroup;
   const int nci = min(kCiGroup, cin - ci0);
@@ -86,33 +114,50 @@ __global__ void __launch_bounds__(kThreads) k_conv3_bwd_data(const float *__rest
   }
   __syncthreads();
   const long vol = (long) d * h * wd;
-  const long q = (long) blockIdx.x * blockDim.x + threadIdx.x;
-  if (q >= vol) return;
-  const int ix = (int) (q % wd), iy = (int) ((q / wd) % h), iz = (int) (q / ((long) wd * h));
+  const int sl = threadIdx.x / VB, pl = threadIdx.x % VB;
+  const long q = (long) blockIdx.x * VB + pl;
+  const bool valid = q < vol;
   float acc[kCiGroup];
 #pragma unroll
   for (int j = 0; j < kCiGroup; j++) acc[j] = 0.f;
-  for (int co = 0; co < cout; co++) {
-    const float *gc = gy + (size_t) co * vol;
-    const float *wc = ws + co * 27;
-    for (int dz = -1; dz <= 1; dz++) {
-      const int z = iz - dz;
-      if (z < 0 || z >= d) continue;
-      for (int dy = -1; dy <= 1; dy++) {
-        const int yy = iy - dy;
-        if (yy < 0 || yy >= h) continue;
-        for (int dx = -1; dx <= 1; dx++) {
-          const int xx = ix - dx;
-          if (xx < 0 || xx >= wd) continue;
-          const float v = gc[((long) z * h + yy) * wd + xx];
-          const int t = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
+  if (valid) {
+    const int ix = (int) (q % wd), iy = (int) ((q / wd) % h), iz = (int) (q / ((long) wd * h));
+    for (int co = sl; co < cout; co += S) {
+      const float *gc = gy + (size_t) co * vol;
+      const float *wc = ws + co * 27;
+      for (int dz = -1; dz <= 1; dz++) {
+        const int z = iz - dz;
+        if (z < 0 || z >= d) continue;
+        for (int dy = -1; dy <= 1; dy++) {
+          const int yy = iy - dy;
+          if (yy < 0 || yy >= h) continue;
+          for (int dx = -1; dx <= 1; dx++) {
+            const int xx = ix - dx;
+            if (xx < 0 || xx >= wd) continue;
+            const float v = gc[((long) z * h + yy) * wd + xx];
+            const int t = (dz + 1) * 9 + (dy + 1) * 3 + (dx + 1);
 #pragma unroll
-          for (int j = 0; j < kCiGroup; j++)
-            if (j < nci) acc[j] = fmaf(v, wc[(size_t) j * cout * 27 + t], acc[j]);
+            for (int j = 0; j < kCiGroup; j++)
+              if (j < nci) acc[j] = fmaf(v, wc[(size_t) j * cout * 27 + t], acc[j]);
+          }
         }
       }
     }
   }
+  if constexpr (S > 1) {
+    __shared__ float red[S][kCiGroup][VB];
+#pragma unroll
+    for (int j = 0; j < kCiGroup; j++) red[sl][j][pl] = acc[j];
+    __syncthreads();
+    if (sl != 0) return;
+#pragma unroll
+    for (int j = 0; j < kCiGroup; j++) {
+      float t = red[0][j][pl];
+      for (int k = 1; k < S; k++) t += red[k][j][pl];
+      acc[j] = t;
+    }
+  }
+  if (!valid) return;
 #pragma unroll
   for (int j = 0; j < kCiGroup; j++) {
     if (j >= nci) break;
@@ -272,8 +317,13 @@ extern "C" int gb_unet_conv3_fwd(const float *x, const uint16_t *w, const float 
   const size_t smem = (size_t) kCoGroup * cin * 27 * sizeof(float);
   if (smem > kMaxStage) return gb__set_error(1102, "gb_unet_conv3_fwd: too many input channels for the weight stage");
   const long vol = (long) d * h * wd;
-  dim3 grid(blocks_for(vol), (cout + kCoGroup - 1) / kCoGroup);
-  k_conv3_fwd<<<grid, kThreads, smem, gb__stream()>>>(x, (const __nv_bfloat16 *) w, b, y, cin, cout, d, h, wd, relu);
+  const unsigned gy = (cout + kCoGroup - 1) / kCoGroup;
+  if (vol <= kSplitVolume)
+    k_conv3_fwd<kSplit><<<dim3((unsigned) ((vol + kThreads / kSplit - 1) / (kThreads / kSplit)), gy), kThreads, smem,
+                          gb__stream()>>>(x, (const __nv_bfloat16 *) w, b, y, cin, cout, d, h, wd, relu);
+  else
+    k_conv3_fwd<1><<<dim3(blocks_for(vol), gy), kThreads, smem, gb__stream()>>>(x, (const __nv_bfloat16 *) w, b, y, cin,
+                                                                               cout, d, h, wd, relu);
   GB_CHECK_LAUNCH("gb_unet_conv3_fwd");
   return 0;
 }
@@ -284,8 +334,13 @@ extern "C" int gb_unet_conv3_bwd_data(const float *gy, const uint16_t *w, float 
   const size_t smem = (size_t) kCiGroup * cout * 27 * sizeof(float);
   if (smem > kMaxStage) return gb__set_error(1102, "gb_unet_conv3_bwd_data: too many output channels for the weight stage");
   const long vol = (long) d * h * wd;
-  dim3 grid(blocks_for(vol), (cin + kCiGroup - 1) / kCiGroup);
-  k_conv3_bwd_data<<<grid, kThreads, smem, gb__stream()>>>(gy, (const __nv_bfloat16 *) w, gx, cin, cout, d, h, wd);
+  const unsigned gyd = (cin + kCiGroup - 1) / kCiGroup;
+  if (vol <= kSplitVolume)
+    k_conv3_bwd_data<kSplit><<<dim3((unsigned) ((vol + kThreads / kSplit - 1) / (kThreads / kSplit)), gyd), kThreads,
+                               smem, gb__stream()>>>(gy, (const __nv_bfloat16 *) w, gx, cin, cout, d, h, wd);
+  else
+    k_conv3_bwd_data<1><<<dim3(blocks_for(vol), gyd), kThreads, smem, gb__stream()>>>(gy, (const __nv_bfloat16 *) w, gx,
+                                                                                     cin, cout, d, h, wd);
   GB_CHECK_LAUNCH("gb_unet_conv3_bwd_data");
   return 0;
 }

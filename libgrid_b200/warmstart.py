@@ -449,6 +449,32 @@ def evaluate(api, net: DeviceUNet, seeds, n=32, step=0.1):
     return rows
 
 
+def time_training_step(net: DeviceUNet, x, y, reps: int = 20):
+    """(forward ms, forward + loss + backward ms) per sample, CUDA events on
+    the library stream, after 3 warm-up repetitions."""
+    lib = net.lib
+    lib.gb_event_record.restype = C.c_int
+    lib.gb_event_record.argtypes = [C.c_int]
+    lib.gb_event_elapsed_ms.restype = C.c_float
+    lib.gb_event_elapsed_ms.argtypes = [C.c_int, C.c_int]
+    net.set_input(x)
+    tgt = net.set_target(y)
+    out = []
+    for with_bwd in (False, True):
+        for r in range(reps + 3):
+            if r == 3:
+                _ok(lib.gb_event_record(0), "event")
+            net.forward()
+            if with_bwd:
+                net.loss_grad(tgt)
+                net.backward()
+        _ok(lib.gb_event_record(1), "event")
+        _ok(lib.gb_synchronize(), "sync")
+        out.append(lib.gb_event_elapsed_ms(0, 1) / reps)
+    _ok(lib.gb_unet_fill(net._g, net.nparam, 0.0), "fill")  # drop the timing runs' gradients
+    return out
+
+
 def main(argv=None):
     """python -m libgrid_b200.warmstart [--train N] [--test N] [--epochs E]
     [--out report.json]: generate, train, evaluate and print one JSON report."""
@@ -458,9 +484,9 @@ def main(argv=None):
     import libgrid_b200
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--train", type=int, default=64)
+    ap.add_argument("--train", type=int, default=128)
     ap.add_argument("--test", type=int, default=16)
-    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--epochs", type=int, default=100)
     ap.add_argument("--n", type=int, default=32)
     ap.add_argument("--step", type=float, default=0.1)
     ap.add_argument("--out", default=None)
@@ -475,6 +501,7 @@ def main(argv=None):
         t0 = time.perf_counter()
         loss = train(net, xs, ys, epochs=a.epochs, batch=8, lr=2e-3)
         t_train = time.perf_counter() - t0
+        step_ms = time_training_step(net, xs[0], ys[0])
         rows = evaluate(api, net, range(5000, 5000 + a.test), a.n, a.step)
     finally:
         net.free()
@@ -483,7 +510,7 @@ def main(argv=None):
         workload="learned warm start, GP imaginary time %d^3 step %.2f, %d training / %d held-out potentials"
         % (a.n, a.step, a.train, a.test),
         params=int(net.nparam), epochs=a.epochs, train_loss=loss, target_ms=float((ys**2).mean()),
-        data_seconds=t_data, train_seconds=t_train,
+        data_seconds=t_data, train_seconds=t_train, forward_ms=step_ms[0], forward_backward_ms=step_ms[1],
         steps_gauss=mean("steps_gauss"), steps_tf=mean("steps_tf"), steps_net=mean("steps_net"),
         sec_gauss=mean("sec_gauss"), sec_tf=mean("sec_tf"), sec_net=mean("sec_net"),
         step_ratio=mean("steps_gauss") / mean("steps_net"), time_ratio=mean("sec_gauss") / mean("sec_net"),

@@ -49,7 +49,7 @@ class Dev:
             self.lib.gb_device_free(p)
 
 
-@pytest.mark.parametrize("cin,cout,shape", [(5, 6, (6, 8, 10)), (24, 8, (8, 8, 8)), (96, 32, (4, 4, 4)), (3, 1, (5, 7, 3))])
+@pytest.mark.parametrize("cin,cout,shape", [(5, 6, (6, 8, 10)), (24, 8, (8, 8, 8)), (96, 32, (4, 4, 4)), (3, 1, (5, 7, 3)), (8, 7, (16, 16, 20)), (64, 64, (4, 4, 4))])
 def test_conv_kernels_vs_oracle(lib, cin, cout, shape):
     rng = np.random.default_rng(cin * 100 + cout)
     d = Dev(lib)
