@@ -16,7 +16,8 @@ enum {
   GB_SCR_STAGE = 5,    // precision-conversion staging
   GB_SCR_KIN2 = 6,     // kinetic factor tables of the merged K(dt) pass
   GB_SCR_CHAIN = 7,    // tile counters and ticket of the plane-chained passes
-  GB_SCR_COUNT = 8
+  GB_SCR_UNET = 8,     // per-chunk weight-gradient partials of the U-Net kernels
+  GB_SCR_COUNT = 9
 };
 
 void *gb__scratch(int slot, size_t bytes);

@@ -18,7 +18,10 @@
 #include <cuda_bf16.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "gb_common.cuh"
+#include "gb_internal_cuda.h"
 
 namespace {
 
@@ -165,41 +168,68 @@ __global__ void __launch_bounds__(kThreads) k_conv3_bwd_data(const float *__rest
   }
 }
 
-// gw[co][ci][t] += sum_p gy[co][p] * x[ci][p + off(t)]; one block per (ci, co).
-__global__ void __launch_bounds__(kThreads) k_conv3_bwd_weight(const float *__restrict__ x, const float *__restrict__ gy,
-                                                               float *__restrict__ gw, int cin, int d, int h, int wd) {
-  __shared__ float red[kThreads / 32][27];
-  const int ci = blockIdx.x, co = blockIdx.y;
+// Weight gradient dL/dw[co][ci][t] = sum_p gy[co][p] * x[ci][p + off(t)].
+// One CTA per (ci, group of kWCo output channels, voxel chunk): each input
+// load serves kWCo output channels.  With one chunk the CTA adds its sums to
+// gw; with several it writes them to part[chunk][co][ci][27], and
+// k_wgrad_finish adds the chunks to gw in chunk order (no atomics).
+constexpr int kWThreads = 128;
+constexpr int kWCo = 4;
+
+__global__ void __launch_bounds__(kWThreads) k_conv3_bwd_weight(const float *__restrict__ x, const float *__restrict__ gy,
+                                                                float *__restrict__ gw, float *__restrict__ part,
+                                                                int cin, int cout, int d, int h, int wd, long chunk) {
+  __shared__ float red[kWThreads / 32][kWCo * 27];
+  const int ci = blockIdx.x, co0 = blockIdx.y * kWCo, c = blockIdx.z;
+  const int nco = min(kWCo, cout - co0);
   const long vol = (long) d * h * wd;
+  const long p0 = (long) c * chunk, p1 = min(vol, p0 + chunk);
   const float *xc = x + (size_t) ci * vol;
-  const float *gc = gy + (size_t) co * vol;
-  float acc[27];
+  float acc[kWCo][27];
 #pragma unroll
-  for (int t = 0; t < 27; t++) acc[t] = 0.f;
-  for (long p = threadIdx.x; p < vol; p += blockDim.x) {
-    const float g = gc[p];
+  for (int j = 0; j < kWCo; j++)
+#pragma unroll
+    for (int t = 0; t < 27; t++) acc[j][t] = 0.f;
+  for (long p = p0 + threadIdx.x; p < p1; p += kWThreads) {
+    float g[kWCo];
+#pragma unroll
+    for (int j = 0; j < kWCo; j++) g[j] = (j < nco) ? gy[(size_t) (co0 + j) * vol + p] : 0.f;
     const int ix = (int) (p % wd), iy = (int) ((p / wd) % h), iz = (int) (p / ((long) wd * h));
 #pragma unroll
     for (int t = 0; t < 27; t++) {
       const int z = iz + t / 9 - 1, yy = iy + (t / 3) % 3 - 1, xx = ix + t % 3 - 1;
       const bool in = z >= 0 && z < d && yy >= 0 && yy < h && xx >= 0 && xx < wd;
       const float v = in ? xc[((long) z * h + yy) * wd + xx] : 0.f;
-      acc[t] = fmaf(g, v, acc[t]);
+#pragma unroll
+      for (int j = 0; j < kWCo; j++) acc[j][t] = fmaf(g[j], v, acc[j][t]);
     }
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int t = 0; t < 27; t++) {
-    float v = acc[t];
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    if (lane == 0) red[warp][t] = v;
-  }
+  for (int j = 0; j < kWCo; j++)
+#pragma unroll
+    for (int t = 0; t < 27; t++) {
+      float v = acc[j][t];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) red[warp][j * 27 + t] = v;
+    }
   __syncthreads();
-  if (threadIdx.x < 27) {
+  for (int i = threadIdx.x; i < nco * 27; i += kWThreads) {
     float s = 0.f;
-    for (int k = 0; k < kThreads / 32; k++) s += red[k][threadIdx.x];
-    gw[((size_t) co * cin + ci) * 27 + threadIdx.x] += s;
+    for (int k = 0; k < kWThreads / 32; k++) s += red[k][i];
+    const int j = i / 27, t = i % 27;
+    const size_t w = ((size_t) (co0 + j) * cin + ci) * 27 + t;
+    if (part) part[(size_t) c * cout * cin * 27 + w] = s;
+    else gw[w] += s;
   }
+}
+
+__global__ void k_wgrad_finish(const float *__restrict__ part, float *__restrict__ gw, long n, int nchunk) {
+  const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float s = 0.f;
+  for (int c = 0; c < nchunk; c++) s += part[(size_t) c * n + i];
+  gw[i] += s;
 }
 
 // gb[co] += sum_p gy[co][p]; one block per output channel.
@@ -349,8 +379,23 @@ extern "C" int gb_unet_conv3_bwd_weight(const float *x, const float *gy, float *
                                         int h, int wd) {
   if (shape_ok("gb_unet_conv3_bwd_weight: bad shape", cin, cout, (long) d * h, wd)) return 1101;
   const long vol = (long) d * h * wd;
-  k_conv3_bwd_weight<<<dim3(cin, cout), kThreads, 0, gb__stream()>>>(x, gy, gw, cin, d, h, wd);
+  // Voxel chunks of at least 2048 (at most 16 chunks): enough CTAs at 32^3,
+  // one chunk (no partials) at 8^3 and below.
+  const int nchunk = (int) std::min<long>(16, std::max<long>(1, vol / 2048));
+  const long chunk = (vol + nchunk - 1) / nchunk;
+  float *part = nullptr;
+  if (nchunk > 1) {
+    part = (float *) gb__scratch(GB_SCR_UNET, (size_t) nchunk * cout * cin * 27 * sizeof(float));
+    if (!part) return gb_last_error();
+  }
+  k_conv3_bwd_weight<<<dim3(cin, (cout + kWCo - 1) / kWCo, nchunk), kWThreads, 0, gb__stream()>>>(x, gy, gw, part, cin, cout,
+                                                                                               d, h, wd, chunk);
   GB_CHECK_LAUNCH("gb_unet_conv3_bwd_weight");
+  if (part) {
+    const long n = (long) cout * cin * 27;
+    k_wgrad_finish<<<blocks_for(n), kThreads, 0, gb__stream()>>>(part, gw, n, nchunk);
+    GB_CHECK_LAUNCH("gb_unet_conv3_bwd_weight finish");
+  }
   if (gb) {
     k_bias_grad<<<cout, kThreads, 0, gb__stream()>>>(gy, gb, vol);
     GB_CHECK_LAUNCH("gb_unet_conv3_bwd_bias");
