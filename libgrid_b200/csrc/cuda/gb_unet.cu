@@ -177,23 +177,31 @@ constexpr int kWThreads = 128;
 constexpr int kWCo = 4;
 
 __global__ void __launch_bounds__(kWThreads) k_conv3_bwd_weight(const float *__restrict__ x, const float *__restrict__ gy,
-                                                                float *__restrict__ gw, float *__restrict__ part,
-                                                                int cin, int cout, int d, int h, int wd, long chunk) {
-  __shared__ float red[kWThreads / 32][kWCo * 27];
+                                                                float *__restrict__ gw, float *__restrict__ gbias,
+                                                                float *__restrict__ part, int cin, int cout, int d, int h,
+                                                                int wd, long chunk, int nchunk) {
+  __shared__ float red[kWThreads / 32][kWCo * 28];  // 27 taps, then the bias sum, per output channel
   const int ci = blockIdx.x, co0 = blockIdx.y * kWCo, c = blockIdx.z;
   const int nco = min(kWCo, cout - co0);
   const long vol = (long) d * h * wd;
   const long p0 = (long) c * chunk, p1 = min(vol, p0 + chunk);
   const float *xc = x + (size_t) ci * vol;
-  float acc[kWCo][27];
+  const bool dob = gbias != nullptr && ci == 0;  // the ci = 0 CTAs also sum the bias gradient
+  float acc[kWCo][27], bs[kWCo];
 #pragma unroll
-  for (int j = 0; j < kWCo; j++)
+  for (int j = 0; j < kWCo; j++) {
+    bs[j] = 0.f;
 #pragma unroll
     for (int t = 0; t < 27; t++) acc[j][t] = 0.f;
+  }
   for (long p = p0 + threadIdx.x; p < p1; p += kWThreads) {
     float g[kWCo];
 #pragma unroll
     for (int j = 0; j < kWCo; j++) g[j] = (j < nco) ? gy[(size_t) (co0 + j) * vol + p] : 0.f;
+    if (dob) {
+#pragma unroll
+      for (int j = 0; j < kWCo; j++) bs[j] += g[j];
+    }
     const int ix = (int) (p % wd), iy = (int) ((p / wd) % h), iz = (int) (p / ((long) wd * h));
 #pragma unroll
     for (int t = 0; t < 27; t++) {
@@ -213,14 +221,30 @@ __global__ void __launch_bounds__(kWThreads) k_conv3_bwd_weight(const float *__r
       for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
       if (lane == 0) red[warp][j * 27 + t] = v;
     }
+  if (dob) {
+#pragma unroll
+    for (int j = 0; j < kWCo; j++) {
+      float v = bs[j];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) red[warp][kWCo * 27 + j] = v;
+    }
+  }
   __syncthreads();
+  const size_t nw = (size_t) cout * cin * 27;
   for (int i = threadIdx.x; i < nco * 27; i += kWThreads) {
     float s = 0.f;
     for (int k = 0; k < kWThreads / 32; k++) s += red[k][i];
     const int j = i / 27, t = i % 27;
     const size_t w = ((size_t) (co0 + j) * cin + ci) * 27 + t;
-    if (part) part[(size_t) c * cout * cin * 27 + w] = s;
+    if (part) part[(size_t) c * nw + w] = s;
     else gw[w] += s;
+  }
+  if (dob && threadIdx.x < nco) {
+    float s = 0.f;
+    for (int k = 0; k < kWThreads / 32; k++) s += red[k][kWCo * 27 + threadIdx.x];
+    // bias partials follow the nchunk weight-partial blocks
+    if (part) part[(size_t) nchunk * nw + (size_t) c * cout + co0 + threadIdx.x] = s;
+    else gbias[co0 + threadIdx.x] += s;
   }
 }
 
@@ -230,22 +254,6 @@ __global__ void k_wgrad_finish(const float *__restrict__ part, float *__restrict
   float s = 0.f;
   for (int c = 0; c < nchunk; c++) s += part[(size_t) c * n + i];
   gw[i] += s;
-}
-
-// gb[co] += sum_p gy[co][p]; one block per output channel.
-__global__ void __launch_bounds__(kThreads) k_bias_grad(const float *__restrict__ gy, float *__restrict__ gb, long vol) {
-  __shared__ float red[kThreads / 32];
-  const float *gc = gy + (size_t) blockIdx.x * vol;
-  float s = 0.f;
-  for (long p = threadIdx.x; p < vol; p += blockDim.x) s += gc[p];
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    float t = 0.f;
-    for (int k = 0; k < kThreads / 32; k++) t += red[k];
-    gb[blockIdx.x] += t;
-  }
 }
 
 __global__ void k_relu_bwd(float *__restrict__ gy, const float *__restrict__ y, long n) {
@@ -384,21 +392,22 @@ extern "C" int gb_unet_conv3_bwd_weight(const float *x, const float *gy, float *
   const int nchunk = (int) std::min<long>(16, std::max<long>(1, vol / 2048));
   const long chunk = (vol + nchunk - 1) / nchunk;
   float *part = nullptr;
+  const long nw = (long) cout * cin * 27;
   if (nchunk > 1) {
-    part = (float *) gb__scratch(GB_SCR_UNET, (size_t) nchunk * cout * cin * 27 * sizeof(float));
+    part = (float *) gb__scratch(GB_SCR_UNET, (size_t) nchunk * (nw + cout) * sizeof(float));
     if (!part) return gb_last_error();
   }
-  k_conv3_bwd_weight<<<dim3(cin, (cout + kWCo - 1) / kWCo, nchunk), kWThreads, 0, gb__stream()>>>(x, gy, gw, part, cin, cout,
-                                                                                               d, h, wd, chunk);
+  k_conv3_bwd_weight<<<dim3(cin, (cout + kWCo - 1) / kWCo, nchunk), kWThreads, 0, gb__stream()>>>(x, gy, gw, gb, part, cin,
+                                                                                               cout, d, h, wd, chunk,
+                                                                                               nchunk);
   GB_CHECK_LAUNCH("gb_unet_conv3_bwd_weight");
   if (part) {
-    const long n = (long) cout * cin * 27;
-    k_wgrad_finish<<<blocks_for(n), kThreads, 0, gb__stream()>>>(part, gw, n, nchunk);
+    k_wgrad_finish<<<blocks_for(nw), kThreads, 0, gb__stream()>>>(part, gw, nw, nchunk);
     GB_CHECK_LAUNCH("gb_unet_conv3_bwd_weight finish");
-  }
-  if (gb) {
-    k_bias_grad<<<cout, kThreads, 0, gb__stream()>>>(gy, gb, vol);
-    GB_CHECK_LAUNCH("gb_unet_conv3_bwd_bias");
+    if (gb) {
+      k_wgrad_finish<<<blocks_for(cout), kThreads, 0, gb__stream()>>>(part + (size_t) nchunk * nw, gb, cout, nchunk);
+      GB_CHECK_LAUNCH("gb_unet_conv3_bwd_bias finish");
+    }
   }
   return 0;
 }

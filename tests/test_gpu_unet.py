@@ -169,3 +169,22 @@ def test_warm_start_cuts_imaginary_time_steps(b200, lib):
           % (steps_g, steps_n, np.mean([r["steps_tf"] for r in rows]), max(r["de"] for r in rows)))
     assert steps_n < steps_g
     assert max(r["de"] for r in rows) < 1e-6
+
+
+def test_training_is_deterministic(b200, lib):
+    """No kernel uses atomics and every sum has a fixed order, so two
+    training runs from the same seed give bit-identical weights."""
+    rng = np.random.default_rng(21)
+    n = 16
+    xs = rng.standard_normal((4, 3, n, n, n)).astype(np.float32)
+    ys = np.abs(rng.standard_normal((4, n, n, n))).astype(np.float32)
+    out = []
+    for _ in range(2):
+        net = ws.DeviceUNet(b200, n, cin=3, seed=7)
+        try:
+            ws.train(net, xs, ys, epochs=3, batch=2, lr=1e-3, seed=3)
+            out.append(net.get("p"))
+        finally:
+            net.free()
+    assert np.array_equal(out[0], out[1])
+    assert np.any(out[0] != 0)
