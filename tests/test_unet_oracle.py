@@ -59,3 +59,36 @@ def test_oracle_gradients_match_finite_differences():
         lm, _ = uo.unet_loss_grads(spec, params, x, tgt)
         b[j] = old
         assert abs((lp - lm) / (2 * eps) - grads[layer][1][j]) <= 1e-5 * max(1.0, abs(grads[layer][1][j])) + 1e-8
+
+
+def test_warm_start_host_logic():
+    from libgrid_b200 import warmstart as ws
+
+    # the seeded problem family is reproducible and in its stated ranges
+    v1, g1, k1 = ws.sample_problem(1234, 16, 0.1)
+    v2, g2, k2 = ws.sample_problem(1234, 16, 0.1)
+    assert np.array_equal(v1, v2) and g1 == g2 and k1 == k2
+    assert 0.001 <= g1 <= 0.01 and 0.005 <= k1 <= 0.02
+    # Thomas-Fermi amplitude is normalised and vanishes where V > mu
+    v, g, _ = ws.sample_problem(7, 32, 0.1)
+    tf = ws.thomas_fermi(v, g, 0.1)
+    assert abs((tf**2).sum() * 0.1**3 - 1.0) < 1e-9
+    assert tf.min() == 0.0 and tf.max() > 0
+    x, s = ws.features(v, g, 0.1)
+    assert x.shape == (3, 32, 32, 32) and x.dtype == np.float32
+    assert abs(x[2].max() - 1.0) < 1e-6 and abs(s - tf.max()) < 1e-12
+    # network: every conv's input channels are its sources' channels, the
+    # skip concatenations pair equal resolutions, and the size is as stated
+    spec, chan = ws.unet_spec()
+    nparam = 0
+    for op in spec:
+        if op[0] == "conv":
+            ci = sum(chan[src] for src in op[1])
+            nparam += chan[op[2]] * ci * 27 + chan[op[2]]
+            assert len({ws._LEVEL[src] for src in op[1]}) == 1
+            assert ws._LEVEL[op[2]] == ws._LEVEL[op[1][0]]
+        elif op[0] == "pool":
+            assert ws._LEVEL[op[2]] == ws._LEVEL[op[1][0]] + 1
+        else:
+            assert ws._LEVEL[op[2]] == ws._LEVEL[op[1][0]] - 1
+    assert nparam == 365825
