@@ -297,17 +297,17 @@ def sample_problem(seed: int, n: int = 32, step: float = 0.1):
 
 
 def thomas_fermi(v, g, step):
-    """Normalised Thomas-Fermi amplitude sqrt(max(mu - V, 0) / g), mu by
-    bisection so that its norm is 1."""
+    """Normalised Thomas-Fermi amplitude sqrt(max(mu - V, 0) / g).  The norm
+    sum_{V_i < mu} (mu - V_i) dv / g is piecewise linear in mu: with the
+    potential sorted, the k lowest points give mu_k = (g / dv + S_k) / k, and
+    mu is the first mu_k that does not pass the next potential value."""
     dv = step**3
-    lo, hi = float(v.min()), float(v.min()) + 1.0
-    for _ in range(80):
-        mu = 0.5 * (lo + hi)
-        if np.maximum(mu - v, 0).sum() * dv / g > 1.0:
-            hi = mu
-        else:
-            lo = mu
-    return np.sqrt(np.maximum(hi - v, 0) / g)
+    vs = np.sort(v, axis=None)
+    k = np.arange(1, vs.size + 1)
+    mus = (g / dv + np.cumsum(vs)) / k
+    nxt = np.append(vs[1:], np.inf)
+    mu = mus[int(np.argmax(mus <= nxt))]
+    return np.sqrt(np.maximum(mu - v, 0) / g)
 
 
 def features(v, g, step):
@@ -427,21 +427,32 @@ def train(net: DeviceUNet, xs, ys, epochs=60, batch=8, lr=2e-3, seed=0, log=None
 
 
 def evaluate(api, net: DeviceUNet, seeds, n=32, step=0.1):
-    """Per held-out potential: steps and loop seconds to convergence from the
+    """Per held-out potential: steps and seconds to convergence from the
     Gaussian guess, from the Thomas-Fermi profile and from the network guess
-    (network inference time included), and the energy differences."""
+    (each including the host time to build its guess; for the network that is
+    the features and the inference), and the energy differences."""
     r = Relaxer(api, n, step)
     rows = []
     try:
         for sd in seeds:
             v, g, _ = sample_problem(sd, n, step)
-            _, e_g, st_g, t_g = r.relax(v, g, gaussian_guess(n, step))
-            x, s = features(v, g, step)
-            _, e_tf, st_tf, t_tf = r.relax(v, g, x[2] * s)
+            # each start is charged the time to prepare its guess on the host
             t0 = time.perf_counter()
+            guess = gaussian_guess(n, step)
+            t_g0 = time.perf_counter() - t0
+            _, e_g, st_g, t_g = r.relax(v, g, guess)
+            t0 = time.perf_counter()
+            x, s = features(v, g, step)
+            guess = x[2] * s
+            t_tf0 = time.perf_counter() - t0
+            _, e_tf, st_tf, t_tf = r.relax(v, g, guess)
+            t0 = time.perf_counter()
+            x, s = features(v, g, step)
             amp = np.maximum(net.predict(x), 0.0) * s + 1e-6
             t_inf = time.perf_counter() - t0
             _, e_n, st_n, t_n = r.relax(v, g, amp)
+            t_g += t_g0
+            t_tf += t_tf0
             rows.append(dict(seed=sd, steps_gauss=st_g, sec_gauss=t_g, steps_tf=st_tf, sec_tf=t_tf, steps_net=st_n,
                              sec_net=t_n + t_inf, e_gauss=e_g, e_net=e_n, de=abs(e_n - e_g)))
     finally:
