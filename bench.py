@@ -15,6 +15,10 @@ split-operator step of that wavefunction.
             psi copied back to the host
   fp32      the same step in the FP32 mode (FP64 phase reduction and FP64
             reductions), with its relative L2 distance from the FP64 result
+            and (err_vs_oracle_*) its psi, energy and norm errors against the
+            reference's FP64 trajectory after 1000 steps
+  oracle_agreement  FP64 and FP32 runs of 1000 steps against the
+            reference's own FP64 trajectory (tests/golden/gp256_traj.npz)
   roofline  the dominant line-pass kernel (per the ncu launch list): its
             algorithmic bytes per launch (32 B/pt: one read + one write of
             complex128) over its mean CUDA-event duration in the timed region
@@ -52,7 +56,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-METRIC = "GP 256^3 split-operator steps/s (FP64, resident in HBM)"
+# the same metric string in both arms (--impl b200 and --impl reference)
+METRIC = "GP 256^3 split-operator steps/s (FP64)"
 PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
 TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dram_traffic.json")
 FALLBACK_HBM = 6650.0
@@ -197,6 +202,8 @@ def allmax(world, x):
 
 
 def cpu_baseline(size: int, steps: int, warmup: int, threads: int | None = None):
+    """Time the reference's CPU step (python -m oracle.refbench) in a child
+    process; returns its JSON record."""
     env = dict(os.environ)
     env.setdefault("OMP_PROC_BIND", "TRUE")
     env.setdefault("OMP_WAIT_POLICY", "ACTIVE")
@@ -215,17 +222,19 @@ def run_reference(args, world, rank):
     if rank != 0:
         return 0
     nproc = len(os.sched_getaffinity(0))
-    # a bounded sample of the workload: at most 60 timed steps (~20 s on 16
-    # host cores at 256^3) after at most 2 warm-up steps
-    r = cpu_baseline(args.size, min(args.steps, 60), min(args.warmup, 2))
+    # a bounded sample of the workload (about 0.3 s per 256^3 step on 16 host
+    # cores): K timed steps after W warm-up steps, capped at 300 and 10 so the
+    # arm ends within a few minutes; the line reports the counts that ran
+    steps, warmup = min(args.steps, 300), min(args.warmup, 10)
+    r = cpu_baseline(args.size, steps, warmup)
     line = {
         "impl": "reference",
-        "metric": METRIC.replace("(FP64, resident in HBM)", "(FP64)"),
+        "metric": METRIC,
         "value": r["steps_per_s"],
         "unit": "steps/s",
         "n_gpus": args.gpus,
-        "steps": args.steps,
-        "warmup": args.warmup,
+        "steps": steps,
+        "warmup": warmup,
         "ms_per_step": 1e3 / r["steps_per_s"],
         "higher_is_better": True,
         "scaling": "weak",
@@ -299,6 +308,59 @@ def run_batch2d(api, lib, prec, steps, world):
         "note": "a step = one 2nd-order split-operator step of every instance; sequential = the same instances "
         "through grid_wf_propagate one at a time",
     }
+
+
+TRAJ_FILE = os.path.join(ROOT, "tests", "golden", "gp256_traj.npz")
+
+
+def oracle_agreement(api, lib, make, g):
+    """FP64 and FP32-mode runs of the 256^3 GP workload (1000 steps from the
+    same start) against the reference's own FP64 trajectory, which the
+    committed fixture tests/golden/gp256_traj.npz holds (psi at a seeded
+    subset of 16384 points, plus full-grid norm, kinetic energy (FFT
+    method), <V_ext> and (g/2) int |psi|^4 at steps 50, 500 and 1000, from
+    libgrid's CPU sources).  Reports per mode and checkpoint the relative
+    L2 distance of psi over the subset and the relative errors of the total
+    energy and of the norm, plus the norm drift of the run."""
+    from libgrid_b200 import capi
+
+    if not os.path.exists(TRAJ_FILE):
+        return {"error": "missing fixture " + os.path.relpath(TRAJ_FILE, ROOT)}
+    z = np.load(TRAJ_FILE)
+    idx = z["idx"]
+    cps = sorted(int(k[4:]) for k in z.files if k.startswith("psi_") and k != "psi_0")
+
+    def fixture_energy(s):
+        return float(z["ekin_%d" % s]) + float(z["epot_%d" % s]) + float(z["eint_%d" % s])
+
+    out = {"reference": "libgrid CPU path (oracle/_ref) with the project's FFTW stand-in, FP64", "checkpoints": cps}
+    for prec, name in ((0, "fp64"), (capi.GRID_PREC_FP32, "fp32")):
+        w, vx = make()
+        if prec:
+            w.precision(prec)
+        n0 = w.norm()
+        rows, done = {}, 0
+        for s in cps:
+            for _ in range(s - done):
+                w.propagate_gp(vx, g, 1.0)
+            done = s
+            psi = w.grid.get()
+            rho = psi.real * psi.real + psi.imag * psi.imag
+            e = (lib.grid_wf_kinetic_energy_fft(w.ptr) + lib.grid_grid_expectation_value(w.s.grid, vx.ptr)
+                 + 0.5 * g * float(np.sum(rho * rho)) * w.s.grid.contents.step ** 3)
+            nrm = w.norm()
+            sub_psi = psi.ravel()[idx]
+            ref_psi = z["psi_%d" % s]
+            rows[str(s)] = {
+                "psi_rel_l2": float(np.linalg.norm(sub_psi - ref_psi) / np.linalg.norm(ref_psi)),
+                "energy_rel": abs(e - fixture_energy(s)) / abs(fixture_energy(s)),
+                "norm_rel": abs(nrm - float(z["norm_%d" % s])) / float(z["norm_%d" % s]),
+            }
+        rows["norm_drift_rel"] = abs(nrm - n0) / n0
+        out[name] = rows
+        api.free(w)
+        api.free(vx)
+    return out
 
 
 def run_b200(args, world, rank, local):
@@ -421,6 +483,9 @@ def run_b200(args, world, rank, local):
     api.free(w)
     api.free(vx)
 
+    # ------------------- agreement with the reference's FP64 trajectory
+    agreement = oracle_agreement(api, lib, make, g) if (rank == 0 and n == 256 and not args.no_oracle) else None
+
     # ---------------------------------- batched uneven 2-D (one launch/call)
     batch = {}
     if not args.no_batch:
@@ -467,6 +532,7 @@ def run_b200(args, world, rank, local):
             "dt": dt,
             "propagator": "2nd-order FFT split operator, V_ext + g|psi|^2 in-kernel",
             "l2": "inputs (403 MB) larger than L2 (126 MB); no flush",
+            "residency": "value: psi and V_ext resident in HBM; e2e: from pinned host buffers through the C API",
             "parallelism": "replicas x%d" % world,
         },
         "fp32": {
@@ -477,6 +543,7 @@ def run_b200(args, world, rank, local):
             "rel_l2_vs_fp64_after_steps": err32,
             "steps_compared": done + args.steps,
         },
+        "oracle_agreement": agreement,
         "roofline": {
             "bound": "hbm",
             "kernel": dom[0],
@@ -514,6 +581,11 @@ def run_b200(args, world, rank, local):
         },
         "clocks": clk.summary(),
     }
+    if agreement and "fp32" in agreement:
+        last = str(max(agreement["checkpoints"]))
+        r = agreement["fp32"][last]
+        line["fp32"].update(err_vs_oracle_psi=r["psi_rel_l2"], err_vs_oracle_energy=r["energy_rel"],
+                            err_vs_oracle_norm=r["norm_rel"], err_vs_oracle_steps=int(last))
     if world == 1 and not args.no_warm_start:
         line["warm_start"] = warm_start_report()
     if world == 1 and not args.no_cpu_baseline:
@@ -566,6 +638,7 @@ def main(argv=None):
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-warm-start", action="store_true")
+    ap.add_argument("--no-oracle", action="store_true")
     ap.add_argument("--batch-steps", type=int, default=200)
     args = ap.parse_args(argv)
     world, rank, local = dist_setup()

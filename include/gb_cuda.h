@@ -109,10 +109,32 @@ int gb_convert_f32_to_f64(void *dst, const void *src, size_t n);
 /* Host FP64 array <-> device FP32 array (n scalars), staged on the device. */
 int gb_upload_f64_as_f32(void *dev32, const void *host64, size_t n);
 int gb_download_f32_as_f64(void *host64, const void *dev32, size_t n);
-/* Status word of the bounded device-side waits (0 = none timed out). */
+/* Status words of the bounded device-side waits (0 = no wait gave up).
+ * Every host sync point of this layer (gb_synchronize, gb_d2h and every
+ * reduction that returns a value) reads them and latches a nonzero word into
+ * gb_last_error() with code GB_ERR_DEVICE_WAIT; the libgrid entry points then
+ * abort with a libgrid message, as for any device failure.  A propagation
+ * call itself does not wait for the GPU, so its failure surfaces at the next
+ * read of a result (a norm, an energy, a host copy of a grid).
+ * gb_clear_error() clears the words.  (No reference counterpart: the
+ * reference's kernels have no device-side waits.) */
+#define GB_ERR_DEVICE_WAIT 1070
+#define GB_STATUS_PASS 0  /* pipelined line pass copy wait, plane-chain dependency wait */
+#define GB_STATUS_CN 1    /* Crank-Nicolson sweep copy wait */
+#define GB_STATUS_BATCH 2 /* batch grid barrier */
+#define GB_STATUS_WORDS 4
 int gb_cn_error_flag(void);
-/* Same for the pipelined FFT line passes; reset != 0 clears it. */
+/* Same for the pipelined FFT line passes and the plane chains; reset != 0
+ * clears it. */
 int gb_pass_error_flag(int reset);
+/* Poll limit of the waits that only wait for other CTAs' progress (the
+ * plane chain's dependency wait and the batch kernel's grid barrier); 0
+ * restores each wait's built-in limit (about a second).  Returns the
+ * previous setting.  A small limit makes those waits give up early, which is
+ * reported as above; it exists so tests can exercise that path.  Copy waits
+ * (TMA, bulk copies) always keep their built-in limit.  (No reference
+ * counterpart.) */
+unsigned gb_wait_limit(unsigned polls);
 /* Pipelined (persistent, TMA-prefetching) strided line passes: on = 1
  * enables (the default), 0 disables, -1 only queries.  Returns the previous
  * setting.  Both forms compute the same values.  (No reference counterpart.) */
@@ -125,6 +147,12 @@ int gb_pass_pipeline(int on);
  * default), 0 disables, -1 only queries; returns the previous setting.  Both
  * schedules compute the same values.  (No reference counterpart.) */
 int gb_plane_passes(int on);
+/* Ticket lag of the plane-chained passes, in percent of one resident wave of
+ * tiles (default 200): the second stage of a plane is issued that far behind
+ * its first stage, so it rarely waits.  Any value >= 0 is free of deadlock and
+ * computes the same values; -1 only queries.  Returns the previous setting.
+ * (No reference counterpart.) */
+int gb_chain_lag(int pct);
 
 /* ----------------------------------------------------------------- FFT */
 /* In-place 3-D complex FFT, unnormalised, then multiplied by scale

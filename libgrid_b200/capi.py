@@ -233,6 +233,13 @@ def bind(lib: C.CDLL, cuda_layout: bool, extensions: bool):
         f("gb_grid_host_modified", None, V)
         f("gb_last_error", C.c_int)
         f("gb_synchronize", C.c_int)
+        f("gb_clear_error", None)
+        f("gb_last_error_where", C.c_char_p)
+        f("gb_wait_limit", C.c_uint, C.c_uint)
+        f("gb_chain_lag", C.c_int, C.c_int)
+        f("gb_pass_error_flag", C.c_int, C.c_int)
+        f("gb_cn_error_flag", C.c_int)
+        f("gb_batch_error_flag", C.c_int, V, C.c_int)
         f("gb_launch_count", L)
         f("gb_event_record", C.c_int, C.c_int)
         f("gb_event_elapsed_ms", C.c_float, C.c_int, C.c_int)

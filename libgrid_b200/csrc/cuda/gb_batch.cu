@@ -45,14 +45,15 @@ struct BatchDev {
   const BatchTile *stiles;
   int nct, nst;
   unsigned *bar;  // [0] arrivals, [1] generation
-  int *err;
+  int *err;       // status word GB_STATUS_BATCH
+  unsigned wait_limit;
 };
 
 #define GB_GRID_WAIT_LIMIT (1u << 24)
 
 // Grid-wide barrier of a cooperative launch (all CTAs resident).  Returns
 // false on every thread of a CTA whose wait gave up (error flag set).
-__device__ __forceinline__ bool batch_grid_barrier(unsigned *bar, int *err) {
+__device__ __forceinline__ bool batch_grid_barrier(unsigned *bar, int *err, unsigned limit) {
   __syncthreads();
   int ok = 1;
   if (threadIdx.x == 0) {
@@ -66,7 +67,7 @@ __device__ __forceinline__ bool batch_grid_barrier(unsigned *bar, int *err) {
     } else {
       unsigned it = 0;
       while (*gen == g0) {
-        if (++it > GB_GRID_WAIT_LIMIT) {
+        if (++it > limit) {
           atomicExch(err, 1);
           ok = 0;
           break;
@@ -183,7 +184,7 @@ __global__ void __launch_bounds__(THREADS, pass_min_blocks<THREADS, sizeof(T)>()
           batch_strided<T, THREADS, OP_FWD, OP_KIN, OP_INV>(d.inst[bt.inst], bt.tile, smraw);
         }
       }
-      if (!batch_grid_barrier(d.bar, d.err)) return;
+      if (!batch_grid_barrier(d.bar, d.err, d.wait_limit)) return;
     }
   }
 }
@@ -301,7 +302,6 @@ struct gb_batch {
   int ntiles[3][2];
   unsigned char *d_kin;
   unsigned *d_bar;
-  int *d_err;
   int grid[3];
   int threads;  // chosen plan: persistent CTA size, -1 for the class graph, 0 until tuned
   // per-shape-class plan: instances ordered by class, one stream per class,
@@ -346,9 +346,15 @@ template <typename T, int THREADS> static int batch_launch(gb_batch *b, int step
   d.nct = b->ntiles[v][0];
   d.nst = b->ntiles[v][1];
   d.bar = b->d_bar;
-  d.err = b->d_err;
+  d.err = gb__status(GB_STATUS_BATCH);
+  if (!d.err) return gb_last_error();
+  d.wait_limit = gb__wait_limit(GB_GRID_WAIT_LIMIT);
   void *args[] = {&d, &steps};
   constexpr size_t sm = batch_smem<T, THREADS>();
+  // every launch starts from a clear barrier: a CTA whose wait gave up in an
+  // earlier launch leaves its arrival counted
+  if (cudaMemsetAsync(b->d_bar, 0, 2 * sizeof(unsigned), gb__stream()) != cudaSuccess)
+    return gb__set_error(1044, "batch: barrier reset");
   const cudaError_t e = cudaLaunchCooperativeKernel((const void *) k_batch_steps<T, THREADS>, dim3(b->grid[v]),
                                                     dim3(THREADS), args, sm, gb__stream());
   gb__count_launch();
@@ -396,7 +402,7 @@ extern "C" gb_batch *gb_batch_create(const gb_batch_item *items, int n) {
     kbytes += (tot * (esz + 8) + 255) & ~(size_t) 255;
   }
   if (cudaMalloc(&b->d_kin, kbytes) != cudaSuccess || cudaMalloc(&b->d_inst, sizeof(BatchInst) * n) != cudaSuccess ||
-      cudaMalloc(&b->d_bar, 2 * sizeof(unsigned)) != cudaSuccess || cudaMalloc(&b->d_err, sizeof(int)) != cudaSuccess) {
+      cudaMalloc(&b->d_bar, 2 * sizeof(unsigned)) != cudaSuccess) {
     cudaGetLastError();
     gb__set_error(2, "batch: cudaMalloc");
     gb_batch_free(b);
@@ -404,7 +410,6 @@ extern "C" gb_batch *gb_batch_create(const gb_batch_item *items, int n) {
   }
   cudaStream_t st = gb__stream();
   cudaMemsetAsync(b->d_bar, 0, 2 * sizeof(unsigned), st);
-  cudaMemsetAsync(b->d_err, 0, sizeof(int), st);
   std::vector<BatchInst> hi(n);
   for (int i = 0; i < n; i++) {
     const gb_batch_item &it = items[i];
@@ -591,13 +596,11 @@ extern "C" int gb_batch_step(gb_batch *b, int steps) {
 
 extern "C" int gb_batch_threads(const gb_batch *b) { return b ? b->threads : 0; }
 
+// The grid barrier's status word (shared by all batches on the library
+// stream); reset != 0 clears it.
 extern "C" int gb_batch_error_flag(gb_batch *b, int reset) {
-  if (!b || !b->d_err) return 0;
-  int h = 0;
-  cudaStreamSynchronize(gb__stream());
-  cudaMemcpy(&h, b->d_err, sizeof(int), cudaMemcpyDeviceToHost);
-  if (reset) cudaMemset(b->d_err, 0, sizeof(int));
-  return h;
+  if (!b) return 0;
+  return gb__status_word(GB_STATUS_BATCH, reset);
 }
 
 extern "C" void gb_batch_free(gb_batch *b) {
@@ -608,7 +611,6 @@ extern "C" void gb_batch_free(gb_batch *b) {
     for (int k = 0; k < 2; k++) cudaFree(b->d_tiles[v][k]);
   cudaFree(b->d_kin);
   cudaFree(b->d_bar);
-  cudaFree(b->d_err);
   cudaFree(b->d_cinst);
   if (b->graph) cudaGraphExecDestroy(b->graph);
   for (int c = 0; c < b->ncls; c++) {

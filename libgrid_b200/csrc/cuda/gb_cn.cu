@@ -534,7 +534,6 @@ static long largest_pow2_divisor(long v, long cap) {
   return p;
 }
 
-static int *g_err_flag = nullptr;
 
 // Per-axis table cache: rebuilt and uploaded only when (n, bc, cp, c2)
 // change, so a run of identical steps issues no host transfers.
@@ -587,10 +586,8 @@ static double2 *fast_tables(int slot, long n, int bc, cd cp, cd c2, cudaStream_t
 extern "C" int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, const gb_potential *pre,
                           const gb_potential *post) {
   if (g->prec != GB_FP64) return gb__set_error(1010, "cn: FP64 storage required");
-  if (!g_err_flag) {
-    if (cudaMalloc(&g_err_flag, sizeof(int)) != cudaSuccess) return gb__set_error(2, "cn err flag");
-    cudaMemset(g_err_flag, 0, sizeof(int));
-  }
+  int *err_flag = gb__status(GB_STATUS_CN);
+  if (!err_flag) return gb_last_error();
   cudaStream_t st = gb__stream();
   const cd c = cd(0.0, 4.0) * p->mass * g->step * g->step / 1.0;  // 4 i m h^2 / hbar (hbar = 1)
   const cd tstep(p->tstep_re, p->tstep_im);
@@ -622,7 +619,7 @@ extern "C" int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, co
     a.axis = axis;
     a.boundary = p->boundary;
     a.step = g->step;
-    a.err = g_err_flag;
+    a.err = err_flag;
     a.c = make_double2(c.real(), c.imag());
     a.tstep = make_double2(p->tstep_re, p->tstep_im);
     const double k0 = axis == 0 ? p->kx0 : (axis == 1 ? p->ky0 : p->kz0);
@@ -731,10 +728,5 @@ extern "C" int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, co
   return 0;
 }
 
-// Error flag written by bounded waits that gave up (0 = none).
-extern "C" int gb_cn_error_flag(void) {
-  if (!g_err_flag) return 0;
-  int h = 0;
-  cudaMemcpy(&h, g_err_flag, sizeof(int), cudaMemcpyDeviceToHost);
-  return h;
-}
+// Status word written by the bounded copy waits that gave up (0 = none).
+extern "C" int gb_cn_error_flag(void) { return gb__status_word(GB_STATUS_CN, 0); }

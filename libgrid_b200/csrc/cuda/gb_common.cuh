@@ -181,6 +181,9 @@ extern "C" cudaStream_t gb__stream(void);
 // and must record an error and leave without touching the data.
 #define GB_WAIT_LIMIT (1u << 22)
 
+// Devices for which per-device launch geometry is cached.
+constexpr int kMaxDevices = 64;
+
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned) __cvta_generic_to_shared(p); }
 
 // Per-thread asynchronous global -> shared copy of one 4- or 8-byte element

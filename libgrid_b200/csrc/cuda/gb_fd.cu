@@ -230,7 +230,7 @@ extern "C" int gb_fd_kinetic_sum(const void *psi, const gb_geom *g, int bc, doub
   if (nb > 148 * 8) nb = 148 * 8;
   if (nb < 1) nb = 1;
   double2 *partial = (double2 *) gb__scratch(GB_SCR_PARTIAL, sizeof(double2) * (size_t) nb);
-  double2 *res = (double2 *) gb__scratch(GB_SCR_RESULT, 64);
+  double2 *res = (double2 *) gb__result_slot();
   if (!partial || !res) return gb_last_error();
   cudaStream_t st = gb__stream();
   if (g->prec == GB_FP32) k_fd_kinetic<float><<<(unsigned) nb, 256, 0, st>>>((const float2 *) psi, a, partial);
@@ -239,7 +239,7 @@ extern "C" int gb_fd_kinetic_sum(const void *psi, const gb_geom *g, int bc, doub
   k_finish_fd<<<1, 32, 0, st>>>(partial, (int) nb, res);
   GB_CHECK_LAUNCH("fd kinetic finish");
   double2 h;
-  int rc = gb_d2h(&h, res, sizeof(double2));
+  int rc = gb__read_result(&h, sizeof(double2));
   out[0] = h.x;
   out[1] = h.y;
   return rc;

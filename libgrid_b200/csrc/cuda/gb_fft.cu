@@ -130,11 +130,11 @@ __global__ void k_sum_partials(const double *__restrict__ p, long n, double *out
 }
 
 int gb__sum_partials(const double *partial, long n, double *out_host) {
-  double *res = (double *) gb__scratch(GB_SCR_RESULT, 64);
+  double *res = (double *) gb__result_slot();
   if (!res) return gb_last_error();
   k_sum_partials<<<1, 1024, 0, gb__stream()>>>(partial, n, res);
   GB_CHECK_LAUNCH("sum partials");
-  return gb_d2h(out_host, res, sizeof(double));
+  return gb__read_result(out_host, sizeof(double));
 }
 
 // ------------------------------------------------- standalone pointwise ops

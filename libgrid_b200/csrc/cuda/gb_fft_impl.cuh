@@ -733,10 +733,13 @@ int launch_strided_pipe(const void *src, void *dst, const PassArgs &a, long oute
     constexpr size_t SM = 2 * (size_t) N * BZ * sizeof(T2) + 128;
     constexpr int THREADS = (N / Sched<N>::P) * BZ;
     auto kern = k_pass_strided_pipe<T, N, BZ, Ops...>;
-    static int rgrid = 0;
+    // resident CTAs per device (0: not yet known, -1: the kernel does not fit)
+    static int rgrids[kMaxDevices] = {};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    int &rgrid = rgrids[dev >= 0 && dev < kMaxDevices ? dev : 0];
     if (!rgrid) {
-      int dev = 0, nsm = 0, per = 0;
-      cudaGetDevice(&dev);
+      int nsm = 0, per = 0;
       cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
       cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) SM);
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, THREADS, SM);

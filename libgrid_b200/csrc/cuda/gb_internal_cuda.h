@@ -29,8 +29,23 @@ const void *gb__twiddles(long n, int prec);
 // complex grid (fp32 = 0: double2 elements, 1: float2), read as reals with
 // the box 2*bz reals x rows lines x 1.  Cached per argument set.
 int gb__tmap_lines(CUtensorMap *out, const void *base, long outer, long n, long inner, int fp32, int bz, int rows);
-// Device flag set by a pipelined pass whose bounded wait gave up.
+// Device flag set by a pipelined pass or plane chain whose bounded wait gave
+// up (status word GB_STATUS_PASS).
 int *gb__pass_errflag(void);
+// Device address of a status word (GB_STATUS_*), allocated on first use.
+int *gb__status(int word);
+// Read (and with reset != 0 clear) one status word after draining the stream.
+int gb__status_word(int word, int reset);
+// Poll limit for waits on other CTAs' progress: gb_wait_limit's setting, or
+// dflt when none is set.
+unsigned gb__wait_limit(unsigned dflt);
+// Plane-chain lag in percent of one resident wave of tickets (gb_chain_lag).
+int gb__chain_lag_pct(void);
+// Device slot for a reduction result (32 bytes) and its read-back: one copy
+// brings the result and the status words; a nonzero status word latches
+// GB_ERR_DEVICE_WAIT.
+void *gb__result_slot(void);
+int gb__read_result(void *host, size_t bytes);
 
 // Kinetic factor tables for (g, kin): per-axis complex factors exp(tm k_a^2)
 // in the storage precision of g and per-axis k_a^2 in FP64.

@@ -254,8 +254,7 @@ static void launch_reduce(int op, int nb, cudaStream_t st, const void *a, const 
     GB_RED_CASE(GB_RED_EXPECT_COMPLEX)
     GB_RED_CASE(GB_RED_EXPECT_REAL)
     GB_RED_CASE(GB_RED_REAL_SUM)
-    default:
-      GB_RED_CASE(GB_RED_KSQ_NORM2)
+    GB_RED_CASE(GB_RED_KSQ_NORM2)
   }
 #undef GB_RED_CASE
 }
@@ -356,12 +355,15 @@ static int reduce_blocks(size_t n) {
   return (int) b;
 }
 
+static bool reduce_op_ok(int op) { return op >= GB_RED_SUM && op <= GB_RED_KSQ_NORM2; }
+
 extern "C" int gb_reduce(int op, const void *a, const void *b, const gb_geom *g, long arow, long brow, int bprec, double *out) {
+  if (!reduce_op_ok(op)) return gb__set_error(1023, "gb_reduce: unknown reduction op");
   const long nxy = g->nx * g->ny;
   const size_t n = (size_t) nxy * g->nz;
   const int nb = reduce_blocks(n);
   double2 *partial = (double2 *) gb__scratch(GB_SCR_PARTIAL, sizeof(double2) * (size_t) (nb + 1));
-  double2 *res = (double2 *) gb__scratch(GB_SCR_RESULT, 64);
+  double2 *res = (double2 *) gb__result_slot();
   if (!partial || !res) return gb_last_error();
   cudaStream_t st = gb__stream();
   const bool af = (g->prec == GB_FP32);
@@ -374,7 +376,7 @@ extern "C" int gb_reduce(int op, const void *a, const void *b, const gb_geom *g,
   k_finish2<<<1, 1024, 0, st>>>(partial, nb, res);
   GB_CHECK_LAUNCH("reduce finish");
   double2 h;
-  int rc = gb_d2h(&h, res, sizeof(double2));
+  int rc = gb__read_result(&h, sizeof(double2));
   out[0] = h.x;
   out[1] = h.y;
   return rc;
@@ -502,6 +504,7 @@ __global__ void k_finish_noalloc(double2 *scratch, int nb) {
 
 extern "C" int gb_reduce_noalloc(int op, const void *a, const void *b, const gb_geom *g, long arow, long brow, int bprec,
                                  double *out) {
+  if (!reduce_op_ok(op)) return gb__set_error(1023, "gb_reduce_noalloc: unknown reduction op");
   const long nxy = g->nx * g->ny;
   const double npts = (double) nxy * (double) g->nz;
   if (npts > (double) (kNoallocMaxBlocks * kNoallocBlockElems)) {

@@ -17,12 +17,10 @@
 #pragma once
 
 #include "gb_fft_impl.cuh"
+#include "gb_internal_cuda.h"
 
 namespace gbfft {
 
-#ifndef GB_CHAIN_LAG_PCT
-#define GB_CHAIN_LAG_PCT 200
-#endif
 
 template <int AX, int... Ops> struct Stage {};
 
@@ -44,6 +42,7 @@ struct ChainArgs {
   int *cnt;           // [stage][plane] completed tiles
   unsigned *ticket;   // ticket counter
   int nplanes, lag;
+  unsigned wait_limit;  // polls before a dependency wait gives up
 };
 
 template <int AX, int... Ops> __host__ __device__ constexpr bool stage_has_pot(Stage<AX, Ops...>) {
@@ -141,7 +140,7 @@ __global__ void __launch_bounds__(ChainCfg<T, N>::THREADS, chain_minb<T, N, Stag
         const int *f = c.cnt + (size_t) (s - 1) * np + p;
         unsigned n = 0;
         while (ld_acquire(f) < (int) TILES) {
-          if (++n > GB_WAIT_LIMIT) {
+          if (++n > c.wait_limit) {
             atomicOr(c.ay.errflag, 8);
             break;
           }
@@ -176,10 +175,13 @@ int launch_chain(void *psi, long nx, const ChainArgs &base, int *counters) {
   constexpr int S = sizeof...(Stages);
   auto kern = k_chain<T, N, Stages...>;
   constexpr size_t smem = chain_smem<T, N, Stages...>();
-  static int rgrid = 0;  // resident CTAs, -1 when the kernel does not fit
+  // resident CTAs per device (0: not yet known, -1: the kernel does not fit)
+  static int rgrids[kMaxDevices] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int &rgrid = rgrids[dev >= 0 && dev < kMaxDevices ? dev : 0];
   if (!rgrid) {
-    int dev = 0, nsm = 0, per = 0;
-    cudaGetDevice(&dev);
+    int nsm = 0, per = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, Cfg::THREADS, smem);
@@ -187,15 +189,17 @@ int launch_chain(void *psi, long nx, const ChainArgs &base, int *counters) {
     rgrid = (nsm > 0 && per > 0) ? nsm * per : -1;
   }
   if (rgrid < 0) return gb__set_error(1062, "chained pass: kernel does not fit");
-  // lag: about GB_CHAIN_LAG_PCT percent of one resident wave of tickets, so
-  // most tiles of a stage find their plane's previous stage complete
+  // lag: about gb_chain_lag's percentage (default 200) of one resident wave
+  // of tickets, so most tiles of a stage find their plane's previous stage
+  // complete; any lag >= 0 is free of deadlock
   const long group = (long) S * Cfg::TILES;
-  const int lag = (int) (((long) rgrid * GB_CHAIN_LAG_PCT / 100 + group - 1) / group);
+  const int lag = (int) (((long) rgrid * gb__chain_lag_pct() / 100 + group - 1) / group);
   ChainArgs c = base;
   c.cnt = counters;
   c.ticket = (unsigned *) (counters + (size_t) S * nx);
   c.nplanes = (int) nx;
   c.lag = lag;
+  c.wait_limit = gb__wait_limit(GB_WAIT_LIMIT);
   cudaStream_t st = gb__stream();
   if (cudaMemsetAsync(counters, 0, sizeof(int) * ((size_t) S * nx + 1), st) != cudaSuccess)
     return gb__set_error(1063, "chained pass: counter reset failed");

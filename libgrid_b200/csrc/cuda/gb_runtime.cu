@@ -36,6 +36,16 @@ struct Twiddle {
 };
 static Twiddle g_tw[13];  // index log2(n), n = 2 .. 4096
 
+// Device status block (see "device status" below).
+struct IoBlock {
+  double2 result[2];
+  int status[GB_STATUS_WORDS];
+  int pad[16 - GB_STATUS_WORDS];
+};
+static IoBlock *g_io = nullptr;       // device
+static IoBlock *g_io_host = nullptr;  // pinned mirror
+static unsigned g_wait_limit = 0;     // 0: each wait's built-in limit
+
 extern "C" void gb__count_launch(void) { g_launches++; }
 
 extern "C" int gb__set_error(int code, const char *where) {
@@ -83,11 +93,18 @@ extern "C" const char *gb_last_error_where(void) { return g_err_where; }
 extern "C" void gb_clear_error(void) {
   g_err = 0;
   g_err_where[0] = 0;
+  if (g_io) {
+    cudaStreamSynchronize(g_stream);
+    cudaMemset(g_io->status, 0, sizeof(int) * GB_STATUS_WORDS);
+  }
 }
+
+static int check_status(void);
 
 extern "C" int gb_synchronize(void) {
   cudaError_t e = cudaStreamSynchronize(g_stream);
   if (e != cudaSuccess) return gb__set_error((int) e, "cudaStreamSynchronize");
+  check_status();
   return g_err;
 }
 
@@ -135,7 +152,7 @@ extern "C" int gb_d2h(void *dst, const void *src, size_t bytes) {
   cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, g_stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(g_stream);
   if (e != cudaSuccess) return gb__set_error((int) e, "d2h");
-  return 0;
+  return check_status();
 }
 
 extern "C" int gb_d2d(void *dst, const void *src, size_t bytes) {
@@ -273,26 +290,101 @@ int gb__tmap_lines(CUtensorMap *out, const void *base, long outer, long n, long 
   return 0;
 }
 
-// Error flag of the pipelined passes (one device int, allocated once).
-static int *g_pass_err = nullptr;
-int *gb__pass_errflag(void) {
-  if (!g_pass_err) {
-    if (cudaMalloc(&g_pass_err, sizeof(int)) != cudaSuccess) {
-      gb__set_error(2, "pass error flag");
+// ------------------------------------------------------------ device status
+//
+// One small device block holds the status words of the bounded device-side
+// waits (GB_STATUS_PASS: the pipelined pass's copy wait and the plane chain's
+// dependency wait; GB_STATUS_CN: the line solver's copy wait;
+// GB_STATUS_BATCH: the batch kernel's grid barrier) next to the reduction
+// result slot, so a reduction brings its result and the status back in one
+// device-to-host copy.  Every host sync point of this layer (gb_synchronize,
+// gb_d2h, reductions) reads the status and latches a nonzero word into
+// gb_last_error() (code GB_ERR_DEVICE_WAIT), so a wait that gave up is
+// reported at the next read of any result instead of leaving wrong values
+// unnoticed.  gb_clear_error() clears the words again.
+
+static IoBlock *io_block(void) {
+  if (!g_io) {
+    if (cudaMalloc(&g_io, sizeof(IoBlock)) != cudaSuccess) {
+      cudaGetLastError();
+      g_io = nullptr;
+      gb__set_error(2, "device status block");
       return nullptr;
     }
-    cudaMemsetAsync(g_pass_err, 0, sizeof(int), g_stream);
+    if (cudaHostAlloc(&g_io_host, sizeof(IoBlock), cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      g_io_host = (IoBlock *) calloc(1, sizeof(IoBlock));
+    }
+    cudaMemsetAsync(g_io, 0, sizeof(IoBlock), g_stream);
   }
-  return g_pass_err;
+  return g_io;
 }
 
-extern "C" int gb_pass_error_flag(int reset) {
-  if (!g_pass_err) return 0;
+int *gb__status(int word) {
+  IoBlock *io = io_block();
+  return (io && word >= 0 && word < GB_STATUS_WORDS) ? &io->status[word] : nullptr;
+}
+
+void *gb__result_slot(void) {
+  IoBlock *io = io_block();
+  return io ? (void *) io->result : nullptr;
+}
+
+static int status_error(const int *st) {
+  if (!(st[GB_STATUS_PASS] | st[GB_STATUS_CN] | st[GB_STATUS_BATCH])) return 0;
+  char msg[160];
+  snprintf(msg, sizeof(msg), "a device-side wait gave up (line passes %d, CN sweeps %d, batch barrier %d)",
+           st[GB_STATUS_PASS], st[GB_STATUS_CN], st[GB_STATUS_BATCH]);
+  return gb__set_error(GB_ERR_DEVICE_WAIT, msg);
+}
+
+int gb__read_result(void *host, size_t bytes) {
+  if (!io_block()) return g_err;
+  cudaError_t e = cudaMemcpyAsync(g_io_host, g_io, sizeof(IoBlock), cudaMemcpyDeviceToHost, g_stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g_stream);
+  if (e != cudaSuccess) return gb__set_error((int) e, "result copy");
+  memcpy(host, g_io_host->result, bytes < sizeof(g_io_host->result) ? bytes : sizeof(g_io_host->result));
+  return status_error(g_io_host->status);
+}
+
+// Status words only (after the stream has drained); no-op before the block
+// exists, since nothing can have written it.
+static int check_status(void) {
+  if (!g_io) return 0;
+  cudaError_t e = cudaMemcpyAsync(g_io_host->status, g_io->status, sizeof(int) * GB_STATUS_WORDS,
+                                  cudaMemcpyDeviceToHost, g_stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g_stream);
+  if (e != cudaSuccess) return gb__set_error((int) e, "status copy");
+  return status_error(g_io_host->status);
+}
+
+static int status_word(int word, int reset) {
+  if (!g_io) return 0;
   int h = 0;
   cudaStreamSynchronize(g_stream);
-  cudaMemcpy(&h, g_pass_err, sizeof(int), cudaMemcpyDeviceToHost);
-  if (reset) cudaMemset(g_pass_err, 0, sizeof(int));
+  cudaMemcpy(&h, &g_io->status[word], sizeof(int), cudaMemcpyDeviceToHost);
+  if (reset) cudaMemset(&g_io->status[word], 0, sizeof(int));
   return h;
+}
+
+int *gb__pass_errflag(void) { return gb__status(GB_STATUS_PASS); }
+
+extern "C" int gb_pass_error_flag(int reset) { return status_word(GB_STATUS_PASS, reset); }
+int gb__status_word(int word, int reset) { return status_word(word, reset); }
+
+extern "C" unsigned gb_wait_limit(unsigned polls) {
+  const unsigned old = g_wait_limit;
+  g_wait_limit = polls;
+  return old;
+}
+unsigned gb__wait_limit(unsigned dflt) { return g_wait_limit ? g_wait_limit : dflt; }
+
+static int g_chain_lag_pct = 200;
+int gb__chain_lag_pct(void) { return g_chain_lag_pct; }
+extern "C" int gb_chain_lag(int pct) {
+  const int old = g_chain_lag_pct;
+  if (pct >= 0) g_chain_lag_pct = pct;
+  return old;
 }
 
 static int g_pipe_on = 1;

@@ -105,88 +105,3 @@ def batch2d(seed: int = 7, sizes=(64, 128, 256, 512), per_size: int = 24, step: 
         psi = np.exp(-r2 / 4.0 + 1j * (ky * y + kz * z))
         out.append(((1, n, n), psi.astype(np.complex128), v.astype(np.complex128)))
     return out
-
-
-def run_gp_steps(n: int = 256, steps: int = 3, prec: int = 0) -> float:
-    """Propagate the GP workload at n^3 for `steps` steps through the C API on
-    the current GPU and return the final norm (a small driver for profilers:
-    ``python -m libgrid_b200.workloads gp 256 3``)."""
-    import libgrid_b200 as gb
-    from libgrid_b200 import capi
-
-    api = gb.load()
-    api.lib.cuda_enable(b"\x01", 0, None)
-    shape, step, g = (n, n, n), 0.5, 0.0025
-    mass = 4.0 / GRID_AUTOAMU
-    psi0, v = gp_wells(shape, step, g, seed=2)
-    w = api.wf(*shape, step, mass, capi.WF_PERIODIC_BOUNDARY, capi.WF_2ND_ORDER_FFT, values=psi0)
-    if prec:
-        w.precision(prec)
-    vx = api.rgrid(*shape, step, values=v)
-    for _ in range(steps):
-        w.propagate_gp(vx, g, 1.0)
-    api.lib.gb_synchronize()
-    nrm = w.norm()
-    api.free(w)
-    api.free(vx)
-    return nrm
-
-
-def run_cn_steps(n: int = 192, steps: int = 3) -> float:
-    """The Crank-Nicolson GP workload at n^3 (Dirichlet walls, step 0.3,
-    g 0.001, 4 amu, dt 0.5) for `steps` steps; returns the final norm."""
-    import libgrid_b200 as gb
-    from libgrid_b200 import capi
-
-    api = gb.load()
-    api.lib.cuda_enable(b"\x01", 0, None)
-    shape, step, g = (n, n, n), 0.3, 0.001
-    psi0, v = cn_wells(shape, step, g)
-    w = api.wf(*shape, step, 4.0 / GRID_AUTOAMU, capi.WF_DIRICHLET_BOUNDARY, capi.WF_2ND_ORDER_CN, values=psi0)
-    vx = api.rgrid(*shape, step, values=v)
-    for _ in range(steps):
-        w.propagate_gp(vx, g, 0.5)
-    api.lib.gb_synchronize()
-    nrm = w.norm()
-    api.free(w)
-    api.free(vx)
-    return nrm
-
-
-def run_batch_steps(steps: int = 8, prec: int = 0) -> None:
-    """The batched 2-D workload (batch2d) for `steps` steps in one call."""
-    import libgrid_b200 as gb
-    from libgrid_b200 import capi
-
-    api = gb.load()
-    api.lib.cuda_enable(b"\x01", 0, None)
-    inst = batch2d(seed=7)
-    wfs = [api.wf(*sh, 0.2, 1.0, capi.WF_PERIODIC_BOUNDARY, capi.WF_2ND_ORDER_FFT, values=p) for sh, p, _ in inst]
-    pots = [api.cgrid(*sh, 0.2, values=v) for sh, _, v in inst]
-    if prec:
-        for w in wfs:
-            w.precision(prec)
-    b = api.batch(wfs, pots, 0.05)
-    b.propagate(steps)
-    api.lib.gb_synchronize()
-    api.free(b)
-    for o in wfs + pots:
-        api.free(o)
-
-
-if __name__ == "__main__":
-    import sys
-
-    usage = ("usage: python -m libgrid_b200.workloads gp [n] [steps] [prec: 0 FP64, 1 FP32]\n"
-             "       python -m libgrid_b200.workloads cn [n] [steps]\n"
-             "       python -m libgrid_b200.workloads batch [steps] [prec]")
-    if len(sys.argv) < 2 or sys.argv[1] not in ("gp", "cn", "batch"):
-        sys.exit(usage)
-    a = [int(x) for x in sys.argv[2:]]
-    if sys.argv[1] == "gp":
-        print("norm", run_gp_steps(*a))
-    elif sys.argv[1] == "cn":
-        print("norm", run_cn_steps(*a))
-    else:
-        run_batch_steps(*a)
-        print("ok")

@@ -6,9 +6,13 @@
 # (make.conf:45,73-97 for REAL=double, INT=long; src/Makefile:18-19,96-104 for
 # git-version.h and proto.h) without running the reference's build system.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh REFERENCE_ROOT   (or set LIBGRID_REFERENCE)
 set -eu
-REF=${1:-/root/reference}
+REF=${1:-${LIBGRID_REFERENCE:-}}
+if [ -z "$REF" ]; then
+  echo "usage: build_ref.sh REFERENCE_ROOT (or set LIBGRID_REFERENCE)" >&2
+  exit 2
+fi
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 GEN="$OUT/gen"

@@ -36,7 +36,7 @@ def main(argv=None):
     import numpy as np
 
     from libgrid_b200 import capi, workloads
-    from oracle import pyoracle
+    from oracle import pyoracle, refsteps
 
     threads = a.threads or len(os.sched_getaffinity(0))
     shape, step, g, dt = (a.size,) * 3, 0.5, 0.0025, 1.0
@@ -44,28 +44,8 @@ def main(argv=None):
     psi0, v = workloads.gp_wells(shape, step, g, seed=2)
     kind = "reference" if pyoracle.reference_available() else "port"
     if kind == "reference":
-        ref = pyoracle.reference(threads)
-        lib = ref.lib
-        w = ref.wf(*shape, step, mass, capi.WF_PERIODIC_BOUNDARY, capi.WF_2ND_ORDER_FFT, values=psi0)
-        vext = ref.rgrid(*shape, step, values=v)
-        dens = ref.rgrid(*shape, step)
-        pot = ref.cgrid(*shape, step)
-        vc = ref.cgrid(*shape, step)
-        lib.grid_real_to_complex_re(vc.ptr, vext.ptr)
-        half = capi.Complex.of(0.5 * dt)
-
-        def one_step():
-            lib.cgrid_fft(w.s.grid)
-            lib.grid_wf_propagate_kinetic_fft(w.ptr, half)
-            lib.cgrid_inverse_fft_norm(w.s.grid)
-            lib.grid_wf_density(w.ptr, dens.ptr)
-            lib.grid_real_to_complex_re(pot.ptr, dens.ptr)
-            lib.cgrid_multiply(pot.ptr, capi.Complex.of(g))
-            lib.cgrid_sum(pot.ptr, pot.ptr, vc.ptr)
-            lib.grid_wf_propagate_potential(w.ptr, capi.Complex.of(dt), pot.ptr, 0.0)
-            lib.cgrid_fft(w.s.grid)
-            lib.grid_wf_propagate_kinetic_fft(w.ptr, half)
-            lib.cgrid_inverse_fft_norm(w.s.grid)
+        stepper = refsteps.GPStepper(pyoracle.reference(threads), psi0, v, step, mass, g, dt)
+        one_step = stepper.step_once
 
     else:
         os.environ.setdefault("OMP_NUM_THREADS", str(threads))

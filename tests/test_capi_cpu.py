@@ -120,3 +120,55 @@ def test_analyze_method_default_is_finite_difference(b200):
     g = b200.cgrid(2, 2, 2, 1.0)
     assert m.value in (b"\x00", b"\x01")
     b200.free(g)
+
+
+def _reference_src():
+    root = os.environ.get("LIBGRID_REFERENCE") or os.path.join(os.path.dirname(ROOT), "reference")
+    return os.path.join(root, "src")
+
+
+STRUCT_FIELDS = {
+    "cgrid": ["value", "id", "grid_len", "nx", "ny", "nz", "step", "x0", "y0", "z0", "kx0", "ky0", "kz0", "omega",
+              "value_outside", "outside_params_ptr", "default_outside_params", "plan", "iplan", "cufft_handle",
+              "host_lock", "fft_norm", "fft_norm2", "flag"],
+    "rgrid": ["value", "id", "grid_len", "nx", "ny", "nz", "nz2", "step", "x0", "y0", "z0", "kx0", "ky0", "kz0",
+              "value_outside", "outside_params_ptr", "default_outside_params", "plan", "iplan", "cufft_handle_r2c",
+              "cufft_handle_c2r", "host_lock", "fft_norm", "fft_norm2", "flag"],
+    "wf": ["grid", "mass", "norm", "cfft_width", "boundary", "propagator", "cworkspace", "cworkspace2", "cworkspace3",
+           "ts_func", "lx", "hx", "ly", "hy", "lz", "hz", "kmax"],
+}
+
+
+def _layout(tmp_path, name, prelude):
+    lines = []
+    for st, fields in STRUCT_FIELDS.items():
+        lines.append('printf("%s sizeof %%zu\\n", sizeof(%s));' % (st, st))
+        for f in fields:
+            lines.append('printf("%s.%s %%zu %%zu\\n", offsetof(%s, %s), sizeof(((%s *) 0)->%s));' % (st, f, st, f, st, f))
+    prog = tmp_path / (name + ".c")
+    prog.write_text(prelude + "\n#include <stddef.h>\n#include <stdio.h>\nint main(void){\n" + "\n".join(lines) +
+                    "\nreturn 0;}\n")
+    exe = tmp_path / name
+    subprocess.run(["gcc", "-std=gnu99", "-I" + INCLUDE, str(prog), "-o", str(exe)], check=True)
+    return subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines()
+
+
+def test_struct_layout_matches_reference_structs_h(tmp_path):
+    """Every field offset and size of cgrid, rgrid and wf in include/grid.h
+    equals the reference's src/structs.h compiled as the reference's CUDA,
+    double-precision build sees it (USE_CUDA, DOUBLE_PREC, REAL double, INT
+    long, fftw_plan a pointer, cufftHandle an int), so existing callers
+    recompile unchanged."""
+    src = _reference_src()
+    if not os.path.exists(os.path.join(src, "structs.h")):
+        pytest.skip("reference sources not present (set LIBGRID_REFERENCE)")
+    ref_prelude = (
+        "#include <complex.h>\n#include <sys/time.h>\n#include <time.h>\n"
+        "#define REAL double\n#define INT long\n#define DOUBLE_PREC\n#define USE_CUDA\n"
+        "typedef struct fftw_plan_s *fftw_plan;\ntypedef int cufftHandle;\n"
+        '#include "%s"\n' % os.path.join(src, "structs.h")
+    )
+    ours = _layout(tmp_path, "ours", '#include "grid.h"')
+    theirs = _layout(tmp_path, "theirs", ref_prelude)
+    assert ours == theirs
+    assert len(ours) == 3 + sum(len(f) for f in STRUCT_FIELDS.values())

@@ -4,9 +4,13 @@ It is meant for callers that cannot let a library allocate on the device: an
 application that hands out every byte of device memory from its own pool or
 budget, or a latency-critical loop where a cudaMalloc, or the device-wide
 synchronisation of cudaFree, is not acceptable.  It must compute the same
-sums as gb_reduce.  This test calls both through the C ABI on the same device
-data, two calls in a row, with the relative tolerance the other reduction
-tests use, and checks that oversized grids are refused before any launch.
+sums as gb_reduce up to rounding (it adds the terms in a different order, so
+the two agree to about 1e-12 relative, not bit for bit; each is deterministic
+from call to call).  This test calls both through the C ABI on the same
+device data, two calls in a row, for every reduction op and for mixed-
+precision operands, with the relative tolerance the other reduction tests
+use, and checks that oversized grids and unknown ops are refused before any
+launch.
 """
 import ctypes as C
 
@@ -17,7 +21,7 @@ from libgrid_b200 import capi
 
 pytestmark = pytest.mark.gpu
 
-RED_SUM, RED_NORM2, RED_CONJ_PRODUCT, RED_EXPECT_REAL, RED_KSQ_NORM2 = 1, 2, 3, 5, 7
+RED_SUM, RED_NORM2, RED_CONJ_PRODUCT, RED_EXPECT_COMPLEX, RED_EXPECT_REAL, RED_REAL_SUM, RED_KSQ_NORM2 = 1, 2, 3, 4, 5, 6, 7
 TOL = 1e-12
 
 
@@ -68,16 +72,24 @@ def test_noalloc_matches_gb_reduce(b200):
     r = np.zeros((nx, ny, nz2))
     r[:, :, :nz] = rng.standard_normal((nx, ny, nz))
     a32 = a.astype(np.complex64)
-    da, db, dr, da32 = (_to_device(lib, x) for x in (a, b, r, a32))
+    b32 = b.astype(np.complex64)
+    r32 = r.astype(np.float32)
+    da, db, dr, da32, db32, dr32 = (_to_device(lib, x) for x in (a, b, r, a32, b32, r32))
     g64 = Geom(nx, ny, nz, 0.3, capi.GRID_PREC_FP64)
     g32 = Geom(nx, ny, nz, 0.3, capi.GRID_PREC_FP32)
     cases = [
         (RED_SUM, da, None, g64, nz, 0, 0),
         (RED_NORM2, da, None, g64, nz, 0, 0),
         (RED_CONJ_PRODUCT, da, db, g64, nz, nz, 0),
+        (RED_EXPECT_COMPLEX, da, db, g64, nz, nz, 0),
         (RED_EXPECT_REAL, da, dr, g64, nz, nz2, 0),
+        (RED_REAL_SUM, dr, None, g64, nz2, 0, 0),
         (RED_KSQ_NORM2, da, None, g64, nz, 0, 0),
         (RED_NORM2, da32, None, g32, nz, 0, 0),
+        # mixed precision: FP64 a with an FP32 second operand, and the reverse
+        (RED_CONJ_PRODUCT, da, db32, g64, nz, nz, capi.GRID_PREC_FP32),
+        (RED_EXPECT_REAL, da, dr32, g64, nz, nz2, capi.GRID_PREC_FP32),
+        (RED_EXPECT_COMPLEX, da32, db, g32, nz, nz, capi.GRID_PREC_FP64),
     ]
     try:
         for op, x, y, geom, arow, brow, bprec in cases:
@@ -89,7 +101,7 @@ def test_noalloc_matches_gb_reduce(b200):
         n2 = _call(lib.gb_reduce_noalloc, RED_NORM2, da, None, g64, nz, 0, 0).real
         assert abs(n2 - np.sum(np.abs(a) ** 2)) <= TOL * n2
     finally:
-        for p in (da, db, dr, da32):
+        for p in (da, db, dr, da32, db32, dr32):
             lib.gb_device_free(p)
 
 
@@ -104,3 +116,16 @@ def test_noalloc_rejects_grids_above_its_limit(b200):
     assert lib.gb_last_error() != 0
     lib.gb_clear_error()
     assert lib.gb_last_error() == 0
+
+
+def test_noalloc_rejects_unknown_op(b200):
+    lib = b200.lib
+    _bind(lib)
+    lib.cuda_enable(b"\x01", 0, None)
+    out = (C.c_double * 2)()
+    g = Geom(8, 8, 8, 0.5, capi.GRID_PREC_FP64)
+    for fn in (lib.gb_reduce_noalloc, lib.gb_reduce):
+        for op in (0, 8, -1):
+            assert fn(op, None, None, C.byref(g), 8, 0, 0, out) != 0
+            assert lib.gb_last_error() != 0
+            lib.gb_clear_error()
