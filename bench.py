@@ -30,6 +30,8 @@ split-operator step of that wavefunction.
             complex potentials, FP64 and FP32): steps/s of all instances in
             one persistent launch per call (grid_wf_batch_propagate) against
             the same instances stepped one at a time (grid_wf_propagate)
+  cn192     the Crank-Nicolson workload (192^3 GP, Dirichlet walls): steps/s,
+            per-sweep times and the step against its 112 B/pt roofline
   warm_start imaginary-time steps and seconds to |dE| < 1e-8 Ha on held-out
             32^3 GP potentials from the learned U-Net guess against a
             Gaussian guess (libgrid_b200.warmstart, child process, N = 1)
@@ -363,6 +365,56 @@ def oracle_agreement(api, lib, make, g):
     return out
 
 
+def run_cn192(api, lib, steps, world, peak):
+    """The Crank-Nicolson workload: 192^3 Gross-Pitaevskii, Dirichlet walls,
+    step 0.3 bohr, 4 amu, g 0.001, dt 0.5 au (grid_wf_propagate_gp on a
+    WF_2ND_ORDER_CN wave function).  Steps/s with CUDA events on the library
+    stream, the time of each line sweep, and the step against its 112 B/pt
+    roofline (x sweep psi in/out + real V_ext for the first V/2, y sweep
+    psi in/out, z sweep psi in/out + V_ext for the second V/2)."""
+    import ctypes as C
+
+    from libgrid_b200 import capi, workloads
+
+    n, step, g, dt = 192, 0.3, 0.001, 0.5
+    psi0, v = workloads.cn_wells((n, n, n), step, g, seed=3)
+    w = api.wf(n, n, n, step, 4.0 / capi.GRID_AUTOAMU, capi.WF_DIRICHLET_BOUNDARY, capi.WF_2ND_ORDER_CN, values=psi0)
+    vx = api.rgrid(n, n, n, step, values=v)
+    for _ in range(5):
+        w.propagate_gp(vx, g, dt)
+    lib.gb_synchronize()
+    barrier(world)
+    lib.gb_pass_timing(1)
+    lib.gb_event_record(10)
+    for _ in range(steps):
+        w.propagate_gp(vx, g, dt)
+    lib.gb_event_record(11)
+    lib.gb_synchronize()
+    ms = allmax(world, lib.gb_event_elapsed_ms(10, 11))
+    kms = (C.c_double * NUM_KINDS)()
+    kcnt = (C.c_long * NUM_KINDS)()
+    lib.gb_pass_timing_report(kms, kcnt, NUM_KINDS)
+    lib.gb_pass_timing(0)
+    api.free(w)
+    api.free(vx)
+    N = n**3
+    step_ms = ms / steps
+    gbs = 112 * N / (step_ms * 1e-3) / 1e9
+    sweeps = {KIND_NAMES[k]: {"ms_mean": kms[k] / kcnt[k], "launches": kcnt[k]} for k in (15, 16, 17) if kcnt[k]}
+    return {
+        "value": world * steps / (ms * 1e-3),
+        "unit": "steps/s",
+        "steps": steps,
+        "ms_per_step": step_ms,
+        "grid": [n, n, n],
+        "bytes_per_point": 112,
+        "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak},
+        "sweeps": sweeps,
+        "note": "2nd-order Crank-Nicolson GP step, V/2 fused into the x and z line sweeps; warp-cooperative "
+        "line solver",
+    }
+
+
 def run_b200(args, world, rank, local):
     import libgrid_b200 as gb
     from libgrid_b200 import capi, workloads
@@ -486,6 +538,9 @@ def run_b200(args, world, rank, local):
     # ------------------- agreement with the reference's FP64 trajectory
     agreement = oracle_agreement(api, lib, make, g) if (rank == 0 and n == 256 and not args.no_oracle) else None
 
+    # ------------------------------------- Crank-Nicolson 192^3 (Dirichlet)
+    cn = None if args.no_cn else run_cn192(api, lib, args.cn_steps, world, hbm_peak()[0])
+
     # ---------------------------------- batched uneven 2-D (one launch/call)
     batch = {}
     if not args.no_batch:
@@ -571,6 +626,7 @@ def run_b200(args, world, rank, local):
             "reported separately",
         },
         "batch2d": batch or None,
+        "cn192": cn,
         "e2e": {
             "value": world * args.steps / e2e_s,
             "unit": "steps/s",
@@ -639,6 +695,8 @@ def main(argv=None):
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-warm-start", action="store_true")
     ap.add_argument("--no-oracle", action="store_true")
+    ap.add_argument("--no-cn", action="store_true")
+    ap.add_argument("--cn-steps", type=int, default=100)
     ap.add_argument("--batch-steps", type=int, default=200)
     args = ap.parse_args(argv)
     world, rank, local = dist_setup()

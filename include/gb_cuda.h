@@ -231,6 +231,22 @@ int gb_complex_real_part(void *r, const void *c, const gb_geom *g, long rrow);
 
 /* Absorbing-boundary blend dst = (1 - a) wr + a wi (src/grid_wf-cuda2.cu:165-176). */
 int gb_wf_merge(void *dst, const void *wr, const void *wi, const gb_geom *g, long lx, long hx, long ly, long hy, long lz, long hz);
+/* k-space convolution product c = (-1)^(i+j+k) a b over nx x ny x nzc
+ * complex entries (src/cgrid.c:1912-1944 with nzc = nz; src/rgrid.c:1848-1878
+ * on the half spectrum, nzc = nz2 / 2); prec of all three arrays. */
+int gb_fft_convolute(void *c, const void *a, const void *b, long nx, long ny, long nzc, int prec);
+/* Geometry of a grid for gb_interpolate: extents, elements per (i, j) row,
+ * step and real-space origin. */
+typedef struct {
+  long nx, ny, nz, row;
+  double step, x0, y0, z0;
+} gb_grid_frame;
+/* dst(i, j, k) = trilinear interpolation of src at dst's point (i, j, k)
+ * (src/cgrid.c:2067-2151, src/rgrid.c:2208-2300), corners outside src
+ * taken by the boundary rule bc (GB_BC_*; Dirichlet value out_re + i out_im).
+ * FP64 complex (is_real = 0) or FP64 padded real grids. */
+int gb_interpolate(void *dst, const gb_grid_frame *d, const void *src, const gb_grid_frame *s, int bc, double out_re,
+                   double out_im, int is_real);
 
 /* ---------------------------------------------------------- reductions */
 /* Deterministic FP64 reductions over the (nx, ny, nz) grid; out[0..1] gets
@@ -299,6 +315,13 @@ typedef struct {
   long lx, hx, ly, hy, lz, hz;
 } gb_cn_params;
 int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, const gb_potential *pre, const gb_potential *post);
+/* Line solver of the Crank-Nicolson fast path (no rotation, no absorbing
+ * region, lines of up to 256 points): 1 (the default) the warp-cooperative
+ * solver (one warp per line, segment carries by a warp-shuffle scan), 0 the
+ * segment-per-warp solver; -1 only queries.  Returns the previous setting.
+ * Both solve the reference's systems; they differ only in rounding.  (No
+ * reference counterpart.) */
+int gb_cn_warp_solver(int on);
 
 /* --------------------------------------------------------------- noise */
 /* Seeded noise added to a device grid (the reference's src/rand.c API and

@@ -190,8 +190,14 @@ void cgrid_random_uniform(cgrid *grid, REAL complex scale);
 void cgrid_random_uniform_sp(cgrid *grid, REAL scale);
 void cgrid_random_normal(cgrid *grid, REAL complex scale);
 void cgrid_random_normal_sp(cgrid *grid, REAL scale);
+/* src/cgrid.c:360 */
 void cgrid_write(cgrid *grid, FILE *out);
+/* src/cgrid.c:383 -- a file of another size is interpolated (cgrid_extrapolate) */
 cgrid *cgrid_read(cgrid *grid, FILE *in);
+/* src/cgrid.c:2126 -- trilinear interpolation of src at dest's points, on the GPU */
+void cgrid_extrapolate(cgrid *dest, cgrid *src);
+/* src/cgrid.c:1912 -- k-space convolution product (-1)^(i+j+k) a b */
+void cgrid_fft_convolute(cgrid *gridc, cgrid *grida, cgrid *gridb);
 /* src/cgrid.c:615 */
 void cgrid_copy(cgrid *dst, cgrid *src);
 /* src/cgrid.c:711,725 */
@@ -269,6 +275,8 @@ void rgrid_fft(rgrid *grid);
 void rgrid_inverse_fft(rgrid *grid);
 void rgrid_scaled_inverse_fft(rgrid *grid, REAL c);
 void rgrid_inverse_fft_norm(rgrid *grid);
+/* src/rgrid.c:1824 */
+void rgrid_inverse_fft_norm2(rgrid *grid);
 /* src/rgrid.c:2020,2064 */
 REAL rgrid_value_at_index(rgrid *grid, INT i, INT j, INT k);
 void rgrid_value_to_index(rgrid *grid, INT i, INT j, INT k, REAL value);
@@ -278,6 +286,13 @@ REAL rgrid_value_outside_neumann(rgrid *grid, INT i, INT j, INT k);
 REAL rgrid_value_outside_periodic(rgrid *grid, INT i, INT j, INT k);
 /* src/rgrid_diff.c:309 */
 void rgrid_fd_laplace(rgrid *grid, rgrid *laplace);
+/* src/rgrid.c:339,360 -- binary grid I/O; rgrid_read interpolates other sizes */
+void rgrid_write(rgrid *grid, FILE *out);
+rgrid *rgrid_read(rgrid *grid, FILE *in);
+/* src/rgrid.c:2267 -- trilinear interpolation of src at dest's points, on the GPU */
+void rgrid_extrapolate(rgrid *dest, rgrid *src);
+/* src/rgrid.c:1848 -- k-space convolution product on the half spectrum */
+void rgrid_fft_convolute(rgrid *gridc, rgrid *grida, rgrid *gridb);
 
 /* ---------------------------------------------------------------- ngrid */
 /* src/ngrid.c:53,186,254,355 */

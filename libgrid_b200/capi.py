@@ -158,6 +158,7 @@ def bind(lib: C.CDLL, cuda_layout: bool, extensions: bool):
     f("cgrid_fft", None, PC)
     f("cgrid_inverse_fft", None, PC)
     f("cgrid_inverse_fft_norm", None, PC)
+    f("cgrid_inverse_fft_norm2", None, PC)
     f("cgrid_multiply", None, PC, Cx)
     f("cgrid_sum", None, PC, PC, PC)
     f("cgrid_difference", None, PC, PC, PC)
@@ -183,12 +184,26 @@ def bind(lib: C.CDLL, cuda_layout: bool, extensions: bool):
     f("cgrid_fft_gradient_y", None, PC, PC)
     f("cgrid_fft_gradient_z", None, PC, PC)
     f("cgrid_fft_laplace_expectation_value", D, PC)
+    f("cgrid_add", None, PC, Cx)
+    f("cgrid_fft_convolute", None, PC, PC, PC)
+    f("cgrid_extrapolate", None, PC, PC)
+    f("cgrid_write", None, PC, V)
+    f("cgrid_read", PC, PC, V)
     f("rgrid_alloc", PR, L, L, L, D, V, V, C.c_char_p)
     f("rgrid_free", None, PR)
     f("rgrid_fd_laplace", None, PR, PR)
     f("rgrid_fft", None, PR)
     f("rgrid_inverse_fft_norm", None, PR)
+    f("rgrid_inverse_fft", None, PR)
+    f("rgrid_inverse_fft_norm2", None, PR)
     f("rgrid_integral", D, PR)
+    f("rgrid_sum", None, PR, PR, PR)
+    f("rgrid_product", None, PR, PR, PR)
+    f("rgrid_multiply", None, PR, D)
+    f("rgrid_fft_convolute", None, PR, PR, PR)
+    f("rgrid_extrapolate", None, PR, PR)
+    f("rgrid_write", None, PR, V)
+    f("rgrid_read", PR, PR, V)
     f("grid_real_to_complex_re", None, PC, PR)
     f("grid_product_norm", None, PR, PR, PC)
     f("grid_product_complex_with_real", None, PC, PR)
@@ -237,6 +252,7 @@ def bind(lib: C.CDLL, cuda_layout: bool, extensions: bool):
         f("gb_last_error_where", C.c_char_p)
         f("gb_wait_limit", C.c_uint, C.c_uint)
         f("gb_chain_lag", C.c_int, C.c_int)
+        f("gb_cn_warp_solver", C.c_int, C.c_int)
         f("gb_pass_error_flag", C.c_int, C.c_int)
         f("gb_cn_error_flag", C.c_int)
         f("gb_batch_error_flag", C.c_int, V, C.c_int)

@@ -344,6 +344,270 @@ template <bool CONTIG> __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast
   bulk_wait_all();
 }
 
+// ---------------------------------------------------------------------------
+// Warp-cooperative fast path for lines of up to 32 * kLaneSegMax points.
+//
+// One warp solves one line.  Lane s owns the contiguous segment
+// [s S, s S + S) of the line, S = ceil(n / 32) <= kLaneSegMax, held in
+// registers.  Each lane runs the two Thomas recurrences of its segment from a
+// zero carry (forward v_i = b_i - m_i v_{i-1}, backward
+// x_i = rb_i v_i + q_i x_{i+1}); the true carries are then the prefix sums of
+// the affine segment maps carry_out = u_end + A_s carry_in (backward:
+// y_start + B_s carry_in), which a warp-shuffle scan (recursive doubling,
+// 5 levels) resolves.  The matrix is the same for every line, so the
+// segment responses A_s = prod(-m) and B_s = prod(q) and their window
+// products for each scan level are host-precomputed tables, and the scan
+// costs one complex multiply-add per level.  The fix-ups add carry x
+// homogeneous response (tables H, G) to every element.  No CTA barrier sits
+// inside the solve.
+//
+// CTAs are persistent and double-buffered: while the warps solve the lines
+// of one tile (W lines, one per warp), warp 0 has the bulk copies of the
+// next tile in flight.  Tiles: W consecutive lines (contiguous axis, rows
+// padded to an odd length) or W adjacent columns x n rows (strided axes, row
+// pitch W + 1), so the lanes' segment accesses hit at most two-way bank
+// conflicts.
+constexpr int kLaneSegMax = 8;
+constexpr int kCnWarpLines = 8;  // lines per tile = warps per CTA
+constexpr int kCnWarpThreads = 32 * kCnWarpLines;
+
+__host__ __device__ inline long warp_pitch(bool contig, long n) { return contig ? contig_row(n) : kCnWarpLines + 1; }
+
+// Offsets of the scan tables behind the six per-element tables.
+__host__ __device__ inline long warp_scan_off(long n) { return 6 * n; }
+
+__device__ __forceinline__ double2 shfl_idx2(double2 v, int src) {
+  return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
+}
+__device__ __forceinline__ double2 shfl_up2(double2 v, int d) {
+  return make_double2(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d));
+}
+__device__ __forceinline__ double2 shfl_down2(double2 v, int d) {
+  return make_double2(__shfl_down_sync(0xffffffffu, v.x, d), __shfl_down_sync(0xffffffffu, v.y, d));
+}
+
+// Solve line l of the tile in place (the whole warp).
+template <bool CONTIG>
+__device__ __forceinline__ void cn_warp_line(double2 *sm, long pitch, int l, const CnAxis &a, int lane) {
+  const long n = a.n;
+  const int S = (int) ((n + 31) >> 5);
+  const int bc = a.boundary;
+  const double2 zero = make_double2(0.0, 0.0);
+  const double2 *tm = a.tab, *trb = a.tab + n, *tz = a.tab + 2 * n, *tH = a.tab + 3 * n, *tQ = a.tab + 4 * n,
+                *tG = a.tab + 5 * n;
+  const double2 *wf = a.tab + warp_scan_off(n), *wb = wf + 5 * 32;
+  auto at = [&](long i) -> double2 & { return CONTIG ? sm[(long) l * pitch + i] : sm[i * pitch + l]; };
+  const long a0 = (long) lane * S;
+  const int cnt = (int) (a0 >= n ? 0 : (n - a0 < S ? n - a0 : S));
+  double2 p[kLaneSegMax];
+#pragma unroll
+  for (int j = 0; j < kLaneSegMax; j++) p[j] = (j < cnt) ? at(a0 + j) : zero;
+  // the line's first and last elements and the segment neighbours, read
+  // before any lane writes (selecting them from the register arrays by a
+  // runtime index would move the arrays to local memory)
+  const double2 pfirst = at(0), plast = at(n - 1);
+  const double2 p_before = (a0 > 0 && a0 <= n) ? at(a0 - 1) : zero;
+  const double2 p_after = (a0 + cnt < n) ? at(a0 + cnt) : zero;
+  __syncwarp();
+
+  // right-hand side and forward particular recurrence (zero carry-in)
+  double2 u = zero, pm = p_before;
+#pragma unroll
+  for (int j = 0; j < kLaneSegMax; j++) {
+    if (j < cnt) {
+      const long i = a0 + j;
+      const double2 p0 = p[j];
+      const double2 pp = (j + 1 < cnt) ? p[j + 1] : p_after;
+      const double2 b = cn_rhs(i, n, bc, a.cp, a.c2, zero, pm, p0, pp, pfirst, plast);
+      u = (j == 0) ? b : cs(b, cm(__ldg(tm + i), u));
+      pm = p0;
+      p[j] = u;
+    }
+  }
+  // forward carries: inclusive scan of carry_out = u_end + A_s carry_in
+  double2 x = (cnt > 0) ? u : zero;
+#pragma unroll
+  for (int d = 0; d < 5; d++) {
+    const double2 y = shfl_up2(x, 1 << d);
+    if (lane >= (1 << d)) x = ca(x, cm(__ldg(wf + d * 32 + lane), y));
+  }
+  double2 vin = shfl_up2(x, 1);
+  if (lane == 0) vin = zero;
+  // forward fix-up fused with the backward particular recurrence
+  double2 yv = zero, ystart = zero;
+#pragma unroll
+  for (int j = kLaneSegMax - 1; j >= 0; j--) {
+    if (j < cnt) {
+      const long i = a0 + j;
+      const double2 v = ca(p[j], cm(__ldg(tH + i), vin));
+      yv = (j == cnt - 1) ? cm(__ldg(trb + i), v) : ca(cm(__ldg(trb + i), v), cm(__ldg(tQ + i), yv));
+      p[j] = yv;
+      ystart = yv;
+    }
+  }
+  // backward carries: suffix scan of carry_out = y_start + B_s carry_in
+  x = ystart;
+#pragma unroll
+  for (int d = 0; d < 5; d++) {
+    const double2 y = shfl_down2(x, 1 << d);
+    if (lane + (1 << d) < 32) x = ca(x, cm(__ldg(wb + d * 32 + lane), y));
+  }
+  double2 xin = shfl_down2(x, 1);
+  if (lane == 31) xin = zero;
+#pragma unroll
+  for (int j = 0; j < kLaneSegMax; j++)
+    if (j < cnt) {
+      p[j] = ca(p[j], cm(__ldg(tG + a0 + j), xin));
+      at(a0 + j) = p[j];
+    }
+  if (bc == 3) {
+    // Sherman-Morrison: fact = (x_0 + beta x_{n-1} / gamma) / den, with
+    // x_0 and x_{n-1} read back from the line
+    __syncwarp();
+    const double2 x0 = at(0), xl = at(n - 1);
+    const double2 fact = cm(ca(x0, cm(a.beta, cm(xl, a.gamma))), a.den);  // gamma, den hold reciprocals
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < kLaneSegMax; j++)
+      if (j < cnt) at(a0 + j) = cs(p[j], cm(fact, __ldg(tz + a0 + j)));
+  }
+}
+
+// Potential half-step on every element of a tile (all threads).
+template <bool CONTIG>
+__device__ __forceinline__ void cn_tile_pot(double2 *sm, long pitch, int nl, long line0, long o, long col0,
+                                            const CnAxis &a, const gb_potential &pt) {
+  const long n = a.n;
+  for (long e = threadIdx.x; e < (long) nl * n; e += blockDim.x) {
+    long l, i;
+    if constexpr (CONTIG) {
+      l = e / n;
+      i = e - l * n;
+    } else {
+      i = e / nl;
+      l = e - i * nl;
+    }
+    long ix, iy, iz;
+    cn_decode(a, CONTIG ? line0 + l : o, i, col0 + l, ix, iy, iz);
+    double2 &r = CONTIG ? sm[l * pitch + i] : sm[i * pitch + l];
+    r = cn_pot(r, ix, iy, iz, a, pt);
+  }
+}
+
+struct CnTile {
+  long line0, o, col0;
+  int nl;
+};
+
+template <bool CONTIG> __device__ __forceinline__ CnTile cn_tile_of(const CnAxis &a, long t, long tpo) {
+  CnTile c;
+  if constexpr (CONTIG) {
+    c.line0 = t * kCnWarpLines;
+    const long rem = a.outer - c.line0;
+    c.nl = (int) (rem < kCnWarpLines ? rem : kCnWarpLines);
+    c.o = c.col0 = 0;
+  } else {
+    c.o = t / tpo;
+    c.col0 = (t - c.o * tpo) * kCnWarpLines;
+    const long rem = a.inner - c.col0;
+    c.nl = (int) (rem < kCnWarpLines ? rem : kCnWarpLines);
+    c.line0 = 0;
+  }
+  return c;
+}
+
+// Bulk copies of one tile between global memory and a shared buffer, issued
+// by the 32 lanes of warp 0 (load: completion on bar).
+template <bool CONTIG, bool LOAD>
+__device__ __forceinline__ void cn_tile_copy(double2 *psi, double2 *buf, long pitch, const CnTile &c, const CnAxis &a,
+                                             uint64_t *bar, int lane) {
+  const long n = a.n;
+  if constexpr (CONTIG) {
+    for (int l = lane; l < c.nl; l += 32) {
+      double2 *g = psi + (c.line0 + l) * n;
+      if (LOAD) bulk_g2s(buf + l * pitch, g, (unsigned) (n * 16), bar);
+      else bulk_s2g(g, buf + l * pitch, (unsigned) (n * 16));
+    }
+  } else {
+    for (long i = lane; i < n; i += 32) {
+      double2 *g = psi + (c.o * n + i) * a.inner + c.col0;
+      if (LOAD) bulk_g2s(buf + i * pitch, g, (unsigned) (c.nl * 16), bar);
+      else bulk_s2g(g, buf + i * pitch, (unsigned) (c.nl * 16));
+    }
+  }
+}
+
+template <bool CONTIG>
+__global__ void __launch_bounds__(kCnWarpThreads, 2) k_cn_warp(double2 *__restrict__ psi, CnAxis a, long ntiles, long tpo) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ __align__(8) uint64_t bars[2];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const long n = a.n;
+  const long pitch = warp_pitch(CONTIG, n);
+  const long bufsz = CONTIG ? (long) kCnWarpLines * pitch : n * pitch;
+  double2 *const buf0 = (double2 *) smraw;
+  auto buf = [&](int b) { return buf0 + (b ? bufsz : 0); };
+  if (tid == 0) {
+    mbar_init(&bars[0], 1);
+    mbar_init(&bars[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  long t = blockIdx.x;
+  if (t >= ntiles) return;
+  if (warp == 0) {
+    const CnTile c0 = cn_tile_of<CONTIG>(a, t, tpo);
+    if (lane == 0) mbar_arrive_expect_tx(&bars[0], (unsigned) (c0.nl * n * 16));
+    __syncwarp();
+    cn_tile_copy<CONTIG, true>(psi, buf(0), pitch, c0, a, &bars[0], lane);
+  }
+  const bool pre = (a.pre.kind != GB_POT_NONE || a.pre.g != 0.0);
+  const bool post = (a.post.kind != GB_POT_NONE || a.post.g != 0.0);
+  for (unsigned it = 0; t < ntiles; t += gridDim.x, it++) {
+    const int b = it & 1;
+    const long next = t + gridDim.x;
+    if (warp == 0 && next < ntiles) {
+      // the other buffer's stores (previous tile) must have read it first
+      bulk_wait_read_all();
+      __syncwarp();
+      const CnTile cn = cn_tile_of<CONTIG>(a, next, tpo);
+      if (lane == 0) mbar_arrive_expect_tx(&bars[b ^ 1], (unsigned) (cn.nl * n * 16));
+      __syncwarp();
+      cn_tile_copy<CONTIG, true>(psi, buf(b ^ 1), pitch, cn, a, &bars[b ^ 1], lane);
+    }
+    const bool ok = mbar_wait_bounded(&bars[b], (it >> 1) & 1u);
+    if (__syncthreads_or(!ok)) {
+      // a copy never completed: record it, let the copies in flight land
+      // (bounded), drain the stores and leave
+      if (tid == 0) {
+        atomicExch(a.err, 1);
+        mbar_wait_bounded(&bars[b], (it >> 1) & 1u);
+        if (next < ntiles) mbar_wait_bounded(&bars[b ^ 1], ((it + 1) >> 1) & 1u);
+      }
+      if (warp == 0) bulk_wait_all();
+      return;
+    }
+    const CnTile c = cn_tile_of<CONTIG>(a, t, tpo);
+    double2 *sm = buf(b);
+    if (pre) {
+      cn_tile_pot<CONTIG>(sm, pitch, c.nl, c.line0, c.o, c.col0, a, a.pre);
+      __syncthreads();
+    }
+    if (warp < c.nl) cn_warp_line<CONTIG>(sm, pitch, warp, a, lane);
+    if (post) {
+      __syncthreads();
+      cn_tile_pot<CONTIG>(sm, pitch, c.nl, c.line0, c.o, c.col0, a, a.post);
+    }
+    fence_proxy_async_smem();
+    __syncthreads();
+    if (warp == 0) {
+      cn_tile_copy<CONTIG, false>(psi, sm, pitch, c, a, nullptr, lane);
+      bulk_commit();
+    }
+  }
+  if (warp == 0) bulk_wait_all();
+}
+
 // General path: one thread per line, element (line, i) of a workspace array
 // at [i * nlines + line].  Handles rotation (c3) and absorbing boundaries.
 __global__ void k_cn_general(double2 *__restrict__ psi, CnAxis a) {
@@ -464,12 +728,18 @@ __global__ void k_cn_general(double2 *__restrict__ psi, CnAxis a) {
 // segment responses H (forward) and G (backward) with Q_i = -c_i / b'_i,
 // plus the periodic scalars.
 struct FastTables {
-  std::vector<double2> tab;  // 6 n: m, rb, z, H, Q, G
+  std::vector<double2> tab;  // 6 n: m, rb, z, H, Q, G; then (32 segments) the scan tables
   double2 beta, inv_gamma, inv_den;
 };
 
-static void build_fast_tables(long n, int bc, cd cp, cd c2, FastTables &t) {
-  t.tab.assign(6 * n, make_double2(0.0, 0.0));
+// nseg segments per line: kSeg for the segment-per-warp kernel, 32 for the
+// warp-cooperative one, whose scan tables follow the six per-element tables:
+// wf[d][s] = prod_{r = s - 2^d + 1 .. s} A_r with A_r = H at the end of
+// segment r, and wb[d][s] = prod_{r = s .. s + 2^d - 1} B_r with B_r = G at
+// the start of segment r (1 for empty segments).
+static void build_fast_tables(long n, int bc, cd cp, cd c2, int nseg, FastTables &t) {
+  const long ntab = 6 * n + (nseg == 32 ? 2 * 5 * 32 : 0);
+  t.tab.assign(ntab, make_double2(0.0, 0.0));
   const cd d = cp - 2.0;
   std::vector<cd> bmod(n, d), m(n, 0.0), rb(n), q(n), H(n), G(n);
   cd alpha = 1.0 + c2, beta = 1.0 - c2, gamma = -d;
@@ -496,11 +766,28 @@ static void build_fast_tables(long n, int bc, cd cp, cd c2, FastTables &t) {
     const cd ci = (i == 0 && bc != 3) ? cd(2.0) : 1.0 + c2;
     q[i] = -rb[i] * ci;
   }
-  const long S = (n + kSeg - 1) / kSeg;
-  for (long s = 0; s < kSeg; s++) {
+  const long S = (n + nseg - 1) / nseg;
+  std::vector<cd> A(nseg, 1.0), B(nseg, 1.0);
+  for (long s = 0; s < nseg; s++) {
     const long as = s * S, es = (as + S < n) ? as + S : n;
     for (long i = as; i < es; i++) H[i] = (i == as) ? -m[i] : H[i - 1] * (-m[i]);
     for (long i = es - 1; i >= as; i--) G[i] = (i == es - 1) ? q[i] : q[i] * G[i + 1];
+    if (as < es) {
+      A[s] = H[es - 1];
+      B[s] = G[as];
+    }
+  }
+  if (nseg == 32) {
+    for (int d = 0; d < 5; d++) {
+      const int w = 1 << d;
+      for (int s = 0; s < 32; s++) {
+        cd pf = 1.0, pb = 1.0;
+        for (int r = s - w + 1; r <= s; r++) pf = (r >= 0) ? pf * A[r] : cd(0.0);
+        for (int r = s; r < s + w; r++) pb = (r < 32) ? pb * B[r] : cd(0.0);
+        t.tab[6 * n + d * 32 + s] = make_double2(pf.real(), pf.imag());
+        t.tab[6 * n + 5 * 32 + d * 32 + s] = make_double2(pb.real(), pb.imag());
+      }
+    }
   }
   std::vector<cd> z(n, 0.0);
   cd den = 1.0;
@@ -540,30 +827,31 @@ static long largest_pow2_divisor(long v, long cap) {
 struct CnCacheEntry {
   bool valid;
   long n;
-  int bc;
+  int bc, nseg;
   cd cp, c2;
   FastTables ft;
 };
 static CnCacheEntry g_cn_cache[3];
 static void *g_cn_tab_base = nullptr;
 
-static double2 *fast_tables(int slot, long n, int bc, cd cp, cd c2, cudaStream_t st, CnAxis *a) {
+static double2 *fast_tables(int slot, long n, int bc, cd cp, cd c2, int nseg, cudaStream_t st, CnAxis *a) {
   const long nmax = 4096;
   if (n > nmax) {
     gb__set_error(1013, "cn: line length above 4096");
     return nullptr;
   }
-  double2 *base = (double2 *) gb__scratch(GB_SCR_CN, sizeof(double2) * (size_t) (6 * nmax) * 3);
+  const long per = 6 * nmax + 2 * 5 * 32;
+  double2 *base = (double2 *) gb__scratch(GB_SCR_CN, sizeof(double2) * (size_t) per * 3);
   if (!base) return nullptr;
   if (base != g_cn_tab_base) {
     for (int i = 0; i < 3; i++) g_cn_cache[i].valid = false;
     g_cn_tab_base = base;
   }
-  double2 *tab = base + (size_t) (6 * nmax) * slot;
+  double2 *tab = base + (size_t) per * slot;
   CnCacheEntry &e = g_cn_cache[slot];
-  if (!(e.valid && e.n == n && e.bc == bc && e.cp == cp && e.c2 == c2)) {
-    build_fast_tables(n, bc, cp, c2, e.ft);
-    if (cudaMemcpyAsync(tab, e.ft.tab.data(), sizeof(double2) * (size_t) (6 * n), cudaMemcpyHostToDevice, st) !=
+  if (!(e.valid && e.n == n && e.bc == bc && e.nseg == nseg && e.cp == cp && e.c2 == c2)) {
+    build_fast_tables(n, bc, cp, c2, nseg, e.ft);
+    if (cudaMemcpyAsync(tab, e.ft.tab.data(), sizeof(double2) * e.ft.tab.size(), cudaMemcpyHostToDevice, st) !=
             cudaSuccess ||
         cudaStreamSynchronize(st) != cudaSuccess) {
       gb__set_error(3, "cn tables h2d");
@@ -572,6 +860,7 @@ static double2 *fast_tables(int slot, long n, int bc, cd cp, cd c2, cudaStream_t
     e.valid = true;
     e.n = n;
     e.bc = bc;
+    e.nseg = nseg;
     e.cp = cp;
     e.c2 = c2;
   }
@@ -581,7 +870,63 @@ static double2 *fast_tables(int slot, long n, int bc, cd cp, cd c2, cudaStream_t
   return tab;
 }
 
+// Persistent launch of the warp-cooperative kernel: one resident wave of
+// CTAs, each walking the tiles with a stride of the grid.
+static int launch_cn_warp(void *psi, CnAxis &a, bool contig, int axis, cudaStream_t st) {
+  const long pitch = warp_pitch(contig, a.n);
+  const size_t sm = 2 * sizeof(double2) * (size_t) (contig ? (long) kCnWarpLines * pitch : a.n * pitch);
+  long ntiles, tpo = 1;
+  if (contig) {
+    ntiles = (a.outer + kCnWarpLines - 1) / kCnWarpLines;
+  } else {
+    tpo = (a.inner + kCnWarpLines - 1) / kCnWarpLines;
+    ntiles = a.outer * tpo;
+  }
+  if (ntiles <= 0) return 0;
+  // resident CTAs for this (device, kernel, tile size), remembered per kernel
+  struct Occ {
+    int dev;
+    size_t sm;
+    int rg;
+  };
+  static Occ occ[2] = {{-1, 0, 0}, {-1, 0, 0}};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  auto kern = contig ? k_cn_warp<true> : k_cn_warp<false>;
+  Occ &o = occ[contig ? 1 : 0];
+  if (o.dev != dev || o.sm != sm) {
+    // the attribute covers the largest tile (lines of 32 * kLaneSegMax points)
+    const size_t sm_max = 2 * sizeof(double2) * (size_t) (contig ? (long) kCnWarpLines * contig_row(32 * kLaneSegMax)
+                                                               : 32 * kLaneSegMax * (kCnWarpLines + 1));
+    int nsm = 0, per = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm_max);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kCnWarpThreads, sm);
+    cudaGetLastError();
+    o.dev = dev;
+    o.sm = sm;
+    o.rg = (nsm > 0 && per > 0) ? nsm * per : -1;
+  }
+  const int rg = o.rg;
+  if (rg < 0) return gb__set_error(1014, "cn: warp kernel does not fit");
+  const long grid = ntiles < rg ? ntiles : rg;
+  const int slot = gb__pass_begin(15 + axis);
+  kern<<<(unsigned) grid, kCnWarpThreads, sm, st>>>((double2 *) psi, a, ntiles, tpo);
+  gb__pass_end(slot);
+  GB_CHECK_LAUNCH("cn warp");
+  return 0;
+}
+
 }  // namespace
+
+// Warp-cooperative line solver on (1, the default) or off (the
+// segment-per-warp kernel); -1 only queries.
+static int g_cn_warp_on = 1;
+extern "C" int gb_cn_warp_solver(int on) {
+  const int old = g_cn_warp_on;
+  if (on >= 0) g_cn_warp_on = on ? 1 : 0;
+  return old;
+}
 
 extern "C" int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, const gb_potential *pre,
                           const gb_potential *post) {
@@ -658,9 +1003,16 @@ extern "C" int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, co
     a.pre = (s == 0) ? *prep : none_pot;
     a.post = (s == na - 1) ? *postp : none_pot;
 
-    if (fast) {
+    if (fast && a.n <= 32 * kLaneSegMax && g_cn_warp_on) {
       const cd cp = c / tstep;
-      double2 *tab = fast_tables(s, a.n, p->boundary, cp, c2, st, &a);
+      double2 *tab = fast_tables(s, a.n, p->boundary, cp, c2, 32, st, &a);
+      if (!tab) return gb_last_error();
+      a.tab = tab;
+      a.cp = make_double2(cp.real(), cp.imag());
+      GB_TRYC(launch_cn_warp(psi, a, contig, axis, st));
+    } else if (fast) {
+      const cd cp = c / tstep;
+      double2 *tab = fast_tables(s, a.n, p->boundary, cp, c2, kSeg, st, &a);
       if (!tab) return gb_last_error();
       a.tab = tab;
       a.cp = make_double2(cp.real(), cp.imag());

@@ -103,6 +103,116 @@ __global__ void k_merge(C2<T> *dst, const C2<T> *wr, const C2<T> *wi, long nx, l
   }
 }
 
+// FFT convolution in k-space (src/cgrid.c:1912-1944, src/rgrid.c:1848-1878):
+// c = a * b with the sign (-1)^(i + j + k) that moves the result's origin to
+// the grid centre.  nzc complex entries per (i, j) row: nz for a cgrid,
+// nz2 / 2 for the half spectrum of a padded rgrid.
+template <typename T>
+__global__ void k_fft_convolute(C2<T> *c, const C2<T> *a, const C2<T> *b, long ny, long nzc, size_t n) {
+  for (size_t g = blockIdx.x * (size_t) blockDim.x + threadIdx.x; g < n; g += (size_t) gridDim.x * blockDim.x) {
+    const long k = (long) (g % nzc), ij = (long) (g / nzc), j = ij % ny, i = ij / ny;
+    const C2<T> p = cmul(a[g], b[g]);
+    c[g] = ((i + j + k) & 1) ? C2<T>{-p.x, -p.y} : p;
+  }
+}
+
+// Trilinear interpolation of a source grid at the destination's points
+// (cgrid_extrapolate / rgrid_extrapolate, src/cgrid.c:2067-2151,
+// src/rgrid.c:2208-2300): the same coordinate arithmetic, the same boundary
+// values for the corners outside the source (Dirichlet constant, Neumann
+// mirror, periodic wrap) and the same summation order as the reference's
+// cgrid_value (nested) and rgrid_value (eight products, left to right), with
+// every product and sum rounded separately.
+struct InterpArgs {
+  long dnx, dny, dnz, drow;
+  double dstep, dx0, dy0, dz0;
+  long snx, sny, snz, srow;
+  double sstep, sx0, sy0, sz0;
+  int bc;
+  double out_re, out_im;
+};
+
+__device__ __forceinline__ bool interp_map(long &i, long n, int bc) {
+  if (i >= 0 && i < n) return true;
+  if (bc == GB_BC_DIRICHLET) return false;
+  if (bc == GB_BC_PERIODIC) {
+    i %= n;
+    if (i < 0) i += n;
+    return true;
+  }
+  if (i < 0) i = -i;
+  if (i > n - 1) i = 2 * n - i - 2;
+  if (i < 0 || i >= n) i = 0;
+  return true;
+}
+
+// Value of the source at (i, j, k), with the boundary rule outside.
+template <bool REAL>
+__device__ __forceinline__ double2 interp_fetch(const void *src, long i, long j, long k, const InterpArgs &a) {
+  if (i < 0 || i >= a.snx || j < 0 || j >= a.sny || k < 0 || k >= a.snz) {
+    if (a.bc == GB_BC_DIRICHLET || !interp_map(i, a.snx, a.bc) || !interp_map(j, a.sny, a.bc) ||
+        !interp_map(k, a.snz, a.bc))
+      return make_double2(a.out_re, REAL ? 0.0 : a.out_im);
+  }
+  const size_t q = (size_t) (i * a.sny + j) * a.srow + k;
+  if (REAL) return make_double2(((const double *) src)[q], 0.0);
+  return ((const double2 *) src)[q];
+}
+
+// index and fraction along one axis (src/cgrid.c:2074-2078)
+__device__ __forceinline__ long interp_axis(double c, double x0, double step, long n, double &f) {
+  double x = __ddiv_rn(__dadd_rn(c, x0), step);
+  long i = (long) x;
+  if (x < 0) i--;
+  f = __dsub_rn(x, (double) i);
+  return i + n / 2;
+}
+
+template <bool REAL> __global__ void k_interp(void *dst, const void *src, InterpArgs a) {
+  const size_t n = (size_t) a.dnx * a.dny * a.dnz;
+  for (size_t g = blockIdx.x * (size_t) blockDim.x + threadIdx.x; g < n; g += (size_t) gridDim.x * blockDim.x) {
+    const long kd = (long) (g % a.dnz), ij = (long) (g / a.dnz), jd = ij % a.dny, id = ij / a.dny;
+    const double xc = __dsub_rn(__dmul_rn((double) (id - a.dnx / 2), a.dstep), a.dx0);
+    const double yc = __dsub_rn(__dmul_rn((double) (jd - a.dny / 2), a.dstep), a.dy0);
+    const double zc = __dsub_rn(__dmul_rn((double) (kd - a.dnz / 2), a.dstep), a.dz0);
+    double x, y, z;
+    const long i = interp_axis(xc, a.sx0, a.sstep, a.snx, x);
+    const long j = interp_axis(yc, a.sy0, a.sstep, a.sny, y);
+    const long k = interp_axis(zc, a.sz0, a.sstep, a.snz, z);
+    const double2 f000 = interp_fetch<REAL>(src, i, j, k, a), f100 = interp_fetch<REAL>(src, i + 1, j, k, a),
+                  f010 = interp_fetch<REAL>(src, i, j + 1, k, a), f001 = interp_fetch<REAL>(src, i, j, k + 1, a),
+                  f110 = interp_fetch<REAL>(src, i + 1, j + 1, k, a), f101 = interp_fetch<REAL>(src, i + 1, j, k + 1, a),
+                  f011 = interp_fetch<REAL>(src, i, j + 1, k + 1, a),
+                  f111 = interp_fetch<REAL>(src, i + 1, j + 1, k + 1, a);
+    const double omx = __dsub_rn(1.0, x), omy = __dsub_rn(1.0, y), omz = __dsub_rn(1.0, z);
+    const size_t q = (size_t) (id * a.dny + jd) * a.drow + kd;
+    if (REAL) {
+      // omx omy omz f000 + x omy omz f100 + omx y omz f010 + omx omy z f001
+      //   + x y omz f110 + x omy z f101 + omx y z f011 + x y z f111
+      auto t3 = [](double p, double q2, double r, double f) { return __dmul_rn(__dmul_rn(__dmul_rn(p, q2), r), f); };
+      double s = t3(omx, omy, omz, f000.x);
+      s = __dadd_rn(s, t3(x, omy, omz, f100.x));
+      s = __dadd_rn(s, t3(omx, y, omz, f010.x));
+      s = __dadd_rn(s, t3(omx, omy, z, f001.x));
+      s = __dadd_rn(s, t3(x, y, omz, f110.x));
+      s = __dadd_rn(s, t3(x, omy, z, f101.x));
+      s = __dadd_rn(s, t3(omx, y, z, f011.x));
+      s = __dadd_rn(s, t3(x, y, z, f111.x));
+      ((double *) dst)[q] = s;
+    } else {
+      // omx (omy (omz f000 + z f001) + y (omz f010 + z f011))
+      //   + x (omy (omz f100 + z f101) + y (omz f110 + z f111)), per component
+      auto lin = [](double w0, double a0, double w1, double a1) { return __dadd_rn(__dmul_rn(w0, a0), __dmul_rn(w1, a1)); };
+      double2 r;
+      r.x = lin(omx, lin(omy, lin(omz, f000.x, z, f001.x), y, lin(omz, f010.x, z, f011.x)), x,
+                lin(omy, lin(omz, f100.x, z, f101.x), y, lin(omz, f110.x, z, f111.x)));
+      r.y = lin(omx, lin(omy, lin(omz, f000.y, z, f001.y), y, lin(omz, f010.y, z, f011.y)), x,
+                lin(omy, lin(omz, f100.y, z, f101.y), y, lin(omz, f110.y, z, f111.y)));
+      ((double2 *) dst)[q] = r;
+    }
+  }
+}
+
 // Padded real rows (nz2 scalars = nz/2 + 1 complex) <-> complex grids.
 __global__ void k_r2c_pack(double2 *r, const double2 *c, long nx, long ny, long nz) {
   const long nh = nz / 2 + 1;
@@ -323,6 +433,49 @@ extern "C" int gb_wf_merge(void *dst, const void *wr, const void *wi, const gb_g
                                                                    (const double2 *) wi, g->nx, g->ny, g->nz, lx, hx, ly,
                                                                    hy, lz, hz);
   GB_CHECK_LAUNCH("merge");
+  return 0;
+}
+
+extern "C" int gb_fft_convolute(void *c, const void *a, const void *b, long nx, long ny, long nzc, int prec) {
+  const size_t n = (size_t) nx * ny * nzc;
+  if (n == 0) return 0;
+  if (prec == GB_FP32)
+    k_fft_convolute<float><<<blocks_for(n), kThreads, 0, gb__stream()>>>((float2 *) c, (const float2 *) a,
+                                                                          (const float2 *) b, ny, nzc, n);
+  else
+    k_fft_convolute<double><<<blocks_for(n), kThreads, 0, gb__stream()>>>((double2 *) c, (const double2 *) a,
+                                                                           (const double2 *) b, ny, nzc, n);
+  GB_CHECK_LAUNCH("fft convolute");
+  return 0;
+}
+
+extern "C" int gb_interpolate(void *dst, const gb_grid_frame *d, const void *src, const gb_grid_frame *s, int bc,
+                              double out_re, double out_im, int is_real) {
+  InterpArgs a;
+  a.dnx = d->nx;
+  a.dny = d->ny;
+  a.dnz = d->nz;
+  a.drow = d->row;
+  a.dstep = d->step;
+  a.dx0 = d->x0;
+  a.dy0 = d->y0;
+  a.dz0 = d->z0;
+  a.snx = s->nx;
+  a.sny = s->ny;
+  a.snz = s->nz;
+  a.srow = s->row;
+  a.sstep = s->step;
+  a.sx0 = s->x0;
+  a.sy0 = s->y0;
+  a.sz0 = s->z0;
+  a.bc = bc;
+  a.out_re = out_re;
+  a.out_im = out_im;
+  const size_t n = (size_t) a.dnx * a.dny * a.dnz;
+  if (n == 0) return 0;
+  if (is_real) k_interp<true><<<blocks_for(n), kThreads, 0, gb__stream()>>>(dst, src, a);
+  else k_interp<false><<<blocks_for(n), kThreads, 0, gb__stream()>>>(dst, src, a);
+  GB_CHECK_LAUNCH("interpolate");
   return 0;
 }
 

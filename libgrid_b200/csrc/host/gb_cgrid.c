@@ -147,8 +147,25 @@ void cgrid_write(cgrid *grid, FILE *out) {
   fwrite(grid->value, sizeof(REAL complex), npts(grid), out);
 }
 
-/* src/cgrid.c:383-420 (same-size files; the reference interpolates other
- * sizes through cgrid_extrapolate, which this path does not provide) */
+/* src/cgrid.c:2126-2151: dest = trilinear interpolation of src at dest's
+ * points (src's boundary rule outside src), on the GPU. */
+void cgrid_extrapolate(cgrid *dest, cgrid *src) {
+  if (dest == src) {
+    fprintf(stderr, "libgrid: Source and destination grids cannot be the same in cgrid_extrapolate().\n");
+    abort();
+  }
+  double ore, oim;
+  const int bc = gbh_cbc(src, &ore, &oim);
+  const gb_grid_frame d = {dest->nx, dest->ny, dest->nz, dest->nz, dest->step, dest->x0, dest->y0, dest->z0};
+  const gb_grid_frame s = {src->nx, src->ny, src->nz, src->nz, src->step, src->x0, src->y0, src->z0};
+  out_prec(dest, GB_FP64);
+  const void *ds = gbh_dev_read(src->value, GB_FP64);
+  void *dd = gbh_dev_write(dest->value, GB_FP64);
+  gbh_check(gb_interpolate(dd, &d, ds, &s, bc, ore, oim, 0), "cgrid_extrapolate");
+}
+
+/* src/cgrid.c:383-420: a file of another size or step is read into a
+ * temporary grid and interpolated onto `grid` (cgrid_extrapolate). */
 cgrid *cgrid_read(cgrid *grid, FILE *in) {
   INT nx, ny, nz;
   REAL step;
@@ -163,10 +180,21 @@ cgrid *cgrid_read(cgrid *grid, FILE *in) {
       return NULL;
     }
   }
-  if (nx != grid->nx || ny != grid->ny || nz != grid->nz || step != grid->step)
-    gbh_die("cgrid_read(): grid in file (%ld x %ld x %ld, step %g) differs from the grid in memory; interpolation between "
-            "grids is not provided.",
-            nx, ny, nz, step);
+  if (nx != grid->nx || ny != grid->ny || nz != grid->nz || step != grid->step) {
+    cgrid *tmp;
+    fprintf(stderr, "libgrid: Grid in file has different size than grid in memory.\n");
+    fprintf(stderr, "libgrid: Interpolating between grids.\n");
+    if (!(tmp = cgrid_alloc(nx, ny, nz, step, grid->value_outside, NULL, "cgrid_read_temp"))) {
+      fprintf(stderr, "libgrid: Error allocating grid in cgrid_read().\n");
+      abort();
+    }
+    if (fread(tmp->value, sizeof(REAL complex), npts(tmp), in) != npts(tmp))
+      fprintf(stderr, "libgrid: Short read in cgrid_read().\n");
+    gbh_host_modified(tmp->value);
+    cgrid_extrapolate(grid, tmp);
+    cgrid_free(tmp);
+    return grid;
+  }
   if (fread(grid->value, sizeof(REAL complex), npts(grid), in) != npts(grid)) {
     fprintf(stderr, "libgrid: Short read in cgrid_read().\n");
   }
@@ -236,6 +264,18 @@ static void binary(int op, cgrid *c, cgrid *a, cgrid *b, const char *fn) {
   const void *db = b ? gbh_dev_read(b->value, p) : NULL;
   void *dc = gbh_dev_write(c->value, p);
   gbh_check(gb_complex_op(op, dc, da, db, npts(c), 0.0, 0.0, p), fn);
+}
+
+/* src/cgrid.c:1912-1944: c = (-1)^(i+j+k) a b in k-space */
+void cgrid_fft_convolute(cgrid *gridc, cgrid *grida, cgrid *gridb) {
+  same_shape(gridc, grida, "cgrid_fft_convolute");
+  same_shape(gridc, gridb, "cgrid_fft_convolute");
+  const int p = op_prec3(gridc, grida, gridb);
+  out_prec(gridc, p);
+  const void *da = gbh_dev_read(grida->value, p);
+  const void *db = gbh_dev_read(gridb->value, p);
+  void *dc = gbh_dev_write(gridc->value, p);
+  gbh_check(gb_fft_convolute(dc, da, db, gridc->nx, gridc->ny, gridc->nz, p), "cgrid_fft_convolute");
 }
 
 /* src/cgrid.c:934,964,994,1169 */

@@ -181,6 +181,80 @@ void rgrid_scaled_inverse_fft(rgrid *grid, REAL c) {
 }
 
 void rgrid_inverse_fft_norm(rgrid *grid) { rgrid_scaled_inverse_fft(grid, grid->fft_norm); }
+/* src/rgrid.c:1824 */
+void rgrid_inverse_fft_norm2(rgrid *grid) { rgrid_scaled_inverse_fft(grid, grid->fft_norm2); }
+
+/* src/rgrid.c:1848-1878: on the half spectrum (nz2 / 2 complex entries per
+ * row) left by rgrid_fft */
+void rgrid_fft_convolute(rgrid *gridc, rgrid *grida, rgrid *gridb) {
+  if (gridc->nx != grida->nx || gridc->ny != grida->ny || gridc->nz != grida->nz || gridc->nx != gridb->nx ||
+      gridc->ny != gridb->ny || gridc->nz != gridb->nz)
+    gbh_die("Different grid dimensions in rgrid_fft_convolute.");
+  const void *da = gbh_dev_read(grida->value, GB_FP64);
+  const void *db = gbh_dev_read(gridb->value, GB_FP64);
+  void *dc = gbh_dev_write(gridc->value, GB_FP64);
+  gbh_check(gb_fft_convolute(dc, da, db, gridc->nx, gridc->ny, gridc->nz2 / 2, GB_FP64), "rgrid_fft_convolute");
+}
+
+/* src/rgrid.c:2267-2291 */
+void rgrid_extrapolate(rgrid *dest, rgrid *src) {
+  double out;
+  const int bc = gbh_rbc(src, &out);
+  const gb_grid_frame d = {dest->nx, dest->ny, dest->nz, dest->nz2, dest->step, dest->x0, dest->y0, dest->z0};
+  const gb_grid_frame s = {src->nx, src->ny, src->nz, src->nz2, src->step, src->x0, src->y0, src->z0};
+  const void *ds = gbh_dev_read(src->value, GB_FP64);
+  void *dd = gbh_dev_rw(dest->value, GB_FP64); /* the row padding keeps its values */
+  gbh_check(gb_interpolate(dd, &d, ds, &s, bc, out, 0.0, 1), "rgrid_extrapolate");
+}
+
+/* src/rgrid.c:339-349: nx, ny, nz (INT), step (REAL), then nx ny nz2 values
+ * (the padded rows as stored) */
+void rgrid_write(rgrid *grid, FILE *out) {
+  gbh_host_read(grid->value);
+  fwrite(&grid->nx, sizeof(INT), 1, out);
+  fwrite(&grid->ny, sizeof(INT), 1, out);
+  fwrite(&grid->nz, sizeof(INT), 1, out);
+  fwrite(&grid->step, sizeof(REAL), 1, out);
+  fwrite(grid->value, sizeof(REAL), nscal(grid), out);
+}
+
+/* src/rgrid.c:360-400: a file of another size or step is read into a
+ * temporary grid and interpolated onto `grid` (rgrid_extrapolate). */
+rgrid *rgrid_read(rgrid *grid, FILE *in) {
+  INT nx, ny, nz, nzz;
+  REAL step;
+  if (fread(&nx, sizeof(INT), 1, in) != 1 || fread(&ny, sizeof(INT), 1, in) != 1 || fread(&nz, sizeof(INT), 1, in) != 1 ||
+      fread(&step, sizeof(REAL), 1, in) != 1) {
+    fprintf(stderr, "libgrid: Error reading grid header in rgrid_read().\n");
+    return NULL;
+  }
+  nzz = 2 * (nz / 2 + 1);
+  if (!grid) {
+    if (!(grid = rgrid_alloc(nx, ny, nz, step, RGRID_PERIODIC_BOUNDARY, NULL, "read_grid"))) {
+      fprintf(stderr, "libgrid: Failed to allocate grid in rgrid_read().\n");
+      return NULL;
+    }
+  }
+  if (nx != grid->nx || ny != grid->ny || nz != grid->nz || step != grid->step) {
+    rgrid *tmp;
+    fprintf(stderr, "libgrid: Grid in file has different size than grid in memory.\n");
+    fprintf(stderr, "libgrid: Interpolating between grids.\n");
+    if (!(tmp = rgrid_alloc(nx, ny, nz, step, grid->value_outside, NULL, "rgrid_read_temp"))) {
+      fprintf(stderr, "libgrid: Error allocating grid in rgrid_read().\n");
+      abort();
+    }
+    if (fread(tmp->value, sizeof(REAL), (size_t) (nx * ny * nzz), in) != (size_t) (nx * ny * nzz))
+      fprintf(stderr, "libgrid: Short read in rgrid_read().\n");
+    gbh_host_modified(tmp->value);
+    rgrid_extrapolate(grid, tmp);
+    rgrid_free(tmp);
+    return grid;
+  }
+  if (fread(grid->value, sizeof(REAL), (size_t) (nx * ny * nzz), in) != (size_t) (nx * ny * nzz))
+    fprintf(stderr, "libgrid: Short read in rgrid_read().\n");
+  gbh_host_modified(grid->value);
+  return grid;
+}
 
 /* src/rgrid.c:2020-2060 */
 REAL rgrid_value_at_index(rgrid *grid, INT i, INT j, INT k) {

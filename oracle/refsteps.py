@@ -51,9 +51,9 @@ class _Base:
             # the reference's non-periodic CN sweeps dereference the third
             # workspace pointer although only the periodic case allocates it
             # (src/grid_wf_cn.c:72-74,126); the caller provides it
+            # (grid_wf_free releases it with the wavefunction, src/grid_wf.c:157-166)
             ws3 = ref.cgrid(*self.shape, step, bc=bcname)
             self.w.s.cworkspace3 = ws3.ptr
-            self._owned.append(ws3)
 
     def psi(self) -> np.ndarray:
         return self.w.grid.get()

@@ -68,11 +68,11 @@ def run_case(ref, name):
         if s in c["checkpoints"]:
             record(s)
             print("%s: step %d (%.0f s)" % (name, s, time.time() - t0), flush=True)
-    st.free()
     meta = {"meta_" + k: np.asarray(val) for k, val in c.items() if k != "kind"}
     meta["meta_mass"] = np.asarray(mass)
     np.savez_compressed(os.path.join(HERE, name + "_traj.npz"), **out, **meta)
     print("wrote", name, flush=True)
+    st.free()
 
 
 def main(argv):

@@ -213,7 +213,7 @@ def b200_cn_run(b200, psi0, v, step, mass, time, bc, nsteps, k0=(0.0, 0.0, 0.0),
 
 
 @pytest.mark.parametrize("bc", [DIR, NEU, PER])
-@pytest.mark.parametrize("shape", [(12, 10, 14), (24, 24, 24), (1, 40, 48), (2, 3, 64)])
+@pytest.mark.parametrize("shape", [(12, 10, 14), (24, 24, 24), (1, 40, 48), (2, 3, 64), (3, 2, 300), (33, 5, 7)])
 @pytest.mark.parametrize("time", [0.05, -0.2j])
 def test_cn_step(b200, restate, bc, shape, time):
     rng = np.random.default_rng(17)
@@ -241,6 +241,27 @@ def test_cn_rotation_and_absorber(b200, restate, bc):
     for _ in range(3):
         want = restate.cn_step(want, step, mass, 0.05, bc, omega=0.3, vc=v, absorb=absorb)
     assert rel(got, want) < TOL_PSI
+
+
+@pytest.mark.parametrize("bc", [DIR, NEU, PER])
+@pytest.mark.parametrize("shape", [(16, 192, 200), (256, 4, 33)])
+def test_cn_line_solvers_agree(b200, bc, shape):
+    """The warp-cooperative line solver (lines up to 256 points, segment
+    carries by a warp-shuffle scan) and the segment-per-warp solver solve the
+    same systems; they differ only in rounding."""
+    lib = b200.lib
+    step, g = 0.3, 0.001
+    mass = 4.0 / workloads.GRID_AUTOAMU
+    psi0, v = workloads.cn_wells(shape, step, g, seed=21)
+    out = []
+    old = lib.gb_cn_warp_solver(-1)
+    try:
+        for on in (1, 0):
+            lib.gb_cn_warp_solver(on)
+            out.append(b200_cn_run(b200, psi0, None, step, mass, 0.5, bc, 3, k0=(0.1, 0.0, -0.2), gp=(v, g)))
+    finally:
+        lib.gb_cn_warp_solver(old)
+    assert rel(out[0], out[1]) < 1e-13
 
 
 def test_cn_gp_dirichlet(b200, restate):
