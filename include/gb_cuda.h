@@ -260,6 +260,15 @@ int gb_interpolate(void *dst, const gb_grid_frame *d, const void *src, const gb_
 #define GB_RED_REAL_SUM 6     /* sum a, a real with rows of arow */
 #define GB_RED_KSQ_NORM2 7    /* sum |k|^2 |a|^2 on the unshifted frequency grid */
 int gb_reduce(int op, const void *a, const void *b, const gb_geom *g, long arow, long brow, int bprec, double *out);
+/* psi *= sqrt(target / (step_factor * sum |psi|^2)) with the sum reduced into
+ * a device scalar that the scale kernel reads: no host synchronisation
+ * (src/grid_wf.c:681-700 computes the same scale on the host).  FP64 or
+ * FP32 storage (g->prec). */
+int gb_normalize_device(void *psi, const gb_geom *g, double target, double step_factor);
+/* out4 = {sum max(0, mu - V), #points with V < mu, min V, sum V} over a
+ * padded real grid (vrow scalars per row): the terms of a Newton iteration
+ * for the Thomas-Fermi chemical potential.  (No reference counterpart.) */
+int gb_tf_stats(const void *v, const gb_geom *g, long vrow, double mu, double *out4);
 
 /*
  * gb_reduce without any device allocation: no reference counterpart.  For
@@ -416,6 +425,38 @@ int gb_unet_adam(float *w, uint16_t *wb, float *m, float *v, float *g, long n, f
 int gb_unet_to_bf16(const float *w, uint16_t *wb, long n);
 /* p[0..n) = v. */
 int gb_unet_fill(float *p, long n, float v);
+/* Convolution engine: 1 (the default) runs the forward and data-gradient
+ * convolutions as tcgen05 implicit GEMMs (bf16 operands in shared memory,
+ * FP32 accumulators in tensor memory) and the weight gradient on mma.sync
+ * bf16 tensor-core instructions (FP32 accumulate), with activations and
+ * gradients rounded to bf16 as operands; 0 runs the FP32 SIMT kernels
+ * (FP32 activations, bf16 weights).  Shapes without a tensor-core plan
+ * (weight gradients of volumes narrower than 16 points, more than 64
+ * output channels) always run SIMT.  -1 only queries; returns the previous
+ * setting.  (No reference counterpart.) */
+int gb_unet_tensor_cores(int on);
+/* Warm-start inputs and guesses built on the device (no host round trip of
+ * the 3-D arrays):
+ *   gb_unet_potential  V = k r^2 / 2 + sum of Gaussian bumps a exp(-|r-c|^2/w^2)
+ *                      on x_i = (i - n/2) step, into a padded real grid;
+ *   gb_unet_features   the network input [3][n]: tanh((V - vmin)/vscale),
+ *                      gfeat, sqrt(max(mu - V, 0)/g) / amax;
+ *   gb_unet_amplitude  psi = max(amp * scale, 0) + floor (real) into a
+ *                      complex grid of precision prec;
+ *   gb_unet_gaussian   exp(-r^2 / width^2).
+ * (No reference counterpart.) */
+#define GB_UNET_MAX_BUMPS 8
+typedef struct {
+  int n;
+  double amp[GB_UNET_MAX_BUMPS], w[GB_UNET_MAX_BUMPS], c[GB_UNET_MAX_BUMPS][3];
+} gb_unet_bumps;
+int gb_unet_potential(double *v, int nx, int ny, int nz, long vrow, double step, double k, const gb_unet_bumps *bumps);
+int gb_unet_features(const double *v, int nx, int ny, int nz, long vrow, double vmin, double vscale, float gfeat,
+                     double mu, double g, double amax, float *out);
+int gb_unet_amplitude(const float *amp, float scale, float floor, void *psi, long n, int prec);
+int gb_unet_gaussian(float *out, int nx, int ny, int nz, double step, double width);
+/* out = |psi| * inv_scale from a complex grid (device pointer, precision prec). */
+int gb_unet_abs(const void *psi, int prec, long n, float inv_scale, float *out);
 
 #ifdef __cplusplus
 }

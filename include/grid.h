@@ -363,6 +363,23 @@ void grid_wf_propagate_gp(wf *gwf, rgrid *vext, REAL g, REAL complex time);
  */
 void grid_wf_propagate_n(wf *gwf, cgrid *potential, REAL complex time, INT nsteps);
 void grid_wf_propagate_gp_n(wf *gwf, rgrid *vext, REAL g, REAL complex time, INT nsteps);
+/*
+ * Imaginary-time relaxation steps (no reference counterpart as one call):
+ * nsteps of grid_wf_propagate_gp(time), each followed by renormalisation to
+ * gwf->norm as grid_wf_normalize makes it (src/grid_wf.c:681-700), with the
+ * norm reduced and applied on the device: no host synchronisation.
+ */
+void grid_wf_relax_gp_n(wf *gwf, rgrid *vext, REAL g, REAL complex time, INT nsteps);
+/* psi = max(amp * scale, 0) + floor (real) from a device float array of
+ * nx ny nz values (a device-side initial guess; no reference counterpart). */
+void grid_wf_set_amplitude_device(wf *gwf, const float *amp, REAL scale, REAL floor);
+/* Host/device coherence of a grid's value array (no reference counterpart):
+ * refresh the host copy; declare host-side writes; or get the FP64 device
+ * copy for device-side producers and consumers (mode 0 read, 1 write (every
+ * value is overwritten), 2 read and write). */
+void gb_grid_sync_host(void *host_mem);
+void gb_grid_host_modified(void *host_mem);
+void *gb_grid_device(void *host_mem, int mode);
 /* Select GRID_PREC_FP64 (default) or GRID_PREC_FP32 for gwf's device data. */
 void grid_wf_precision(wf *gwf, char mode);
 char grid_wf_get_precision(wf *gwf);

@@ -96,17 +96,18 @@ __device__ __forceinline__ double cn_absorb(long i, long j, long k, const CnAxis
   return t > 1.0 ? 1.0 : t;
 }
 
-// psi * exp(c (cons + V + g |psi|^2)) (src/grid_wf.c:586-598)
-__device__ __forceinline__ double2 cn_pot(double2 x, long ix, long iy, long iz, const CnAxis &a, const gb_potential &pt) {
-  double wr = pt.cons, wi = 0.0;
+// V at (ix, iy, iz) as (re, im); zero without a potential grid.
+__device__ __forceinline__ double2 cn_pot_v(long ix, long iy, long iz, const CnAxis &a, const gb_potential &pt) {
   const long vidx = (ix * a.ny + iy) * pt.vrow + iz;
-  if (pt.kind == GB_POT_COMPLEX) {
-    const double2 v = ((const double2 *) pt.v)[vidx];
-    wr += v.x;
-    wi += v.y;
-  } else if (pt.kind == GB_POT_REAL) {
-    wr += ((const double *) pt.v)[vidx];
-  }
+  if (pt.kind == GB_POT_COMPLEX) return ((const double2 *) pt.v)[vidx];
+  if (pt.kind == GB_POT_REAL) return make_double2(((const double *) pt.v)[vidx], 0.0);
+  return make_double2(0.0, 0.0);
+}
+
+// psi * exp(c (cons + V + g |psi|^2)) (src/grid_wf.c:586-598), V given
+__device__ __forceinline__ double2 cn_pot_with(double2 x, double2 v, long ix, long iy, long iz,
+                                               const gb_potential &pt) {
+  double wr = pt.cons + v.x, wi = v.y;
   if (pt.g != 0.0) wr += pt.g * (x.x * x.x + x.y * x.y);
   double cr = pt.c_re, ci = pt.c_im;
   if (pt.absorb) {
@@ -131,6 +132,10 @@ __device__ __forceinline__ double2 cn_pot(double2 x, long ix, long iy, long iz, 
     c *= m;
   }
   return cm(x, make_double2(c, s));
+}
+
+__device__ __forceinline__ double2 cn_pot(double2 x, long ix, long iy, long iz, const CnAxis &a, const gb_potential &pt) {
+  return cn_pot_with(x, cn_pot_v(ix, iy, iz, a, pt), ix, iy, iz, pt);
 }
 
 // Right-hand side row i of a line (src/grid_wf_cn.c:139-201 and the y/z
@@ -368,10 +373,15 @@ template <bool CONTIG> __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast
 // pitch W + 1), so the lanes' segment accesses hit at most two-way bank
 // conflicts.
 constexpr int kLaneSegMax = 8;
-constexpr int kCnWarpLines = 8;  // lines per tile = warps per CTA
-constexpr int kCnWarpThreads = 32 * kCnWarpLines;
+constexpr int kCnWarps = 8;  // warps per CTA
+constexpr int kCnWarpThreads = 32 * kCnWarps;
+// lines per tile: one per warp on the contiguous axis; two per warp on the
+// strided axes, so each row of a strided tile is one 256-byte copy
+template <bool CONTIG> __host__ __device__ constexpr int tile_lines() { return CONTIG ? kCnWarps : 2 * kCnWarps; }
 
-__host__ __device__ inline long warp_pitch(bool contig, long n) { return contig ? contig_row(n) : kCnWarpLines + 1; }
+__host__ __device__ inline long warp_pitch(bool contig, long n) {
+  return contig ? contig_row(n) : (contig ? kCnWarps : 2 * kCnWarps) + 1;
+}
 
 // Offsets of the scan tables behind the six per-element tables.
 __host__ __device__ inline long warp_scan_off(long n) { return 6 * n; }
@@ -386,8 +396,8 @@ __device__ __forceinline__ double2 shfl_down2(double2 v, int d) {
   return make_double2(__shfl_down_sync(0xffffffffu, v.x, d), __shfl_down_sync(0xffffffffu, v.y, d));
 }
 
-// Solve line l of the tile in place (the whole warp).
-template <bool CONTIG>
+// Solve line l of the tile in place (the whole warp); SMAX >= ceil(n / 32).
+template <bool CONTIG, int SMAX>
 __device__ __forceinline__ void cn_warp_line(double2 *sm, long pitch, int l, const CnAxis &a, int lane) {
   const long n = a.n;
   const int S = (int) ((n + 31) >> 5);
@@ -399,9 +409,9 @@ __device__ __forceinline__ void cn_warp_line(double2 *sm, long pitch, int l, con
   auto at = [&](long i) -> double2 & { return CONTIG ? sm[(long) l * pitch + i] : sm[i * pitch + l]; };
   const long a0 = (long) lane * S;
   const int cnt = (int) (a0 >= n ? 0 : (n - a0 < S ? n - a0 : S));
-  double2 p[kLaneSegMax];
+  double2 p[SMAX];
 #pragma unroll
-  for (int j = 0; j < kLaneSegMax; j++) p[j] = (j < cnt) ? at(a0 + j) : zero;
+  for (int j = 0; j < SMAX; j++) p[j] = (j < cnt) ? at(a0 + j) : zero;
   // the line's first and last elements and the segment neighbours, read
   // before any lane writes (selecting them from the register arrays by a
   // runtime index would move the arrays to local memory)
@@ -413,7 +423,7 @@ __device__ __forceinline__ void cn_warp_line(double2 *sm, long pitch, int l, con
   // right-hand side and forward particular recurrence (zero carry-in)
   double2 u = zero, pm = p_before;
 #pragma unroll
-  for (int j = 0; j < kLaneSegMax; j++) {
+  for (int j = 0; j < SMAX; j++) {
     if (j < cnt) {
       const long i = a0 + j;
       const double2 p0 = p[j];
@@ -436,7 +446,7 @@ __device__ __forceinline__ void cn_warp_line(double2 *sm, long pitch, int l, con
   // forward fix-up fused with the backward particular recurrence
   double2 yv = zero, ystart = zero;
 #pragma unroll
-  for (int j = kLaneSegMax - 1; j >= 0; j--) {
+  for (int j = SMAX - 1; j >= 0; j--) {
     if (j < cnt) {
       const long i = a0 + j;
       const double2 v = ca(p[j], cm(__ldg(tH + i), vin));
@@ -455,7 +465,7 @@ __device__ __forceinline__ void cn_warp_line(double2 *sm, long pitch, int l, con
   double2 xin = shfl_down2(x, 1);
   if (lane == 31) xin = zero;
 #pragma unroll
-  for (int j = 0; j < kLaneSegMax; j++)
+  for (int j = 0; j < SMAX; j++)
     if (j < cnt) {
       p[j] = ca(p[j], cm(__ldg(tG + a0 + j), xin));
       at(a0 + j) = p[j];
@@ -468,17 +478,20 @@ __device__ __forceinline__ void cn_warp_line(double2 *sm, long pitch, int l, con
     const double2 fact = cm(ca(x0, cm(a.beta, cm(xl, a.gamma))), a.den);  // gamma, den hold reciprocals
     __syncwarp();
 #pragma unroll
-    for (int j = 0; j < kLaneSegMax; j++)
+    for (int j = 0; j < SMAX; j++)
       if (j < cnt) at(a0 + j) = cs(p[j], cm(fact, __ldg(tz + a0 + j)));
   }
 }
 
-// Potential half-step on every element of a tile (all threads).
+// Potential half-step on every element of a tile (all threads); the V
+// values of a batch of elements are loaded before any phase is applied, so
+// their global loads overlap.
 template <bool CONTIG>
 __device__ __forceinline__ void cn_tile_pot(double2 *sm, long pitch, int nl, long line0, long o, long col0,
                                             const CnAxis &a, const gb_potential &pt) {
-  const long n = a.n;
-  for (long e = threadIdx.x; e < (long) nl * n; e += blockDim.x) {
+  constexpr int B = 4;
+  const long n = a.n, total = (long) nl * n;
+  auto where = [&](long e, long &ix, long &iy, long &iz) -> int {
     long l, i;
     if constexpr (CONTIG) {
       l = e / n;
@@ -487,10 +500,30 @@ __device__ __forceinline__ void cn_tile_pot(double2 *sm, long pitch, int nl, lon
       i = e / nl;
       l = e - i * nl;
     }
-    long ix, iy, iz;
     cn_decode(a, CONTIG ? line0 + l : o, i, col0 + l, ix, iy, iz);
-    double2 &r = CONTIG ? sm[l * pitch + i] : sm[i * pitch + l];
-    r = cn_pot(r, ix, iy, iz, a, pt);
+    return (int) (CONTIG ? l * pitch + i : i * pitch + l);
+  };
+  for (long e0 = threadIdx.x; e0 < total; e0 += (long) blockDim.x * B) {
+    double2 v[B];
+#pragma unroll
+    for (int k = 0; k < B; k++) {
+      const long e = e0 + (long) k * blockDim.x;
+      v[k] = make_double2(0.0, 0.0);
+      if (e < total) {
+        long ix, iy, iz;
+        where(e, ix, iy, iz);
+        v[k] = cn_pot_v(ix, iy, iz, a, pt);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < B; k++) {
+      const long e = e0 + (long) k * blockDim.x;
+      if (e < total) {
+        long ix, iy, iz;
+        const int q = where(e, ix, iy, iz);
+        sm[q] = cn_pot_with(sm[q], v[k], ix, iy, iz, pt);
+      }
+    }
   }
 }
 
@@ -501,16 +534,17 @@ struct CnTile {
 
 template <bool CONTIG> __device__ __forceinline__ CnTile cn_tile_of(const CnAxis &a, long t, long tpo) {
   CnTile c;
+  constexpr int TL = tile_lines<CONTIG>();
   if constexpr (CONTIG) {
-    c.line0 = t * kCnWarpLines;
+    c.line0 = t * TL;
     const long rem = a.outer - c.line0;
-    c.nl = (int) (rem < kCnWarpLines ? rem : kCnWarpLines);
+    c.nl = (int) (rem < TL ? rem : TL);
     c.o = c.col0 = 0;
   } else {
     c.o = t / tpo;
-    c.col0 = (t - c.o * tpo) * kCnWarpLines;
+    c.col0 = (t - c.o * tpo) * TL;
     const long rem = a.inner - c.col0;
-    c.nl = (int) (rem < kCnWarpLines ? rem : kCnWarpLines);
+    c.nl = (int) (rem < TL ? rem : TL);
     c.line0 = 0;
   }
   return c;
@@ -537,14 +571,14 @@ __device__ __forceinline__ void cn_tile_copy(double2 *psi, double2 *buf, long pi
   }
 }
 
-template <bool CONTIG>
+template <bool CONTIG, int SMAX>
 __global__ void __launch_bounds__(kCnWarpThreads, 2) k_cn_warp(double2 *__restrict__ psi, CnAxis a, long ntiles, long tpo) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ __align__(8) uint64_t bars[2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const long n = a.n;
   const long pitch = warp_pitch(CONTIG, n);
-  const long bufsz = CONTIG ? (long) kCnWarpLines * pitch : n * pitch;
+  const long bufsz = CONTIG ? (long) tile_lines<CONTIG>() * pitch : n * pitch;
   double2 *const buf0 = (double2 *) smraw;
   auto buf = [&](int b) { return buf0 + (b ? bufsz : 0); };
   if (tid == 0) {
@@ -593,7 +627,7 @@ __global__ void __launch_bounds__(kCnWarpThreads, 2) k_cn_warp(double2 *__restri
       cn_tile_pot<CONTIG>(sm, pitch, c.nl, c.line0, c.o, c.col0, a, a.pre);
       __syncthreads();
     }
-    if (warp < c.nl) cn_warp_line<CONTIG>(sm, pitch, warp, a, lane);
+    for (int l = warp; l < c.nl; l += kCnWarps) cn_warp_line<CONTIG, SMAX>(sm, pitch, l, a, lane);
     if (post) {
       __syncthreads();
       cn_tile_pot<CONTIG>(sm, pitch, c.nl, c.line0, c.o, c.col0, a, a.post);
@@ -872,16 +906,24 @@ static double2 *fast_tables(int slot, long n, int bc, cd cp, cd c2, int nseg, cu
 
 // Persistent launch of the warp-cooperative kernel: one resident wave of
 // CTAs, each walking the tiles with a stride of the grid.
+template <int SMAX> static void *warp_kernel(bool contig) {
+  return contig ? (void *) k_cn_warp<true, SMAX> : (void *) k_cn_warp<false, SMAX>;
+}
+
 static int launch_cn_warp(void *psi, CnAxis &a, bool contig, int axis, cudaStream_t st) {
   const long pitch = warp_pitch(contig, a.n);
-  const size_t sm = 2 * sizeof(double2) * (size_t) (contig ? (long) kCnWarpLines * pitch : a.n * pitch);
+  const long tl = contig ? tile_lines<true>() : tile_lines<false>();
+  const size_t sm = 2 * sizeof(double2) * (size_t) (contig ? tl * pitch : a.n * pitch);
   long ntiles, tpo = 1;
   if (contig) {
-    ntiles = (a.outer + kCnWarpLines - 1) / kCnWarpLines;
+    ntiles = (a.outer + tl - 1) / tl;
   } else {
-    tpo = (a.inner + kCnWarpLines - 1) / kCnWarpLines;
+    tpo = (a.inner + tl - 1) / tl;
     ntiles = a.outer * tpo;
   }
+  // segment length bound: the register arrays hold ceil(n / 32) <= SMAX points
+  const int smax = a.n <= 64 ? 2 : a.n <= 128 ? 4 : a.n <= 192 ? 6 : 8;
+  const int si = smax / 2 - 1;
   if (ntiles <= 0) return 0;
   // resident CTAs for this (device, kernel, tile size), remembered per kernel
   struct Occ {
@@ -889,15 +931,22 @@ static int launch_cn_warp(void *psi, CnAxis &a, bool contig, int axis, cudaStrea
     size_t sm;
     int rg;
   };
-  static Occ occ[2] = {{-1, 0, 0}, {-1, 0, 0}};
+  static Occ occ[2][4] = {};
+  static bool occ_init = false;
+  if (!occ_init) {
+    for (auto &r : occ)
+      for (auto &e : r) e.dev = -1;
+    occ_init = true;
+  }
   int dev = 0;
   cudaGetDevice(&dev);
-  auto kern = contig ? k_cn_warp<true> : k_cn_warp<false>;
-  Occ &o = occ[contig ? 1 : 0];
+  void *kern = si == 0 ? warp_kernel<2>(contig) : si == 1 ? warp_kernel<4>(contig) : si == 2 ? warp_kernel<6>(contig)
+                                                                                  : warp_kernel<8>(contig);
+  Occ &o = occ[contig ? 1 : 0][si];
   if (o.dev != dev || o.sm != sm) {
     // the attribute covers the largest tile (lines of 32 * kLaneSegMax points)
-    const size_t sm_max = 2 * sizeof(double2) * (size_t) (contig ? (long) kCnWarpLines * contig_row(32 * kLaneSegMax)
-                                                               : 32 * kLaneSegMax * (kCnWarpLines + 1));
+    const size_t sm_max = 2 * sizeof(double2) * (size_t) (contig ? tl * contig_row(32 * kLaneSegMax)
+                                                               : 32 * kLaneSegMax * warp_pitch(false, 0));
     int nsm = 0, per = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm_max);
@@ -911,7 +960,13 @@ static int launch_cn_warp(void *psi, CnAxis &a, bool contig, int axis, cudaStrea
   if (rg < 0) return gb__set_error(1014, "cn: warp kernel does not fit");
   const long grid = ntiles < rg ? ntiles : rg;
   const int slot = gb__pass_begin(15 + axis);
-  kern<<<(unsigned) grid, kCnWarpThreads, sm, st>>>((double2 *) psi, a, ntiles, tpo);
+  void *args[] = {&psi, &a, &ntiles, &tpo};
+  const cudaError_t e = cudaLaunchKernel(kern, dim3((unsigned) grid), dim3(kCnWarpThreads), args, sm, st);
+  if (e != cudaSuccess) {
+    gb__pass_end(slot);
+    gb__count_launch();
+    return gb__set_error((int) e, "cn warp");
+  }
   gb__pass_end(slot);
   GB_CHECK_LAUNCH("cn warp");
   return 0;

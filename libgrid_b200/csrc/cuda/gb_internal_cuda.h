@@ -17,7 +17,8 @@ enum {
   GB_SCR_KIN2 = 6,     // kinetic factor tables of the merged K(dt) pass
   GB_SCR_CHAIN = 7,    // tile counters and ticket of the plane-chained passes
   GB_SCR_UNET = 8,     // per-chunk weight-gradient partials of the U-Net kernels
-  GB_SCR_COUNT = 9
+  GB_SCR_UNETB = 9,    // packed weight operand of the U-Net tensor-core convolutions
+  GB_SCR_COUNT = 10
 };
 
 void *gb__scratch(int slot, size_t bytes);
@@ -64,6 +65,14 @@ template <typename T> int gb__split_step_t(void *psi, const gb_geom *g, const gb
 template <typename T>
 int gb__split_steps_t(void *psi, const gb_geom *g, const gb_kinetic *kin, const gb_potential *pot, int nsteps);
 template <typename T> int gb__ksq_sum_t(const void *psi, void *work, const gb_geom *g, double *out);
+
+// Tensor-core U-Net convolutions (gb_unet_tc.cu): return -1 when the path is
+// off or the shape has no plan (the caller runs the SIMT kernel), else a
+// status.  mode 0: y = conv(x) (+ bias, ReLU); mode 1: y = data gradient of
+// x = gy.
+int gb__unet_conv_tc(const float *x, const uint16_t *w, const float *b, float *y, int cin, int cout, int d, int h,
+                     int wd, int relu, int mode);
+int gb__unet_wgrad_tc(const float *x, const float *gy, float *gw, float *gb, int cin, int cout, int d, int h, int wd);
 
 // Deterministic sum of n partials into out (FP64), on the library stream.
 int gb__sum_partials(const double *partial, long n, double *out_host);

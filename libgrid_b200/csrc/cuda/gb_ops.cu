@@ -536,6 +536,113 @@ extern "C" int gb_reduce(int op, const void *a, const void *b, const gb_geom *g,
 }
 
 // ---------------------------------------------------------------------------
+// Normalisation without a host round trip: the norm is reduced into a device
+// scalar (fixed order, as gb_reduce) and the scale kernel reads it, so a loop
+// of propagation steps and renormalisations never waits for the host.
+
+template <typename T>
+__global__ void k_scale_to_norm(C2<T> *__restrict__ psi, size_t n, const double2 *__restrict__ sum, double target,
+                                double step_factor) {
+  const double nrm = sum->x * step_factor;
+  const T s = (T) (nrm > 0.0 ? sqrt(target / nrm) : 1.0);
+  for (size_t i = blockIdx.x * (size_t) blockDim.x + threadIdx.x; i < n; i += (size_t) gridDim.x * blockDim.x)
+    psi[i] = cscale(psi[i], s);
+}
+
+extern "C" int gb_normalize_device(void *psi, const gb_geom *g, double target, double step_factor) {
+  const long nxy = g->nx * g->ny;
+  const size_t n = (size_t) nxy * g->nz;
+  const int nb = reduce_blocks(n);
+  double2 *partial = (double2 *) gb__scratch(GB_SCR_PARTIAL, sizeof(double2) * (size_t) (nb + 1));
+  double2 *res = (double2 *) gb__scratch(GB_SCR_RESULT, 64);
+  if (!partial || !res) return gb_last_error();
+  cudaStream_t st = gb__stream();
+  if (g->prec == GB_FP32) {
+    launch_reduce<float, float>(GB_RED_NORM2, nb, st, psi, nullptr, nxy, g->nz, g->nz, 0, partial, g->nx, g->ny, g->step);
+    GB_CHECK_LAUNCH("normalize: reduce");
+    k_finish2<<<1, 1024, 0, st>>>(partial, nb, res);
+    GB_CHECK_LAUNCH("normalize: finish");
+    k_scale_to_norm<float><<<blocks_for(n), kThreads, 0, st>>>((float2 *) psi, n, res, target, step_factor);
+  } else {
+    launch_reduce<double, double>(GB_RED_NORM2, nb, st, psi, nullptr, nxy, g->nz, g->nz, 0, partial, g->nx, g->ny,
+                                  g->step);
+    GB_CHECK_LAUNCH("normalize: reduce");
+    k_finish2<<<1, 1024, 0, st>>>(partial, nb, res);
+    GB_CHECK_LAUNCH("normalize: finish");
+    k_scale_to_norm<double><<<blocks_for(n), kThreads, 0, st>>>((double2 *) psi, n, res, target, step_factor);
+  }
+  GB_CHECK_LAUNCH("normalize: scale");
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Thomas-Fermi statistics of a padded real potential for a trial chemical
+// potential mu: sum max(0, mu - V), the number of points with V < mu, and
+// min V (the caller's Newton iteration on the piecewise-linear norm).
+
+__global__ void __launch_bounds__(kThreads) k_tf_stats(const double *__restrict__ v, long nxy, long nz, long vrow,
+                                                       double mu, double *__restrict__ part) {
+  __shared__ double sb[2 * kThreads / 32];
+  __shared__ double sm[kThreads / 32];
+  const size_t n = (size_t) nxy * nz;
+  double s = 0.0, c = 0.0, vmin = 1e300, vs = 0.0;
+  for (size_t g = blockIdx.x * (size_t) blockDim.x + threadIdx.x; g < n; g += (size_t) gridDim.x * blockDim.x) {
+    const size_t ij = g / nz, k = g - ij * nz;
+    const double x = v[ij * vrow + k];
+    if (x < mu) {
+      s += mu - x;
+      c += 1.0;
+    }
+    vmin = fmin(vmin, x);
+    vs += x;
+  }
+  block_sum2<kThreads>(s, c, sb);
+  __syncthreads();
+  double zero = 0.0;
+  block_sum2<kThreads>(vs, zero, sb);
+  for (int o = 16; o > 0; o >>= 1) vmin = fmin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = vmin;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < kThreads / 32; w++) vmin = fmin(vmin, sm[w]);
+    part[4 * blockIdx.x] = s;
+    part[4 * blockIdx.x + 1] = c;
+    part[4 * blockIdx.x + 2] = vmin;
+    part[4 * blockIdx.x + 3] = vs;
+  }
+}
+
+__global__ void k_tf_finish(const double *__restrict__ part, int nb, double *out) {
+  if (threadIdx.x != 0) return;
+  double s = 0.0, c = 0.0, vmin = 1e300, vs = 0.0;
+  for (int b = 0; b < nb; b++) {
+    s += part[4 * b];
+    c += part[4 * b + 1];
+    vmin = fmin(vmin, part[4 * b + 2]);
+    vs += part[4 * b + 3];
+  }
+  out[0] = s;
+  out[1] = c;
+  out[2] = vmin;
+  out[3] = vs;
+}
+
+extern "C" int gb_tf_stats(const void *v, const gb_geom *g, long vrow, double mu, double *out4) {
+  const long nxy = g->nx * g->ny;
+  const size_t n = (size_t) nxy * g->nz;
+  const int nb = reduce_blocks(n);
+  double *part = (double *) gb__scratch(GB_SCR_PARTIAL, sizeof(double) * 4 * (size_t) nb);
+  double *res = (double *) gb__result_slot();
+  if (!part || !res) return gb_last_error();
+  cudaStream_t st = gb__stream();
+  k_tf_stats<<<nb, kThreads, 0, st>>>((const double *) v, nxy, g->nz, vrow, mu, part);
+  GB_CHECK_LAUNCH("tf stats");
+  k_tf_finish<<<1, 32, 0, st>>>(part, nb, res);
+  GB_CHECK_LAUNCH("tf stats finish");
+  return gb__read_result(out4, 4 * sizeof(double));
+}
+
+// ---------------------------------------------------------------------------
 // Allocation-free reduction (gb_reduce_noalloc).
 //
 // Some callers cannot let a library allocate device memory on their behalf:

@@ -340,7 +340,68 @@ __global__ void k_fill(float *__restrict__ p, long n, float v) {
   if (i < n) p[i] = v;
 }
 
+// ---- warm-start inputs and guesses, built on the device
+
+// V = k r^2 / 2 + sum_b a_b exp(-|r - c_b|^2 / w_b^2) on the grid
+// x_i = (i - n/2) step (padded real rows of vrow).
+__global__ void k_unet_potential(double *__restrict__ v, int nx, int ny, int nz, long vrow, double step, double k,
+                                 gb_unet_bumps bm) {
+  const long n = (long) nx * ny * nz;
+  for (long i = (long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long) gridDim.x * blockDim.x) {
+    const int iz = (int) (i % nz), iy = (int) ((i / nz) % ny), ix = (int) (i / ((long) nz * ny));
+    const double x = (ix - nx / 2) * step, y = (iy - ny / 2) * step, z = (iz - nz / 2) * step;
+    double s = 0.5 * k * (x * x + y * y + z * z);
+    for (int b = 0; b < bm.n; b++) {
+      const double dx = x - bm.c[b][0], dy = y - bm.c[b][1], dz = z - bm.c[b][2];
+      s += bm.amp[b] * exp(-(dx * dx + dy * dy + dz * dz) / (bm.w[b] * bm.w[b]));
+    }
+    v[((long) ix * ny + iy) * vrow + iz] = s;
+  }
+}
+
+// Network input [3][n]: tanh((V - vmin) / vscale), the constant gfeat, and
+// the Thomas-Fermi amplitude sqrt(max(mu - V, 0) / g) / amax.
+__global__ void k_unet_features(const double *__restrict__ v, int nx, int ny, int nz, long vrow, double vmin,
+                                double vscale, float gfeat, double mu, double g, double amax, float *__restrict__ out) {
+  const long n = (long) nx * ny * nz;
+  for (long i = (long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long) gridDim.x * blockDim.x) {
+    const long ij = i / nz, k = i - ij * nz;
+    const double x = v[ij * vrow + k];
+    out[i] = (float) tanh((x - vmin) / vscale);
+    out[n + i] = gfeat;
+    out[2 * n + i] = (float) (sqrt(fmax(mu - x, 0.0) / g) / amax);
+  }
+}
+
+// psi = max(amp * scale, 0) + floor (real), into a complex grid
+template <typename T>
+__global__ void k_unet_amplitude(const float *__restrict__ amp, float scale, float floor, C2<T> *__restrict__ psi,
+                                 long n) {
+  for (long i = (long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long) gridDim.x * blockDim.x)
+    psi[i] = C2<T>{(T) (fmaxf(amp[i] * scale, 0.f) + floor), (T) 0};
+}
+
+// out = |psi| * inv_scale (a training target from a complex grid)
+template <typename T>
+__global__ void k_unet_abs(const C2<T> *__restrict__ psi, float inv_scale, float *__restrict__ out, long n) {
+  for (long i = (long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long) gridDim.x * blockDim.x) {
+    const C2<T> v = psi[i];
+    out[i] = (float) sqrt((double) v.x * v.x + (double) v.y * v.y) * inv_scale;
+  }
+}
+
+// a Gaussian exp(-r^2 / width^2) amplitude
+__global__ void k_unet_gaussian(float *__restrict__ out, int nx, int ny, int nz, double step, double width) {
+  const long n = (long) nx * ny * nz;
+  for (long i = (long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long) gridDim.x * blockDim.x) {
+    const int iz = (int) (i % nz), iy = (int) ((i / nz) % ny), ix = (int) (i / ((long) nz * ny));
+    const double x = (ix - nx / 2) * step, y = (iy - ny / 2) * step, z = (iz - nz / 2) * step;
+    out[i] = (float) exp(-(x * x + y * y + z * z) / (width * width));
+  }
+}
+
 inline unsigned blocks_for(long n) { return (unsigned) ((n + kThreads - 1) / kThreads); }
+inline unsigned grid_for(long n) { return (unsigned) std::min<long>((n + kThreads - 1) / kThreads, 148L * 16); }
 
 inline int shape_ok(const char *where, long a, long b, long c, long d) {
   if (a <= 0 || b <= 0 || c <= 0 || d <= 0) return gb__set_error(1101, where);
@@ -352,6 +413,8 @@ inline int shape_ok(const char *where, long a, long b, long c, long d) {
 extern "C" int gb_unet_conv3_fwd(const float *x, const uint16_t *w, const float *b, float *y, int cin, int cout, int d,
                                  int h, int wd, int relu) {
   if (shape_ok("gb_unet_conv3_fwd: bad shape", cin, cout, (long) d * h, wd)) return 1101;
+  const int tc = gb__unet_conv_tc(x, w, b, y, cin, cout, d, h, wd, relu, 0);
+  if (tc >= 0) return tc;
   const size_t smem = (size_t) kCoGroup * cin * 27 * sizeof(float);
   if (smem > kMaxStage) return gb__set_error(1102, "gb_unet_conv3_fwd: too many input channels for the weight stage");
   const long vol = (long) d * h * wd;
@@ -369,6 +432,8 @@ extern "C" int gb_unet_conv3_fwd(const float *x, const uint16_t *w, const float 
 extern "C" int gb_unet_conv3_bwd_data(const float *gy, const uint16_t *w, float *gx, int cin, int cout, int d, int h,
                                       int wd) {
   if (shape_ok("gb_unet_conv3_bwd_data: bad shape", cin, cout, (long) d * h, wd)) return 1101;
+  const int tc = gb__unet_conv_tc(gy, w, nullptr, gx, cin, cout, d, h, wd, 0, 1);
+  if (tc >= 0) return tc;
   const size_t smem = (size_t) kCiGroup * cout * 27 * sizeof(float);
   if (smem > kMaxStage) return gb__set_error(1102, "gb_unet_conv3_bwd_data: too many output channels for the weight stage");
   const long vol = (long) d * h * wd;
@@ -386,6 +451,8 @@ extern "C" int gb_unet_conv3_bwd_data(const float *gy, const uint16_t *w, float 
 extern "C" int gb_unet_conv3_bwd_weight(const float *x, const float *gy, float *gw, float *gb, int cin, int cout, int d,
                                         int h, int wd) {
   if (shape_ok("gb_unet_conv3_bwd_weight: bad shape", cin, cout, (long) d * h, wd)) return 1101;
+  const int tc = gb__unet_wgrad_tc(x, gy, gw, gb, cin, cout, d, h, wd);
+  if (tc >= 0) return tc;
   const long vol = (long) d * h * wd;
   // Voxel chunks of at least 2048 (at most 16 chunks): enough CTAs at 32^3,
   // one chunk (no partials) at 8^3 and below.
@@ -479,5 +546,50 @@ extern "C" int gb_unet_fill(float *p, long n, float v) {
   if (n <= 0) return 0;
   k_fill<<<blocks_for(n), kThreads, 0, gb__stream()>>>(p, n, v);
   GB_CHECK_LAUNCH("gb_unet_fill");
+  return 0;
+}
+
+extern "C" int gb_unet_potential(double *v, int nx, int ny, int nz, long vrow, double step, double k,
+                                 const gb_unet_bumps *bumps) {
+  if (shape_ok("gb_unet_potential: bad shape", nx, ny, nz, vrow) || bumps->n < 0 || bumps->n > GB_UNET_MAX_BUMPS)
+    return gb__set_error(1101, "gb_unet_potential: bad shape or bump count");
+  k_unet_potential<<<grid_for((long) nx * ny * nz), kThreads, 0, gb__stream()>>>(v, nx, ny, nz, vrow, step, k, *bumps);
+  GB_CHECK_LAUNCH("gb_unet_potential");
+  return 0;
+}
+
+extern "C" int gb_unet_features(const double *v, int nx, int ny, int nz, long vrow, double vmin, double vscale,
+                                float gfeat, double mu, double g, double amax, float *out) {
+  if (shape_ok("gb_unet_features: bad shape", nx, ny, nz, vrow)) return 1101;
+  k_unet_features<<<grid_for((long) nx * ny * nz), kThreads, 0, gb__stream()>>>(v, nx, ny, nz, vrow, vmin, vscale, gfeat,
+                                                                                mu, g, amax, out);
+  GB_CHECK_LAUNCH("gb_unet_features");
+  return 0;
+}
+
+extern "C" int gb_unet_amplitude(const float *amp, float scale, float floor, void *psi, long n, int prec) {
+  if (n <= 0) return 0;
+  if (prec == GB_FP32)
+    k_unet_amplitude<float><<<grid_for(n), kThreads, 0, gb__stream()>>>(amp, scale, floor, (float2 *) psi, n);
+  else
+    k_unet_amplitude<double><<<grid_for(n), kThreads, 0, gb__stream()>>>(amp, scale, floor, (double2 *) psi, n);
+  GB_CHECK_LAUNCH("gb_unet_amplitude");
+  return 0;
+}
+
+extern "C" int gb_unet_gaussian(float *out, int nx, int ny, int nz, double step, double width) {
+  if (shape_ok("gb_unet_gaussian: bad shape", nx, ny, nz, 1)) return 1101;
+  k_unet_gaussian<<<grid_for((long) nx * ny * nz), kThreads, 0, gb__stream()>>>(out, nx, ny, nz, step, width);
+  GB_CHECK_LAUNCH("gb_unet_gaussian");
+  return 0;
+}
+
+extern "C" int gb_unet_abs(const void *psi, int prec, long n, float inv_scale, float *out) {
+  if (n <= 0) return 0;
+  if (prec == GB_FP32)
+    k_unet_abs<float><<<grid_for(n), kThreads, 0, gb__stream()>>>((const float2 *) psi, inv_scale, out, n);
+  else
+    k_unet_abs<double><<<grid_for(n), kThreads, 0, gb__stream()>>>((const double2 *) psi, inv_scale, out, n);
+  GB_CHECK_LAUNCH("gb_unet_abs");
   return 0;
 }

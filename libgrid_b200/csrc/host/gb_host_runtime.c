@@ -348,3 +348,13 @@ void gb_grid_sync_host(void *host_mem) {
 void gb_grid_host_modified(void *host_mem) {
   if (gbh_find(host_mem)) gbh_host_modified(host_mem);
 }
+
+/* FP64 device copy of a grid for device-side producers and consumers:
+ * mode 0 read (uploaded if stale), 1 write (the caller overwrites every
+ * value; the device copy becomes authoritative), 2 read and write. */
+void *gb_grid_device(void *host_mem, int mode) {
+  if (!gbh_find(host_mem)) return NULL;
+  if (mode == 1) return gbh_dev_write(host_mem, GB_FP64);
+  if (mode == 2) return gbh_dev_rw(host_mem, GB_FP64);
+  return gbh_dev_read(host_mem, GB_FP64);
+}

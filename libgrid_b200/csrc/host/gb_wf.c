@@ -786,3 +786,29 @@ void grid_wf_propagate_gp_n(wf *gwf, rgrid *vext, REAL g, REAL complex time, INT
   }
   for (INT s = 0; s < nsteps; s++) grid_wf_propagate_gp(gwf, vext, g, time);
 }
+
+/* Imaginary-time relaxation steps (no reference counterpart as one call; the
+ * reference's callers compose grid_wf_propagate(-i dt) and grid_wf_normalize,
+ * src/grid_wf.c:379-556, 681-700): nsteps of grid_wf_propagate_gp(time), each
+ * followed by renormalisation to gwf->norm, with the norm reduced and applied
+ * on the device, so the whole loop runs without a host synchronisation. */
+void grid_wf_relax_gp_n(wf *gwf, rgrid *vext, REAL g, REAL complex time, INT nsteps) {
+  cgrid *grid = gwf->grid;
+  for (INT s = 0; s < nsteps; s++) {
+    grid_wf_propagate_gp(gwf, vext, g, time);
+    const int p = psi_prec(gwf);
+    gb_geom geo = wf_geom(gwf);
+    gbh_check(gb_normalize_device(gbh_dev_rw(grid->value, p), &geo, gwf->norm,
+                                  gbh_step_factor(grid->nx, grid->ny, grid->nz, grid->step)),
+              "grid_wf_relax_gp_n");
+  }
+}
+
+/* psi = max(amp * scale, 0) + floor (real) from a device float array of
+ * nx ny nz values, e.g. a network's guess (no reference counterpart). */
+void grid_wf_set_amplitude_device(wf *gwf, const float *amp, REAL scale, REAL floor) {
+  cgrid *grid = gwf->grid;
+  const int p = psi_prec(gwf);
+  gbh_check(gb_unet_amplitude(amp, (float) scale, (float) floor, gbh_dev_write(grid->value, p), (long) npts(grid), p),
+            "grid_wf_set_amplitude_device");
+}

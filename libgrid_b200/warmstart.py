@@ -281,24 +281,35 @@ class DeviceUNet:
 # --------------------------------------------------------------- physics
 
 
-def sample_problem(seed: int, n: int = 32, step: float = 0.1):
-    """(V, g, k) of one seeded potential of the family above."""
+def problem_params(seed: int):
+    """(k, g, bumps) of one seeded potential of the family above; bumps is a
+    list of (amplitude, width, centre[3])."""
     rng = np.random.default_rng(seed)
     k = rng.uniform(0.005, 0.02)
     g = rng.uniform(0.001, 0.01)
-    x, y, z = workloads.mesh(n, n, n, step)
-    v = 0.5 * k * (x * x + y * y + z * z)
+    bumps = []
     for _ in range(int(rng.integers(1, 7))):
         amp = rng.uniform(0.5e-3, 2e-3) * (1 if rng.random() < 0.5 else -1)
         w = rng.uniform(0.2, 0.6)
         c = rng.uniform(-0.8, 0.8, 3)
+        bumps.append((amp, w, c))
+    return k, g, bumps
+
+
+def sample_problem(seed: int, n: int = 32, step: float = 0.1):
+    """(V, g, k) of one seeded potential on the host (the definition the
+    device potential kernel follows)."""
+    k, g, bumps = problem_params(seed)
+    x, y, z = workloads.mesh(n, n, n, step)
+    v = 0.5 * k * (x * x + y * y + z * z)
+    for amp, w, c in bumps:
         v += amp * np.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) / w**2)
     return v, g, k
 
 
-def thomas_fermi(v, g, step):
-    """Normalised Thomas-Fermi amplitude sqrt(max(mu - V, 0) / g).  The norm
-    sum_{V_i < mu} (mu - V_i) dv / g is piecewise linear in mu: with the
+def thomas_fermi_mu(v, g, step):
+    """Chemical potential of the normalised Thomas-Fermi profile: the norm
+    sum_{V_i < mu} (mu - V_i) dv / g is piecewise linear in mu; with the
     potential sorted, the k lowest points give mu_k = (g / dv + S_k) / k, and
     mu is the first mu_k that does not pass the next potential value."""
     dv = step**3
@@ -306,13 +317,18 @@ def thomas_fermi(v, g, step):
     k = np.arange(1, vs.size + 1)
     mus = (g / dv + np.cumsum(vs)) / k
     nxt = np.append(vs[1:], np.inf)
-    mu = mus[int(np.argmax(mus <= nxt))]
-    return np.sqrt(np.maximum(mu - v, 0) / g)
+    return float(mus[int(np.argmax(mus <= nxt))])
+
+
+def thomas_fermi(v, g, step):
+    """Normalised Thomas-Fermi amplitude sqrt(max(mu - V, 0) / g)."""
+    return np.sqrt(np.maximum(thomas_fermi_mu(v, g, step) - v, 0) / g)
 
 
 def features(v, g, step):
     """Network input [3, n, n, n] and the amplitude scale s (targets and
-    predictions are amplitudes / s)."""
+    predictions are amplitudes / s) on the host (the definition the device
+    features kernel follows)."""
     tf = thomas_fermi(v, g, step)
     s = float(tf.max())
     x = np.stack([np.tanh((v - v.min()) / 0.01), np.full_like(v, g / 0.01), tf / s]).astype(np.float32)
@@ -324,143 +340,268 @@ def gaussian_guess(n, step, width=1.0):
     return np.exp(-(x * x + y * y + z * z) / width**2)
 
 
+class Bumps(C.Structure):
+    _fields_ = [("n", C.c_int), ("amp", C.c_double * 8), ("w", C.c_double * 8), ("c", (C.c_double * 3) * 8)]
+
+
+def _bind_device(lib):
+    V, I, L, D, F = C.c_void_p, C.c_int, C.c_long, C.c_double, C.c_float
+    sig = {
+        "gb_unet_potential": (I, [V, I, I, I, L, D, D, C.POINTER(Bumps)]),
+        "gb_unet_features": (I, [V, I, I, I, L, D, D, F, D, D, D, V]),
+        "gb_unet_gaussian": (I, [V, I, I, I, D, D]),
+        "gb_unet_abs": (I, [V, I, L, F, V]),
+        "gb_tf_stats": (I, [V, V, L, D, C.POINTER(D)]),
+        "gb_grid_device": (V, [V, I]),
+        "grid_wf_set_amplitude_device": (None, [V, V, D, D]),
+        "grid_wf_relax_gp_n": (None, [V, V, D, capi.Complex, L]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+class Geom(C.Structure):
+    _fields_ = [("nx", C.c_long), ("ny", C.c_long), ("nz", C.c_long), ("step", C.c_double), ("prec", C.c_int)]
+
+
 class Relaxer:
     """The plain imaginary-time loop on the device through the libgrid API:
-    grid_wf_propagate_gp(-i dt) -> grid_wf_normalize every step, the GP
-    energy every M steps."""
+    grid_wf_propagate_gp(-i dt) and a renormalisation every step
+    (grid_wf_relax_gp_n: the norm is reduced and applied on the device), the
+    GP energy E = T (FFT) + <V> + g/2 int |psi|^4 every M steps.  The
+    potential, the Thomas-Fermi features and every initial guess are built on
+    the device too, so a relaxation moves no 3-D array across PCIe."""
 
     def __init__(self, api, n: int, step: float, mass: float = 4.0 / AMU):
         self.api, self.lib, self.n, self.step = api, api.lib, n, step
         _bind(self.lib)
+        _bind_device(self.lib)
         self.lib.grid_wf_analyze_method(b"\x01")
         self.w = api.wf(n, n, n, step, mass, capi.WF_PERIODIC_BOUNDARY, capi.WF_2ND_ORDER_FFT)
         self.vx = api.rgrid(n, n, n, step)
         self.rho = api.rgrid(n, n, n, step)
         self.rho2 = api.rgrid(n, n, n, step)
+        self.vol = n**3
+        self.work = self.lib.gb_device_alloc(4 * self.vol)
+        self.feat = self.lib.gb_device_alloc(4 * 3 * self.vol)
+        if not self.work or not self.feat:
+            raise MemoryError("gb_device_alloc failed")
+        self.g = 0.0
 
     def free(self):
         for o in (self.w, self.vx, self.rho, self.rho2):
             self.api.free(o)
+        self.lib.gb_device_free(self.work)
+        self.lib.gb_device_free(self.feat)
 
-    def energy(self, g):
-        lib = self.lib
+    def _vdev(self, mode=0):
+        return self.lib.gb_grid_device(C.c_void_p(self.vx.s.value), mode)
+
+    def set_problem(self, seed):
+        """The seeded potential on the device; returns g."""
+        k, g, bumps = problem_params(seed)
+        b = Bumps()
+        b.n = len(bumps)
+        for i, (amp, w, c) in enumerate(bumps):
+            b.amp[i], b.w[i] = amp, w
+            for j in range(3):
+                b.c[i][j] = c[j]
+        n = self.n
+        _ok(self.lib.gb_unet_potential(self._vdev(1), n, n, n, self.vx.s.nz2, self.step, k, C.byref(b)), "potential")
+        self.g = g
+        return g
+
+    def tf_features(self, out=None):
+        """Thomas-Fermi chemical potential by Newton's method on the device
+        sums (sum max(0, mu - V) is convex and piecewise linear in mu, so
+        Newton from above ends on the exact root), then the network input
+        [3][n^3] into `out` (default: the relaxer's own buffer).  Returns
+        (out, amplitude scale s)."""
+        lib, n, g = self.lib, self.n, self.g
+        geo = Geom(n, n, n, self.step, 0)
+        st = (C.c_double * 4)()
+        vd = self._vdev(0)
+        target = g / self.step**3
+        _ok(lib.gb_tf_stats(vd, C.byref(geo), self.vx.s.nz2, -1e300, st), "tf stats")
+        vmin, vsum = st[2], st[3]
+        mu = (target + vsum) / self.vol  # at or above the root
+        for _ in range(64):
+            _ok(lib.gb_tf_stats(vd, C.byref(geo), self.vx.s.nz2, mu, st), "tf stats")
+            f, cnt = st[0], st[1]
+            if cnt <= 0:
+                break
+            nmu = mu - (f - target) / cnt
+            if not (nmu < mu) or abs(f - target) <= 1e-13 * target:
+                break
+            mu = nmu
+        s = math.sqrt(max(mu - vmin, 0.0) / g)
+        out = self.feat if out is None else out
+        _ok(lib.gb_unet_features(vd, n, n, n, self.vx.s.nz2, vmin, 0.01, g / 0.01, mu, g, s, out), "features")
+        return out, s
+
+    def set_guess(self, amp_dev, scale, floor=0.0):
+        self.lib.grid_wf_set_amplitude_device(self.w.ptr, amp_dev, scale, floor)
+        self.w.normalize()
+
+    def gaussian(self, width=1.0):
+        n = self.n
+        _ok(self.lib.gb_unet_gaussian(self.work, n, n, n, self.step, width), "gaussian")
+        self.set_guess(self.work, 1.0)
+
+    def energy(self):
+        lib, g = self.lib, self.g
         e = self.w.energy(self.vx)
         lib.grid_wf_density(self.w.ptr, self.rho.ptr)
         lib.rgrid_product(C.cast(self.rho2.ptr, C.c_void_p), C.cast(self.rho.ptr, C.c_void_p),
                           C.cast(self.rho.ptr, C.c_void_p))
         return e + 0.5 * g * lib.rgrid_integral(self.rho2.ptr)
 
-    def relax(self, v, g, psi0, dt=2.0, m=10, tol=1e-8, max_steps=20000):
-        """Returns (psi, E, steps, seconds); seconds covers the loop only."""
-        self.vx.set(v)
-        self.w.grid.set(psi0.astype(np.complex128))
-        self.w.normalize()
-        t0 = time.perf_counter()
-        e_prev = self.energy(g)
+    def relax(self, dt=2.0, m=10, tol=1e-8, max_steps=50000):
+        """From the guess in place: returns (E, steps)."""
+        e_prev = self.energy()
         steps = 0
         while steps < max_steps:
-            for _ in range(m):
-                self.w.propagate_gp(self.vx, g, complex(0.0, -dt))
-                self.w.normalize()
+            self.lib.grid_wf_relax_gp_n(self.w.ptr, self.vx.ptr, self.g, capi.Complex.of(complex(0.0, -dt)), m)
             steps += m
-            e = self.energy(g)
+            e = self.energy()
             if abs(e - e_prev) < tol:
                 break
             e_prev = e
-        secs = time.perf_counter() - t0
-        return self.w.grid.get(), e, steps, secs
+        return e, steps
+
+    def target(self, out, s):
+        """|psi| / s of the relaxed state into a device float array."""
+        _ok(self.lib.gb_unet_abs(self.lib.gb_grid_device(C.c_void_p(self.w.s.grid.contents.value), 0), 0, self.vol,
+                                 1.0 / s, out), "abs")
 
 
-def make_dataset(api, seeds, n=32, step=0.1, **kw):
-    """Ground states of the seeded potentials from a Gaussian start."""
+class DeviceSet:
+    """Inputs [N][3][n^3] and targets [N][n^3] of a training set, resident on
+    the device."""
+
+    def __init__(self, lib, count, vol):
+        self.lib, self.count, self.vol = lib, count, vol
+        self.x = lib.gb_device_alloc(4 * 3 * vol * count)
+        self.y = lib.gb_device_alloc(4 * vol * count)
+        if not self.x or not self.y:
+            raise MemoryError("training set does not fit the device")
+
+    def xp(self, i):
+        return self.x + 4 * 3 * self.vol * int(i)
+
+    def yp(self, i):
+        return self.y + 4 * self.vol * int(i)
+
+    def free(self):
+        self.lib.gb_device_free(self.x)
+        self.lib.gb_device_free(self.y)
+
+
+def make_dataset(api, seeds, n=32, step=0.1, tol=1e-9):
+    """Ground states of the seeded potentials, relaxed by the plain
+    imaginary-time loop from the Thomas-Fermi profile; features and targets
+    stay on the device.  Returns (DeviceSet, meta)."""
+    seeds = list(seeds)
     r = Relaxer(api, n, step)
-    xs, ys, meta = [], [], []
+    ds = DeviceSet(r.lib, len(seeds), n**3)
+    meta = []
     try:
-        for sd in seeds:
-            v, g, _ = sample_problem(sd, n, step)
-            psi, e, steps, secs = r.relax(v, g, gaussian_guess(n, step), **kw)
-            x, s = features(v, g, step)
-            xs.append(x)
-            ys.append((np.abs(psi) / s).astype(np.float32))
-            meta.append(dict(seed=sd, g=g, energy=e, steps=steps, seconds=secs, scale=s))
+        for i, sd in enumerate(seeds):
+            g = r.set_problem(sd)
+            _, s = r.tf_features(ds.xp(i))
+            r.set_guess(ds.xp(i) + 4 * 2 * r.vol, s)
+            e, steps = r.relax(tol=tol)
+            r.target(ds.yp(i), s)
+            meta.append(dict(seed=sd, g=g, energy=e, steps=steps, scale=s))
+        _ok(r.lib.gb_synchronize(), "sync")
     finally:
         r.free()
-    return np.stack(xs), np.stack(ys), meta
+    return ds, meta
 
 
-def train(net: DeviceUNet, xs, ys, epochs=60, batch=8, lr=2e-3, seed=0, log=None):
-    """Adam over minibatches of samples; inputs and targets live on the
-    device for the whole run.  Returns the mean loss of the last epoch."""
-    lib = net.lib
-    nb, vol = xs.shape[0], net.vol[0]
-    dx = net._alloc(xs.nbytes)
-    dy = net._alloc(ys.nbytes)
-    try:
-        _ok(lib.gb_h2d(dx, np.ascontiguousarray(xs).ctypes.data, xs.nbytes), "h2d")
-        _ok(lib.gb_h2d(dy, np.ascontiguousarray(ys).ctypes.data, ys.nbytes), "h2d")
-        rng = np.random.default_rng(seed)
-        xbytes = xs[0].nbytes
-        last = float("nan")
-        for ep in range(epochs):
-            order = rng.permutation(nb)
-            for b0 in range(0, nb, batch):
-                idx = order[b0 : b0 + batch]
-                for i in idx:
-                    net.set_input_device(dx + int(i) * xbytes)
-                    net.forward()
-                    net.loss_grad(dy + int(i) * 4 * vol, 2.0 / (vol * len(idx)))
-                    net.backward()
-                net.adam(lr * (0.5 * (1 + math.cos(math.pi * ep / epochs)) * 0.95 + 0.05))
-            if log is not None or ep == epochs - 1:
-                errs = []
-                for i in range(min(nb, 8)):
-                    net.set_input_device(dx + i * xbytes)
-                    net.forward()
-                    errs.append(float(((net.activation("out")[0] - ys[i]) ** 2).mean()))
-                last = float(np.mean(errs))
-                if log is not None:
-                    log(ep, last)
-    finally:
-        lib.gb_device_free(dx)
-        lib.gb_device_free(dy)
+def host_dataset(api, xs, ys):
+    """A DeviceSet from host arrays (tests)."""
+    ds = DeviceSet(api.lib, xs.shape[0], int(np.prod(ys.shape[1:])))
+    _ok(api.lib.gb_h2d(ds.x, np.ascontiguousarray(xs, np.float32).ctypes.data, xs.nbytes), "h2d")
+    _ok(api.lib.gb_h2d(ds.y, np.ascontiguousarray(ys, np.float32).ctypes.data, ys.nbytes), "h2d")
+    return ds
+
+
+def train(net: DeviceUNet, ds: DeviceSet, epochs=60, batch=8, lr=2e-3, seed=0, log=None, monitor=8):
+    """Adam over minibatches of samples of a device-resident set.  Returns
+    the mean squared error on the first `monitor` samples after the last
+    epoch."""
+    nb, vol = ds.count, net.vol[0]
+    rng = np.random.default_rng(seed)
+    last = float("nan")
+    for ep in range(epochs):
+        order = rng.permutation(nb)
+        for b0 in range(0, nb, batch):
+            idx = order[b0 : b0 + batch]
+            for i in idx:
+                net.set_input_device(ds.xp(i))
+                net.forward()
+                net.loss_grad(ds.yp(i), 2.0 / (vol * len(idx)))
+                net.backward()
+            net.adam(lr * (0.5 * (1 + math.cos(math.pi * ep / epochs)) * 0.95 + 0.05))
+        if log is not None or ep == epochs - 1:
+            errs = []
+            for i in range(min(nb, monitor)):
+                net.set_input_device(ds.xp(i))
+                net.forward()
+                y = np.empty(vol, np.float32)
+                _ok(net.lib.gb_d2h(y.ctypes.data, ds.yp(i), y.nbytes), "d2h")
+                errs.append(float(((net.activation("out")[0].ravel() - y) ** 2).mean()))
+            last = float(np.mean(errs))
+            if log is not None:
+                log(ep, last)
     return last
 
 
-def evaluate(api, net: DeviceUNet, seeds, n=32, step=0.1):
+def evaluate(api, net: DeviceUNet, seeds, n=32, step=0.1, tol=1e-9, ref_tol=1e-12):
     """Per held-out potential: steps and seconds to convergence from the
-    Gaussian guess, from the Thomas-Fermi profile and from the network guess
-    (each including the host time to build its guess; for the network that is
-    the features and the inference), and the energy differences."""
+    Gaussian guess, from the Thomas-Fermi profile and from the network guess.
+    Each start's seconds run from the potential on the device to the
+    converged state and include building its guess (for the network: the
+    Thomas-Fermi features and the inference).  The converged energies are
+    compared with each other and with a reference relaxed to ref_tol."""
     r = Relaxer(api, n, step)
+    lib = r.lib
     rows = []
     try:
         for sd in seeds:
-            v, g, _ = sample_problem(sd, n, step)
-            # each start is charged the time to prepare its guess on the host
+            r.set_problem(sd)
+            _ok(lib.gb_synchronize(), "sync")
             t0 = time.perf_counter()
-            guess = gaussian_guess(n, step)
-            t_g0 = time.perf_counter() - t0
-            _, e_g, st_g, t_g = r.relax(v, g, guess)
+            r.gaussian()
+            e_g, st_g = r.relax(tol=tol)
+            _ok(lib.gb_synchronize(), "sync")
+            t_g = time.perf_counter() - t0
             t0 = time.perf_counter()
-            x, s = features(v, g, step)
-            guess = x[2] * s
-            t_tf0 = time.perf_counter() - t0
-            _, e_tf, st_tf, t_tf = r.relax(v, g, guess)
+            _, s = r.tf_features()
+            r.set_guess(r.feat + 4 * 2 * r.vol, s)
+            e_tf, st_tf = r.relax(tol=tol)
+            _ok(lib.gb_synchronize(), "sync")
+            t_tf = time.perf_counter() - t0
             t0 = time.perf_counter()
-            x, s = features(v, g, step)
-            amp = np.maximum(net.predict(x), 0.0) * s + 1e-6
-            t_inf = time.perf_counter() - t0
-            _, e_n, st_n, t_n = r.relax(v, g, amp)
-            t_g += t_g0
-            t_tf += t_tf0
+            _, s = r.tf_features(net._act("in"))
+            net.forward()
+            r.set_guess(net._act("out"), s, 1e-6)
+            e_n, st_n = r.relax(tol=tol)
+            _ok(lib.gb_synchronize(), "sync")
+            t_n = time.perf_counter() - t0
+            e_ref, st_ref = r.relax(tol=ref_tol)  # continue to a tighter limit
             rows.append(dict(seed=sd, steps_gauss=st_g, sec_gauss=t_g, steps_tf=st_tf, sec_tf=t_tf, steps_net=st_n,
-                             sec_net=t_n + t_inf, e_gauss=e_g, e_net=e_n, de=abs(e_n - e_g)))
+                             sec_net=t_n, e_gauss=e_g, e_net=e_n, e_ref=e_ref, de=abs(e_n - e_g),
+                             de_net_ref=abs(e_n - e_ref), de_gauss_ref=abs(e_g - e_ref)))
     finally:
         r.free()
     return rows
 
 
-def time_training_step(net: DeviceUNet, x, y, reps: int = 20):
+def time_training_step(net: DeviceUNet, ds: DeviceSet, reps: int = 10):
     """(forward ms, forward + loss + backward ms) per sample, CUDA events on
     the library stream, after 3 warm-up repetitions."""
     lib = net.lib
@@ -468,8 +609,7 @@ def time_training_step(net: DeviceUNet, x, y, reps: int = 20):
     lib.gb_event_record.argtypes = [C.c_int]
     lib.gb_event_elapsed_ms.restype = C.c_float
     lib.gb_event_elapsed_ms.argtypes = [C.c_int, C.c_int]
-    net.set_input(x)
-    tgt = net.set_target(y)
+    net.set_input_device(ds.xp(0))
     out = []
     for with_bwd in (False, True):
         for r in range(reps + 3):
@@ -477,7 +617,7 @@ def time_training_step(net: DeviceUNet, x, y, reps: int = 20):
                 _ok(lib.gb_event_record(0), "event")
             net.forward()
             if with_bwd:
-                net.loss_grad(tgt)
+                net.loss_grad(ds.yp(0))
                 net.backward()
         _ok(lib.gb_event_record(1), "event")
         _ok(lib.gb_synchronize(), "sync")
@@ -487,8 +627,9 @@ def time_training_step(net: DeviceUNet, x, y, reps: int = 20):
 
 
 def main(argv=None):
-    """python -m libgrid_b200.warmstart [--train N] [--test N] [--epochs E]
-    [--out report.json]: generate, train, evaluate and print one JSON report."""
+    """python -m libgrid_b200.warmstart [--n N] [--step H] [--train N] [--test N]
+    [--epochs E] [--out report.json]: generate, train, evaluate and print one
+    JSON report."""
     import argparse
     import json
 
@@ -498,34 +639,42 @@ def main(argv=None):
     ap.add_argument("--train", type=int, default=128)
     ap.add_argument("--test", type=int, default=16)
     ap.add_argument("--epochs", type=int, default=100)
+    ap.add_argument("--batch", type=int, default=8)
+    ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--n", type=int, default=32)
     ap.add_argument("--step", type=float, default=0.1)
+    ap.add_argument("--tol", type=float, default=1e-9)
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     api = libgrid_b200.load()
     api.lib.cuda_enable(b"\x01", 0, None)
     t0 = time.perf_counter()
-    xs, ys, meta = make_dataset(api, range(1000, 1000 + a.train), a.n, a.step)
+    ds, meta = make_dataset(api, range(1000, 1000 + a.train), a.n, a.step, tol=a.tol)
     t_data = time.perf_counter() - t0
     net = DeviceUNet(api, a.n, cin=3, seed=0)
     try:
         t0 = time.perf_counter()
-        loss = train(net, xs, ys, epochs=a.epochs, batch=8, lr=2e-3)
+        loss = train(net, ds, epochs=a.epochs, batch=a.batch, lr=a.lr)
+        api.lib.gb_synchronize()
         t_train = time.perf_counter() - t0
-        step_ms = time_training_step(net, xs[0], ys[0])
-        rows = evaluate(api, net, range(5000, 5000 + a.test), a.n, a.step)
+        step_ms = time_training_step(net, ds)
+        ds.free()
+        rows = evaluate(api, net, range(5000, 5000 + a.test), a.n, a.step, tol=a.tol)
     finally:
         net.free()
     mean = lambda k: float(np.mean([r[k] for r in rows]))
     rep = dict(
-        workload="learned warm start, GP imaginary time %d^3 step %.2f, %d training / %d held-out potentials"
+        workload="learned warm start, GP imaginary time %d^3 step %.3f bohr, %d training / %d held-out potentials"
         % (a.n, a.step, a.train, a.test),
-        params=int(net.nparam), epochs=a.epochs, train_loss=loss, target_ms=float((ys**2).mean()),
-        data_seconds=t_data, train_seconds=t_train, forward_ms=step_ms[0], forward_backward_ms=step_ms[1],
+        stopping="|E_n - E_(n-10)| < %.0e Ha (converged energies agree to 1e-8 Ha)" % a.tol,
+        params=int(net.nparam), epochs=a.epochs, train_loss=loss, data_seconds=t_data, train_seconds=t_train,
+        forward_ms=step_ms[0], forward_backward_ms=step_ms[1],
+        data_steps_mean=float(np.mean([m["steps"] for m in meta])),
         steps_gauss=mean("steps_gauss"), steps_tf=mean("steps_tf"), steps_net=mean("steps_net"),
         sec_gauss=mean("sec_gauss"), sec_tf=mean("sec_tf"), sec_net=mean("sec_net"),
         step_ratio=mean("steps_gauss") / mean("steps_net"), time_ratio=mean("sec_gauss") / mean("sec_net"),
-        max_de=float(max(r["de"] for r in rows)), rows=rows,
+        max_de=float(max(r["de"] for r in rows)), max_de_net_ref=float(max(r["de_net_ref"] for r in rows)),
+        max_de_gauss_ref=float(max(r["de_gauss_ref"] for r in rows)), rows=rows,
     )
     line = json.dumps(rep)
     if a.out:

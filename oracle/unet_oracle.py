@@ -1,7 +1,11 @@
 """CPU oracle (test infrastructure only) for the U-Net warm-start kernels.
 
 Plain numpy, float64 accumulation, bf16 weights rounded to nearest even as the
-device kernels round them.  The reference has no learned part, so nothing
+device kernels round them.  With tc=True the convolution operands are also
+rounded to bf16 (activations in the forward and data-gradient convolutions,
+activations and output gradients in the weight gradient), as the library's
+tensor-core convolutions do; with tc=False they stay as given (the SIMT
+kernels: FP32 activations).  The reference has no learned part, so nothing
 here follows a reference file: these are the textbook definitions of a 3x3x3
 zero-padded convolution, its two gradients, 2x2x2 average pooling and
 nearest-neighbour upsampling.  Layouts match the device kernels: activations
@@ -35,9 +39,13 @@ def _shift(x, dz, dy, dx):
     return p[..., 1 + dz : 1 + dz + d, 1 + dy : 1 + dy + h, 1 + dx : 1 + dx + w]
 
 
-def conv3_fwd(x, w, b, relu):
+def _op(a, tc):
+    return bf16_round(a) if tc else np.asarray(a, np.float64)
+
+
+def conv3_fwd(x, w, b, relu, tc=False):
     """y[co] = sum_ci sum_t x[ci](p + off t) w[co, ci, t] + b[co]."""
-    x = np.asarray(x, np.float64)
+    x = _op(x, tc)
     y = np.zeros((w.shape[0],) + x.shape[1:])
     for t, (dz, dy, dx) in enumerate(TAPS):
         y += np.tensordot(w[:, :, t], _shift(x, dz, dy, dx), axes=(1, 0))
@@ -45,21 +53,23 @@ def conv3_fwd(x, w, b, relu):
     return np.maximum(y, 0.0) if relu else y
 
 
-def conv3_bwd_data(gy, w):
-    gy = np.asarray(gy, np.float64)
+def conv3_bwd_data(gy, w, tc=False):
+    gy = _op(gy, tc)
     gx = np.zeros((w.shape[1],) + gy.shape[1:])
     for t, (dz, dy, dx) in enumerate(TAPS):
         gx += np.tensordot(w[:, :, t].T, _shift(gy, -dz, -dy, -dx), axes=(1, 0))
     return gx
 
 
-def conv3_bwd_weight(x, gy):
-    x = np.asarray(x, np.float64)
-    gy = np.asarray(gy, np.float64)
+def conv3_bwd_weight(x, gy, tc=False):
+    """Weight and bias gradients; the bias gradient sums the unrounded gy."""
+    gsum = np.asarray(gy, np.float64).sum(axis=(1, 2, 3))
+    x = _op(x, tc)
+    gy = _op(gy, tc)
     gw = np.zeros((gy.shape[0], x.shape[0], 27))
     for t, (dz, dy, dx) in enumerate(TAPS):
         gw[:, :, t] = np.tensordot(gy, _shift(x, dz, dy, dx), axes=([1, 2, 3], [1, 2, 3]))
-    return gw, gy.sum(axis=(1, 2, 3))
+    return gw, gsum
 
 
 def pool2_fwd(x):
@@ -80,7 +90,7 @@ def up2_bwd(gy):
     return np.asarray(gy, np.float64).reshape(c, d // 2, 2, h // 2, 2, w // 2, 2).sum(axis=(2, 4, 6))
 
 
-def unet_forward(spec, params, x):
+def unet_forward(spec, params, x, tc=False):
     """Whole network on the CPU.  spec: list of ops as built by
     libgrid_b200.warmstart.unet_spec; params: {layer: (w float64 [co,ci,27]
     already bf16-rounded, b)}.  Returns (prediction, activations)."""
@@ -90,7 +100,7 @@ def unet_forward(spec, params, x):
         src = np.concatenate([acts[n] for n in op[1]], axis=0)
         if kind == "conv":
             w, b = params[op[3]]
-            acts[op[2]] = conv3_fwd(src, w, b, op[4])
+            acts[op[2]] = conv3_fwd(src, w, b, op[4], tc)
         elif kind == "pool":
             acts[op[2]] = pool2_fwd(src)
         elif kind == "up":
@@ -98,10 +108,10 @@ def unet_forward(spec, params, x):
     return acts[spec[-1][2]], acts
 
 
-def unet_loss_grads(spec, params, x, tgt):
+def unet_loss_grads(spec, params, x, tgt, tc=False):
     """Loss = sum (pred - tgt)^2 / n and its gradients for every layer, by
     reverse-mode through the same ops (float64)."""
-    pred, acts = unet_forward(spec, params, x)
+    pred, acts = unet_forward(spec, params, x, tc)
     n = pred.size
     loss = float(((pred - tgt) ** 2).sum() / n)
     grads = {k: np.zeros_like(v) for k, v in acts.items()}
@@ -115,9 +125,9 @@ def unet_loss_grads(spec, params, x, tgt):
             if op[4]:
                 g = g * (acts[out] > 0)
             w, _ = params[op[3]]
-            gw, gb = conv3_bwd_weight(src, g)
+            gw, gb = conv3_bwd_weight(src, g, tc)
             pgrads[op[3]] = (gw, gb)
-            gsrc = conv3_bwd_data(g, w)
+            gsrc = conv3_bwd_data(g, w, tc)
         elif kind == "pool":
             gsrc = pool2_bwd(g)
         else:
