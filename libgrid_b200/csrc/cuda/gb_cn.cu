@@ -398,17 +398,21 @@ __device__ __forceinline__ double2 shfl_down2(double2 v, int d) {
 
 // Solve line l of the tile in place (the whole warp); SMAX >= ceil(n / 32).
 template <bool CONTIG, int SMAX>
-__device__ __forceinline__ void cn_warp_line(double2 *sm, long pitch, int l, const CnAxis &a, int lane) {
-  const long n = a.n;
-  const int S = (int) ((n + 31) >> 5);
+__device__ __forceinline__ void cn_warp_line(double2 *sm, int pitch, int l, const CnAxis &a, int lane) {
+  const int n = (int) a.n;
+  const int S = (n + 31) >> 5;
   const int bc = a.boundary;
   const double2 zero = make_double2(0.0, 0.0);
   const double2 *tm = a.tab, *trb = a.tab + n, *tz = a.tab + 2 * n, *tH = a.tab + 3 * n, *tQ = a.tab + 4 * n,
                 *tG = a.tab + 5 * n;
   const double2 *wf = a.tab + warp_scan_off(n), *wb = wf + 5 * 32;
-  auto at = [&](long i) -> double2 & { return CONTIG ? sm[(long) l * pitch + i] : sm[i * pitch + l]; };
-  const long a0 = (long) lane * S;
-  const int cnt = (int) (a0 >= n ? 0 : (n - a0 < S ? n - a0 : S));
+  // element i of the line: contiguous tiles hold lines as rows, strided
+  // tiles hold them as columns
+  double2 *const base = CONTIG ? sm + l * pitch : sm + l;
+  const int es = CONTIG ? 1 : pitch;
+  auto at = [&](int i) -> double2 & { return base[i * es]; };
+  const int a0 = lane * S;
+  const int cnt = a0 >= n ? 0 : (n - a0 < S ? n - a0 : S);
   double2 p[SMAX];
 #pragma unroll
   for (int j = 0; j < SMAX; j++) p[j] = (j < cnt) ? at(a0 + j) : zero;
@@ -425,7 +429,7 @@ __device__ __forceinline__ void cn_warp_line(double2 *sm, long pitch, int l, con
 #pragma unroll
   for (int j = 0; j < SMAX; j++) {
     if (j < cnt) {
-      const long i = a0 + j;
+      const int i = a0 + j;
       const double2 p0 = p[j];
       const double2 pp = (j + 1 < cnt) ? p[j + 1] : p_after;
       const double2 b = cn_rhs(i, n, bc, a.cp, a.c2, zero, pm, p0, pp, pfirst, plast);
@@ -448,7 +452,7 @@ __device__ __forceinline__ void cn_warp_line(double2 *sm, long pitch, int l, con
 #pragma unroll
   for (int j = SMAX - 1; j >= 0; j--) {
     if (j < cnt) {
-      const long i = a0 + j;
+      const int i = a0 + j;
       const double2 v = ca(p[j], cm(__ldg(tH + i), vin));
       yv = (j == cnt - 1) ? cm(__ldg(trb + i), v) : ca(cm(__ldg(trb + i), v), cm(__ldg(tQ + i), yv));
       p[j] = yv;
@@ -483,45 +487,69 @@ __device__ __forceinline__ void cn_warp_line(double2 *sm, long pitch, int l, con
   }
 }
 
-// Potential half-step on every element of a tile (all threads); the V
-// values of a batch of elements are loaded before any phase is applied, so
-// their global loads overlap.
+// Potential half-step on every element of a tile (all threads).  Each
+// thread keeps one line (contiguous) or one column (strided) and walks its
+// elements, so the grid coordinates of the line are decoded once; the V
+// values of a batch of elements are loaded before any phase is applied.
 template <bool CONTIG>
-__device__ __forceinline__ void cn_tile_pot(double2 *sm, long pitch, int nl, long line0, long o, long col0,
+__device__ __forceinline__ void cn_tile_pot(double2 *sm, int pitch, int nl, long line0, long o, long col0,
                                             const CnAxis &a, const gb_potential &pt) {
   constexpr int B = 4;
-  const long n = a.n, total = (long) nl * n;
-  auto where = [&](long e, long &ix, long &iy, long &iz) -> int {
-    long l, i;
-    if constexpr (CONTIG) {
-      l = e / n;
-      i = e - l * n;
+  const int n = (int) a.n;
+  const long vrow = pt.vrow;
+  int l, i0, di;
+  long ix = 0, iy = 0, iz = 0, vbase = 0, vstep = 0;  // V index of element i: vbase + i * vstep
+  if constexpr (CONTIG) {
+    l = threadIdx.x >> 5;  // one line per warp
+    i0 = threadIdx.x & 31;
+    di = 32;
+    if (l >= nl) return;
+    const long lid = line0 + l;
+    ix = lid / a.ny;
+    iy = lid - ix * a.ny;
+    vbase = (ix * a.ny + iy) * vrow;
+    vstep = 1;
+  } else {
+    constexpr int TL = tile_lines<false>();
+    l = threadIdx.x % TL;  // one column per thread, TL columns side by side
+    i0 = threadIdx.x / TL;
+    di = kCnWarpThreads / TL;
+    if (l >= nl) return;
+    const long q = col0 + l;
+    if (a.axis == 0) {
+      iy = q / a.nz;
+      iz = q - iy * a.nz;
+      vbase = iy * vrow + iz;
+      vstep = a.ny * vrow;
     } else {
-      i = e / nl;
-      l = e - i * nl;
+      ix = o;
+      iz = q;
+      vbase = ix * a.ny * vrow + iz;
+      vstep = vrow;
     }
-    cn_decode(a, CONTIG ? line0 + l : o, i, col0 + l, ix, iy, iz);
-    return (int) (CONTIG ? l * pitch + i : i * pitch + l);
-  };
-  for (long e0 = threadIdx.x; e0 < total; e0 += (long) blockDim.x * B) {
+  }
+  double2 *const base = CONTIG ? sm + l * pitch : sm + l;
+  const int es = CONTIG ? 1 : pitch;
+  for (int ib = i0; ib < n; ib += di * B) {
     double2 v[B];
 #pragma unroll
     for (int k = 0; k < B; k++) {
-      const long e = e0 + (long) k * blockDim.x;
+      const int i = ib + k * di;
       v[k] = make_double2(0.0, 0.0);
-      if (e < total) {
-        long ix, iy, iz;
-        where(e, ix, iy, iz);
-        v[k] = cn_pot_v(ix, iy, iz, a, pt);
+      if (i < n) {
+        const long vi = vbase + i * vstep;
+        if (pt.kind == GB_POT_COMPLEX) v[k] = ((const double2 *) pt.v)[vi];
+        else if (pt.kind == GB_POT_REAL) v[k].x = ((const double *) pt.v)[vi];
       }
     }
 #pragma unroll
     for (int k = 0; k < B; k++) {
-      const long e = e0 + (long) k * blockDim.x;
-      if (e < total) {
-        long ix, iy, iz;
-        const int q = where(e, ix, iy, iz);
-        sm[q] = cn_pot_with(sm[q], v[k], ix, iy, iz, pt);
+      const int i = ib + k * di;
+      if (i < n) {
+        double2 &r = base[i * es];
+        const long jx = CONTIG ? ix : (a.axis == 0 ? i : ix), jy = CONTIG ? iy : (a.axis == 0 ? iy : i);
+        const long jz = CONTIG ? i : iz;
+        r = cn_pot_with(r, v[k], jx, jy, jz, pt);
       }
     }
   }
@@ -550,20 +578,21 @@ template <bool CONTIG> __device__ __forceinline__ CnTile cn_tile_of(const CnAxis
   return c;
 }
 
-// Bulk copies of one tile between global memory and a shared buffer, issued
-// by the 32 lanes of warp 0 (load: completion on bar).
+// This thread's bulk copy of one tile between global memory and a shared
+// buffer: contiguous tiles one line per thread, strided tiles one row per
+// thread (n <= 256 rows; load completion on bar).
 template <bool CONTIG, bool LOAD>
-__device__ __forceinline__ void cn_tile_copy(double2 *psi, double2 *buf, long pitch, const CnTile &c, const CnAxis &a,
-                                             uint64_t *bar, int lane) {
+__device__ __forceinline__ void cn_tile_copy(double2 *psi, double2 *buf, int pitch, const CnTile &c, const CnAxis &a,
+                                             uint64_t *bar, int tid) {
   const long n = a.n;
   if constexpr (CONTIG) {
-    for (int l = lane; l < c.nl; l += 32) {
-      double2 *g = psi + (c.line0 + l) * n;
-      if (LOAD) bulk_g2s(buf + l * pitch, g, (unsigned) (n * 16), bar);
-      else bulk_s2g(g, buf + l * pitch, (unsigned) (n * 16));
+    if (tid < c.nl) {
+      double2 *g = psi + (c.line0 + tid) * n;
+      if (LOAD) bulk_g2s(buf + tid * pitch, g, (unsigned) (n * 16), bar);
+      else bulk_s2g(g, buf + tid * pitch, (unsigned) (n * 16));
     }
   } else {
-    for (long i = lane; i < n; i += 32) {
+    for (int i = tid; i < n; i += kCnWarpThreads) {
       double2 *g = psi + (c.o * n + i) * a.inner + c.col0;
       if (LOAD) bulk_g2s(buf + i * pitch, g, (unsigned) (c.nl * 16), bar);
       else bulk_s2g(g, buf + i * pitch, (unsigned) (c.nl * 16));
@@ -576,39 +605,33 @@ __global__ void __launch_bounds__(kCnWarpThreads, 2) k_cn_warp(double2 *__restri
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ __align__(8) uint64_t bars[2];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const long n = a.n;
-  const long pitch = warp_pitch(CONTIG, n);
-  const long bufsz = CONTIG ? (long) tile_lines<CONTIG>() * pitch : n * pitch;
+  const int n = (int) a.n;
+  const int pitch = (int) warp_pitch(CONTIG, n);
+  const int bufsz = CONTIG ? tile_lines<CONTIG>() * pitch : n * pitch;
   double2 *const buf0 = (double2 *) smraw;
   auto buf = [&](int b) { return buf0 + (b ? bufsz : 0); };
+  long t = blockIdx.x;
+  if (t >= ntiles) return;
   if (tid == 0) {
     mbar_init(&bars[0], 1);
     mbar_init(&bars[1], 1);
     fence_mbar_init();
+    mbar_arrive_expect_tx(&bars[0], (unsigned) (cn_tile_of<CONTIG>(a, t, tpo).nl * a.n * 16));
   }
   __syncthreads();
-  long t = blockIdx.x;
-  if (t >= ntiles) return;
-  if (warp == 0) {
-    const CnTile c0 = cn_tile_of<CONTIG>(a, t, tpo);
-    if (lane == 0) mbar_arrive_expect_tx(&bars[0], (unsigned) (c0.nl * n * 16));
-    __syncwarp();
-    cn_tile_copy<CONTIG, true>(psi, buf(0), pitch, c0, a, &bars[0], lane);
-  }
+  cn_tile_copy<CONTIG, true>(psi, buf(0), pitch, cn_tile_of<CONTIG>(a, t, tpo), a, &bars[0], tid);
   const bool pre = (a.pre.kind != GB_POT_NONE || a.pre.g != 0.0);
   const bool post = (a.post.kind != GB_POT_NONE || a.post.g != 0.0);
   for (unsigned it = 0; t < ntiles; t += gridDim.x, it++) {
     const int b = it & 1;
     const long next = t + gridDim.x;
-    if (warp == 0 && next < ntiles) {
-      // the other buffer's stores (previous tile) must have read it first
-      bulk_wait_read_all();
-      __syncwarp();
-      const CnTile cn = cn_tile_of<CONTIG>(a, next, tpo);
-      if (lane == 0) mbar_arrive_expect_tx(&bars[b ^ 1], (unsigned) (cn.nl * n * 16));
-      __syncwarp();
-      cn_tile_copy<CONTIG, true>(psi, buf(b ^ 1), pitch, cn, a, &bars[b ^ 1], lane);
-    }
+    // prefetch the next tile into the other buffer once the previous tile's
+    // stores (issued by the same threads) have read it
+    bulk_wait_read_all();
+    if (tid == 0 && next < ntiles)
+      mbar_arrive_expect_tx(&bars[b ^ 1], (unsigned) (cn_tile_of<CONTIG>(a, next, tpo).nl * a.n * 16));
+    __syncthreads();
+    if (next < ntiles) cn_tile_copy<CONTIG, true>(psi, buf(b ^ 1), pitch, cn_tile_of<CONTIG>(a, next, tpo), a, &bars[b ^ 1], tid);
     const bool ok = mbar_wait_bounded(&bars[b], (it >> 1) & 1u);
     if (__syncthreads_or(!ok)) {
       // a copy never completed: record it, let the copies in flight land
@@ -618,7 +641,7 @@ __global__ void __launch_bounds__(kCnWarpThreads, 2) k_cn_warp(double2 *__restri
         mbar_wait_bounded(&bars[b], (it >> 1) & 1u);
         if (next < ntiles) mbar_wait_bounded(&bars[b ^ 1], ((it + 1) >> 1) & 1u);
       }
-      if (warp == 0) bulk_wait_all();
+      bulk_wait_all();
       return;
     }
     const CnTile c = cn_tile_of<CONTIG>(a, t, tpo);
@@ -634,12 +657,10 @@ __global__ void __launch_bounds__(kCnWarpThreads, 2) k_cn_warp(double2 *__restri
     }
     fence_proxy_async_smem();
     __syncthreads();
-    if (warp == 0) {
-      cn_tile_copy<CONTIG, false>(psi, sm, pitch, c, a, nullptr, lane);
-      bulk_commit();
-    }
+    cn_tile_copy<CONTIG, false>(psi, sm, pitch, c, a, nullptr, tid);
+    bulk_commit();
   }
-  if (warp == 0) bulk_wait_all();
+  bulk_wait_all();
 }
 
 // General path: one thread per line, element (line, i) of a workspace array

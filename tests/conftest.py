@@ -13,6 +13,15 @@ def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (runs the sm_100a kernels)")
 
 
+def pytest_collection_modifyitems(config, items):
+    # every test ends within 15 minutes: a test that never returns (a CPU
+    # oracle stuck in C code, say) ends the run instead of holding it (the
+    # thread method also stops code that never returns to Python)
+    for item in items:
+        if item.get_closest_marker("timeout") is None:
+            item.add_marker(pytest.mark.timeout(900, method="thread"))
+
+
 @pytest.fixture(scope="session")
 def b200():
     import libgrid_b200
