@@ -410,7 +410,7 @@ def run_cn192(api, lib, steps, world, peak):
         "bytes_per_point": 112,
         "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak},
         "sweeps": sweeps,
-        "note": "2nd-order Crank-Nicolson GP step, V/2 fused into the x and z line sweeps; warp-cooperative "
+        "note": "2nd-order Crank-Nicolson GP step, V/2 fused into the x and z line sweeps; segment-per-warp "
         "line solver",
     }
 

@@ -325,11 +325,13 @@ typedef struct {
 } gb_cn_params;
 int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, const gb_potential *pre, const gb_potential *post);
 /* Line solver of the Crank-Nicolson fast path (no rotation, no absorbing
- * region, lines of up to 256 points): 1 (the default) the warp-cooperative
- * solver (one warp per line, segment carries by a warp-shuffle scan), 0 the
- * segment-per-warp solver; -1 only queries.  Returns the previous setting.
- * Both solve the reference's systems; they differ only in rounding.  (No
- * reference counterpart.) */
+ * region, lines of up to 256 points): 0 (the default) the segment-per-warp
+ * solver (a lane per line, a warp per segment, carries chained through
+ * shared memory), 1 the warp-cooperative solver (one warp per line, segment
+ * carries by a warp-shuffle scan, persistent double-buffered tiles; measured
+ * slower on B200: 0.487 against 0.447 ms per 192^3 step); -1 only queries.
+ * Returns the previous setting.  Both solve the reference's systems; they
+ * differ only in rounding.  (No reference counterpart.) */
 int gb_cn_warp_solver(int on);
 
 /* --------------------------------------------------------------- noise */
