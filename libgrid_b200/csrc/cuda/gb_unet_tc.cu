@@ -107,7 +107,7 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
 
 // ---------------------------------------------------------- forward (tcgen05)
 
-constexpr int kTcThreads = 128;
+constexpr int kTcThreads = 256;  // two warpgroups: staging, epilogue
 constexpr int kTcM = 128;
 constexpr int kTcN = 16;  // output channels per CTA
 
@@ -159,25 +159,30 @@ __global__ void __launch_bounds__(kTcThreads) k_conv3_tc(TcConv p) {
   const int nb16 = p.nmma * 2 * (kTcN / 8) * 8;  // 16-byte units
   const uint4 *bsrc = p.bp + (size_t) blockIdx.y * nb16;
   for (int i = tid; i < nb16; i += kTcThreads) ((uint4 *) b_sm)[i] = bsrc[i];
-  // A operand: the zero-padded halo block, bf16 channel-chunk planes
-  const int npos = (p.tz + 2) * p.sz;
-  for (int c = 0; c < p.c8; c++) {
-    uint4 *plane = (uint4 *) (a_sm + (size_t) c * plane_bytes) + p.guard;
-    for (int s = tid; s < npos; s += kTcThreads) {
-      const int zs = s / p.sz, rem = s - zs * p.sz, ys = rem / p.sy, xs = rem - ys * p.sy;
-      const int z = z0 + zs - 1, y = y0 + ys - 1, x = xs - 1;
+  // A operand: the zero-padded halo block, bf16 channel-chunk planes; one
+  // staged row (chunk c, zs, ys) per warp at a time, lanes along x, the
+  // eight channel loads of a position issued together
+  const int rows_per_plane = (p.tz + 2) * (p.ty + 2);
+  for (int row = warp; row < p.c8 * rows_per_plane; row += kTcThreads / 32) {
+    const int c = row / rows_per_plane, rr = row - c * rows_per_plane;
+    const int zs = rr / (p.ty + 2), ys = rr - zs * (p.ty + 2);
+    const int z = z0 + zs - 1, y = y0 + ys - 1;
+    const bool inrow = z >= 0 && z < p.d && y >= 0 && y < p.h;
+    const long vrow = ((long) z * p.h + y) * p.w;
+    uint4 *prow = (uint4 *) (a_sm + (size_t) c * plane_bytes) + p.guard + zs * p.sz + ys * p.sy;
+    for (int xs = lane; xs < p.sy; xs += 32) {
+      const int x = xs - 1;
       float v[8];
 #pragma unroll
       for (int e = 0; e < 8; e++) v[e] = 0.f;
-      if (z >= 0 && z < p.d && y >= 0 && y < p.h && x >= 0 && x < p.w) {
-        const long vox = ((long) z * p.h + y) * p.w + x;
+      if (inrow && x >= 0 && x < p.w) {
 #pragma unroll
         for (int e = 0; e < 8; e++) {
           const int ch = c * 8 + e;
-          if (ch < p.cx) v[e] = __ldg(p.x + (size_t) ch * vol + vox);
+          if (ch < p.cx) v[e] = __ldg(p.x + (size_t) ch * vol + vrow + x);
         }
       }
-      plane[s] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
+      prow[xs] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
                             pack_bf16x2(v[6], v[7]));
     }
   }
@@ -212,15 +217,17 @@ __global__ void __launch_bounds__(kTcThreads) k_conv3_tc(TcConv p) {
     if (!mbar_wait_bounded(&bar, (unsigned) (batch & 1))) ok = false;
     if (__syncthreads_or(!ok)) break;
     tc_fence_after();
-    // epilogue: warp w reads TMEM lanes 32w..32w+31 = rows of each tile
-    for (int k = 0; k < nt; k++) {
-      const int pos = p.sz + (b0 + k) * kTcM + warp * 32 + lane;
+    // epilogue: warpgroup g takes tiles k = g, g + 2, ...; warp w reads TMEM
+    // lanes 32 (w % 4) .. + 31 = those rows of a tile
+    const int wq = warp & 3, wg = warp >> 2;
+    for (int k = wg; k < nt; k += kTcThreads / 128) {
+      const int pos = p.sz + (b0 + k) * kTcM + wq * 32 + lane;
       const int zs = pos / p.sz, rem = pos - zs * p.sz, ys = rem / p.sy, xs = rem - ys * p.sy;
       const bool useful = zs >= 1 && zs <= p.tz && ys >= 1 && ys <= p.ty && xs >= 1 && xs <= p.w;
       const long vox = ((long) (z0 + zs - 1) * p.h + (y0 + ys - 1)) * p.w + (xs - 1);
       for (int nb = 0; nb < p.np; nb += 16) {
         float v[16];
-        tc_ld16(tmem + ((uint32_t) (warp * 32) << 16) + (uint32_t) (k * p.np + nb), v);
+        tc_ld16(tmem + ((uint32_t) (wq * 32) << 16) + (uint32_t) (k * p.np + nb), v);
         if (useful) {
 #pragma unroll
           for (int q = 0; q < 16; q++) {
@@ -330,24 +337,49 @@ __global__ void __launch_bounds__(kWgThreads) k_conv3_wgrad_mma(TcWgrad p) {
   const int z0 = (blk / nby) * p.tz, y0 = (blk % nby) * p.ty;
   const long vol = (long) p.d * p.h * p.w;
   const int nq = p.tz * p.ty * p.w;
-  // gy of the block, bf16 [co][q] (rows past cout are zero)
-  for (int e = tid; e < 16 * p.co16 * nq; e += kWgThreads) {
-    const int co = e / nq, q = e - co * nq;
-    const int x = q % p.w, yz = q / p.w, yi = yz % p.ty, zi = yz / p.ty;
-    float v = 0.f;
-    if (co < p.cout) v = __ldg(p.gy + (size_t) co * vol + ((long) (z0 + zi) * p.h + (y0 + yi)) * p.w + x);
-    gys[(size_t) co * p.qp + q] = __float2bfloat16_rn(v);
+  // gy of the block, bf16 [co][q] (rows past cout are zero); one row
+  // (co, zi, yi) per warp at a time, lanes along x; the warp also sums the
+  // row (FP32, unrounded) for the bias gradient
+  const int bz = p.tz * p.ty;
+  __shared__ float brow[64 * 16];  // [co][zi ty + yi] row sums (co < 64, tz ty <= 16)
+  for (int row = warp; row < 16 * p.co16 * bz; row += kWgThreads / 32) {
+    const int co = row / bz, rr = row - co * bz, zi = rr / p.ty, yi = rr - zi * p.ty;
+    const float *src = p.gy + (size_t) co * vol + ((long) (z0 + zi) * p.h + (y0 + yi)) * p.w;
+    __nv_bfloat16 *dst = gys + (size_t) co * p.qp + (size_t) rr * p.w;
+    float s = 0.f;
+    for (int x = lane; x < p.w; x += 32) {
+      const float v = co < p.cout ? __ldg(src + x) : 0.f;
+      dst[x] = __float2bfloat16_rn(v);
+      s += v;
+    }
+    if (p.dobias && cz == 0 && co < p.cout) {
+      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+      if (lane == 0) brow[co * 16 + rr] = s;
+    }
   }
-  // three x-shifted copies of the x halo block for this chunk of 8 channels
+  // three x-shifted copies of the x halo block for this chunk of 8 channels:
+  // copy cp holds x[. + cp - 1]; each input value is loaded once and stored
+  // into the three copies
   const int srows = (p.tz + 2) * (p.ty + 2);
-  for (int e = tid; e < 3 * 8 * srows * p.w; e += kWgThreads) {
-    const int x = e % p.w, r = (e / p.w) % srows, c = (e / (p.w * srows)) % 8, cp = e / (p.w * srows * 8);
-    const int zs = r / (p.ty + 2), ys = r % (p.ty + 2);
-    const int z = z0 + zs - 1, y = y0 + ys - 1, xx = x + cp - 1, ci = cz * 8 + c;
-    float v = 0.f;
-    if (ci < p.cin && z >= 0 && z < p.d && y >= 0 && y < p.h && xx >= 0 && xx < p.w)
-      v = __ldg(p.x + (size_t) ci * vol + ((long) z * p.h + y) * p.w + xx);
-    xs[(size_t) cp * p.xcp + (size_t) c * p.xpp + (size_t) r * p.xrp + x] = __float2bfloat16_rn(v);
+  for (int row = warp; row < 8 * srows; row += kWgThreads / 32) {
+    const int c = row / srows, r = row - c * srows;
+    const int zs = r / (p.ty + 2), ys = r - zs * (p.ty + 2);
+    const int z = z0 + zs - 1, y = y0 + ys - 1, ci = cz * 8 + c;
+    const bool inrow = ci < p.cin && z >= 0 && z < p.d && y >= 0 && y < p.h;
+    const float *src = p.x + (size_t) ci * vol + ((long) z * p.h + y) * p.w;
+    __nv_bfloat16 *d0 = xs + (size_t) c * p.xpp + (size_t) r * p.xrp;
+    __nv_bfloat16 *d1 = d0 + p.xcp, *d2 = d0 + 2 * (size_t) p.xcp;
+    const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
+    for (int x = lane; x < p.w; x += 32) {
+      const __nv_bfloat16 v = __float2bfloat16_rn(inrow ? __ldg(src + x) : 0.f);
+      d1[x] = v;
+      if (x + 1 < p.w) d0[x + 1] = v;
+      if (x >= 1) d2[x - 1] = v;
+    }
+    if (lane == 0) {
+      d0[0] = zero;
+      d2[p.w - 1] = zero;
+    }
   }
   __syncthreads();
   float acc[kWgTaps][kWgCo16][4];
@@ -401,17 +433,12 @@ __global__ void __launch_bounds__(kWgThreads) k_conv3_wgrad_mma(TcWgrad p) {
       }
     }
   }
-  // bias partials (the first channel chunk's CTAs): sum of gy over the block
-  if (p.dobias && cz == 0) {
-    for (int co = warp; co < p.cout; co += kWgThreads / 32) {
-      float s = 0.f;
-      for (int q = lane; q < nq; q += 32) {
-        const int x = q % p.w, yzq = q / p.w, yq = yzq % p.ty, zq = yzq / p.ty;
-        s += __ldg(p.gy + (size_t) co * vol + ((long) (z0 + zq) * p.h + (y0 + yq)) * p.w + x);
-      }
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) p.part[(size_t) p.nblk * p.ncz * p.cout * 8 * 27 + (size_t) blk * p.cout + co] = s;
-    }
+  // bias partials (the first channel chunk's CTAs): the block's row sums
+  // of gy in row order
+  if (p.dobias && cz == 0 && tid < p.cout) {
+    float s = 0.f;
+    for (int rr = 0; rr < bz; rr++) s += brow[tid * 16 + rr];
+    p.part[(size_t) p.nblk * p.ncz * p.cout * 8 * 27 + (size_t) blk * p.cout + tid] = s;
   }
 }
 

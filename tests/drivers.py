@@ -83,19 +83,93 @@ def run_batch_steps(steps: int = 8, prec: int = 0) -> None:
         api.free(o)
 
 
+def run_unet_step(n: int = 128, tensor_cores: int = 1, reps: int = 1) -> None:
+    """One forward and backward pass of the warm-start U-Net at n^3 with
+    random weights and inputs (tensor-core or SIMT convolutions)."""
+    import ctypes as C
+
+    import numpy as np
+
+    import libgrid_b200 as gb
+    from libgrid_b200 import warmstart as ws
+
+    api = gb.load()
+    api.lib.cuda_enable(b"\x01", 0, None)
+    api.lib.gb_unet_tensor_cores.argtypes = [C.c_int]
+    api.lib.gb_unet_tensor_cores(tensor_cores)
+    rng = np.random.default_rng(1)
+    net = ws.DeviceUNet(api, n, cin=3, seed=0)
+    net.set_input(rng.standard_normal((3, n, n, n)).astype(np.float32))
+    tgt = net.set_target(rng.standard_normal((n, n, n)).astype(np.float32))
+    for _ in range(reps):
+        net.forward()
+        net.loss_grad(tgt)
+        net.backward()
+    api.lib.gb_synchronize()
+    net.free()
+
+
+def run_ops(n: int = 256) -> None:
+    """One call of each grid operation of the path at n^3 (FD stencils,
+    k-space operators, pointwise products, FFT, convolution, interpolation,
+    density, reductions), for an ncu launch list of those kernels."""
+    import numpy as np
+
+    import libgrid_b200 as gb
+    from libgrid_b200 import capi
+
+    api = gb.load()
+    lib = api.lib
+    lib.cuda_enable(b"\x01", 0, None)
+    rng = np.random.default_rng(2)
+    shape = (n, n, n)
+    a = api.cgrid(*shape, 0.2, values=rng.standard_normal(shape) + 1j * rng.standard_normal(shape))
+    b = api.cgrid(*shape, 0.2, values=rng.standard_normal(shape) + 1j * rng.standard_normal(shape))
+    c = api.cgrid(*shape, 0.2)
+    d = api.cgrid(*shape, 0.17)
+    r = api.rgrid(*shape, 0.2, values=rng.standard_normal(shape))
+    r2 = api.rgrid(*shape, 0.2)
+    w = api.wf(*shape, 0.2, 1.0, capi.WF_PERIODIC_BOUNDARY, capi.WF_2ND_ORDER_FFT)
+    lib.cgrid_copy(w.s.grid, a.ptr)
+    lib.cgrid_fd_laplace(a.ptr, c.ptr)
+    lib.cgrid_fd_gradient_x(a.ptr, c.ptr)
+    lib.rgrid_fd_laplace(r.ptr, r2.ptr)
+    lib.cgrid_product(c.ptr, a.ptr, b.ptr)
+    lib.cgrid_multiply(c.ptr, capi.Complex.of(0.5 - 0.25j))
+    lib.grid_wf_density(w.ptr, r2.ptr)
+    lib.cgrid_integral_of_square(a.ptr)
+    lib.cgrid_fft(a.ptr)
+    lib.cgrid_fft(b.ptr)
+    lib.cgrid_fft_laplace(a.ptr, c.ptr)
+    lib.cgrid_fft_convolute(c.ptr, a.ptr, b.ptr)
+    lib.cgrid_inverse_fft_norm(c.ptr)
+    lib.cgrid_extrapolate(d.ptr, c.ptr)
+    lib.gb_synchronize()
+    for o in (a, b, c, d, r, r2, w):
+        api.free(o)
+
+
 if __name__ == "__main__":
     import sys
 
     usage = ("usage: python tests/drivers.py gp [n] [steps] [prec: 0 FP64, 1 FP32]\n"
              "       python tests/drivers.py cn [n] [steps]\n"
-             "       python tests/drivers.py batch [steps] [prec]")
-    if len(sys.argv) < 2 or sys.argv[1] not in ("gp", "cn", "batch"):
+             "       python tests/drivers.py batch [steps] [prec]\n"
+             "       python tests/drivers.py unet [n] [tensor cores: 1 or 0] [reps]\n"
+             "       python tests/drivers.py ops [n]")
+    if len(sys.argv) < 2 or sys.argv[1] not in ("gp", "cn", "batch", "unet", "ops"):
         sys.exit(usage)
     a = [int(x) for x in sys.argv[2:]]
     if sys.argv[1] == "gp":
         print("norm", run_gp_steps(*a))
     elif sys.argv[1] == "cn":
         print("norm", run_cn_steps(*a))
+    elif sys.argv[1] == "unet":
+        run_unet_step(*a)
+        print("ok")
+    elif sys.argv[1] == "ops":
+        run_ops(*a)
+        print("ok")
     else:
         run_batch_steps(*a)
         print("ok")

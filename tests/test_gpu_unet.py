@@ -199,11 +199,11 @@ def test_warm_start_cuts_imaginary_time_steps(b200, lib):
     print("warm start: steps %.0f (Gaussian) -> %.0f (network); TF start %.0f; max |dE| %.2e"
           % (steps_g, steps_n, np.mean([r["steps_tf"] for r in rows]), max(r["de"] for r in rows)))
     assert steps_n < steps_g
-    # stopping rule |dE| < 1e-9 over 10 steps: the converged energies of the
-    # network and the Gaussian start agree to 1e-8 Ha; both lie within a few
-    # 1e-8 Ha of the limit a far tighter stopping rule (1e-12) reaches
+    # the stopping rule estimates the remaining distance to the limit: the
+    # network and the Gaussian start converge to energies within 1e-8 Ha of
+    # each other and of the limit a far tighter rule (1e-12 change) reaches
     assert max(r["de"] for r in rows) < 1e-8
-    assert max(r["de_net_ref"] for r in rows) < 5e-8
+    assert max(r["de_net_ref"] for r in rows) < 1e-8
 
 
 def test_device_problem_features_match_host(b200, lib):
