@@ -75,7 +75,8 @@ for _ax, _an in enumerate("xyz"):
 KIND_NAMES[18] = "zy_fwd_chain"
 KIND_NAMES[19] = "z_inv_pot_fwd_y_fwd_chain"
 KIND_NAMES[20] = "yz_inv_chain"
-NUM_KINDS = 21
+KIND_NAMES[21] = "y_inv_z_inv_pot_fwd_y_fwd_chain"
+NUM_KINDS = 22
 
 
 def measured_traffic(kind, n):

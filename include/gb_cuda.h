@@ -143,9 +143,11 @@ int gb_pass_pipeline(int on);
  * y INV + z INV transforms of a split-operator step (in FP64 also the
  * potential pass with the y FWD after it) each run as one persistent launch
  * that works plane by plane, so the intermediate result stays in L2 (grids
- * with nx >= 2 and ny = nz = 256).  on = 1 enables (the
- * default), 0 disables, -1 only queries; returns the previous setting.  Both
- * schedules compute the same values.  (No reference counterpart.) */
+ * with nx >= 2 and ny = nz = 256).  on = 1 enables, 2 also chains the y INV
+ * pass in front of the FP64 potential chain (y INV | z INV.V.FWD | y FWD in
+ * one launch: five launches per step), 0 disables, -1 only queries; returns
+ * the previous setting.  All schedules compute the same values.  (No
+ * reference counterpart.) */
 int gb_plane_passes(int on);
 /* Ticket lag of the plane-chained passes, in percent of one resident wave of
  * tiles (default 200): the second stage of a plane is issued that far behind

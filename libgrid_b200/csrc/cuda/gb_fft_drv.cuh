@@ -73,7 +73,7 @@ template <typename T> bool plane_ok(const gb_geom *g) {
 }
 
 // Timing kinds of the chains: 18 [z FWD, y FWD], 19 [z INV.V.FWD (or
-// INV.FWD), y FWD], 20 [y INV, z INV].
+// INV.FWD), y FWD], 20 [y INV, z INV], 21 [y INV, z INV.V.FWD, y FWD].
 template <typename T, class... Stages>
 int plane_chain(const gb_geom *g, void *psi, const PassArgs &a, int kind, Stages...) {
   ChainArgs c;
@@ -98,6 +98,18 @@ int plane_chain(const gb_geom *g, void *psi, const PassArgs &a, int kind, Stages
 // two run as one chain (the potential stage at 3 CTAs per SM); in FP32 the
 // chain is slower than the two passes, and all three stay line passes.
 template <typename T> int plane_mid(const gb_geom *g, void *psi, const PassArgs &a, bool has_pot) {
+  if constexpr (sizeof(T) == 8) {
+    // schedule 2: the y INV pass joins the chain as its first stage (kind 21)
+    if (plane_enabled() == 2) {
+      if (has_pot && a.pot.kind == GB_POT_REAL && !a.pot.absorb && a.pot.c_re == 0.0)
+        return plane_chain<T>(g, psi, a, 21, Stage<1, OP_INV>{}, Stage<2, OP_INV, OP_POT_RP, OP_FWD>{},
+                              Stage<1, OP_FWD>{});
+      return has_pot ? plane_chain<T>(g, psi, a, 21, Stage<1, OP_INV>{}, Stage<2, OP_INV, OP_POT, OP_FWD>{},
+                                      Stage<1, OP_FWD>{})
+                     : plane_chain<T>(g, psi, a, 21, Stage<1, OP_INV>{}, Stage<2, OP_INV, OP_FWD>{},
+                                      Stage<1, OP_FWD>{});
+    }
+  }
   int rc = pass<T>(g, 1, psi, psi, a, OpL<OP_INV>{});
   if (rc) return rc;
   if constexpr (sizeof(T) == 8) {

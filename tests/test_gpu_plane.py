@@ -59,46 +59,53 @@ def _run(b200, shape, prec, time, steps=3, multi=False, g=0.0025, kind="gp"):
     return out, psi0, v
 
 
-def _both(b200, *args, **kw):
+def _both(b200, *args, mode=1, **kw):
     lib = _lib(b200)
     old = lib.gb_plane_passes(0)
     try:
         nine, psi0, v = _run(b200, *args, **kw)
-        lib.gb_plane_passes(1)
+        lib.gb_plane_passes(mode)
         plane, _, _ = _run(b200, *args, **kw)
     finally:
         lib.gb_plane_passes(old)
     return plane, nine, psi0, v
 
 
+MODES = [1, 2]  # 2: y INV chained in front of the potential chain
+
+
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("shape", [(2, 256, 256), (16, 256, 256)])
 @pytest.mark.parametrize("time", [1.0, -1.0j])
 @pytest.mark.parametrize("prec", [0, capi.GRID_PREC_FP32])
-def test_plane_matches_nine_pass(b200, shape, time, prec):
-    plane, nine, _, _ = _both(b200, shape, prec, time)
+def test_plane_matches_nine_pass(b200, shape, time, prec, mode):
+    plane, nine, _, _ = _both(b200, shape, prec, time, mode=mode)
     assert rel(plane, nine) <= (1e-15 if not prec else 1e-7)
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("kind", ["free", "complex"])
-def test_plane_other_programs(b200, kind):
-    plane, nine, _, _ = _both(b200, (4, 256, 256), 0, 1.0, kind=kind)
+def test_plane_other_programs(b200, kind, mode):
+    plane, nine, _, _ = _both(b200, (4, 256, 256), 0, 1.0, kind=kind, mode=mode)
     assert rel(plane, nine) <= 1e-15
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("kind", ["gp", "free"])
 @pytest.mark.parametrize("prec", [0, capi.GRID_PREC_FP32])
-def test_plane_multistep(b200, kind, prec):
-    plane, nine, _, _ = _both(b200, (8, 256, 256), prec, 1.0, steps=7, multi=True, kind=kind)
+def test_plane_multistep(b200, kind, prec, mode):
+    plane, nine, _, _ = _both(b200, (8, 256, 256), prec, 1.0, steps=7, multi=True, kind=kind, mode=mode)
     assert rel(plane, nine) <= (1e-15 if not prec else 1e-7)
 
 
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("prec", [0, capi.GRID_PREC_FP32])
-def test_plane_chains_full_size(b200, prec):
+def test_plane_chains_full_size(b200, prec, mode):
     """The 256^3 workload: 256 planes per chain, two steps and a multi-step
     call, bit for bit against the nine-pass schedule."""
-    plane, nine, _, _ = _both(b200, (256, 256, 256), prec, 1.0, steps=2)
+    plane, nine, _, _ = _both(b200, (256, 256, 256), prec, 1.0, steps=2, mode=mode)
     assert rel(plane, nine) <= (1e-15 if not prec else 1e-7)
-    plane, nine, _, _ = _both(b200, (256, 256, 256), prec, -1.0j, steps=4, multi=True)
+    plane, nine, _, _ = _both(b200, (256, 256, 256), prec, -1.0j, steps=4, multi=True, mode=mode)
     assert rel(plane, nine) <= (1e-15 if not prec else 1e-7)
 
 
@@ -116,28 +123,34 @@ def test_plane_against_oracle(b200, restate):
     assert rel(got, want) < 1e-11
 
 
-def test_plane_timing_kinds(b200):
+@pytest.mark.parametrize("mode", MODES)
+def test_plane_timing_kinds(b200, mode):
     """A chained FP64 step runs six launches: the three chains (kinds 18, 19
-    and 20), the x FWD.K.INV pass twice and the y INV pass; the pass error
-    flag stays clear."""
+    and 20), the x FWD.K.INV pass twice and the y INV pass; with the y INV
+    pass chained in front of the potential chain (kind 21) five launches;
+    the pass error flag stays clear."""
     lib = _lib(b200)
     lib.gb_pass_timing.argtypes = [C.c_int]
     lib.gb_pass_timing_report.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_long), C.c_int]
     lib.gb_pass_error_flag.argtypes = [C.c_int]
     lib.gb_pass_error_flag.restype = C.c_int
-    old = lib.gb_plane_passes(1)
+    old = lib.gb_plane_passes(mode)
     try:
         lib.gb_pass_timing(1)
         _run(b200, (4, 256, 256), 0, 1.0, steps=1)
-        ms = (C.c_double * 21)()
-        cnt = (C.c_long * 21)()
-        lib.gb_pass_timing_report(ms, cnt, 21)
+        ms = (C.c_double * 22)()
+        cnt = (C.c_long * 22)()
+        lib.gb_pass_timing_report(ms, cnt, 22)
         lib.gb_pass_timing(0)
     finally:
         lib.gb_plane_passes(old)
     counts = list(cnt)
-    assert counts[18] == 1 and counts[19] == 1 and counts[20] == 1
+    assert counts[18] == 1 and counts[20] == 1
     assert counts[2] == 2  # x FWD.K.INV
-    assert counts[6] == 1  # y INV
-    assert sum(counts) == 6
+    if mode == 1:
+        assert counts[19] == 1 and counts[6] == 1  # y INV
+        assert sum(counts) == 6
+    else:
+        assert counts[21] == 1
+        assert sum(counts) == 5
     assert lib.gb_pass_error_flag(1) == 0
