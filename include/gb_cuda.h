@@ -79,6 +79,17 @@ void gb_clear_error(void);
 int gb_synchronize(void);
 void *gb_stream_handle(void);
 long gb_launch_count(void);
+/* CUDA graphs of library calls (no reference counterpart): gb_graph_begin
+ * captures the library stream, so the kernels the following calls issue are
+ * recorded instead of run; gb_graph_end instantiates them (*graph receives a
+ * handle); gb_graph_launch replays them on the library stream with the same
+ * arguments and pointers; gb_graph_free releases the handle.  Captured calls
+ * must not read results back to the host; run the same calls once without
+ * capture first, so that scratch buffers already have their size. */
+int gb_graph_begin(void);
+int gb_graph_end(void **graph);
+int gb_graph_launch(void *graph);
+int gb_graph_free(void *graph);
 void *gb_device_alloc(size_t bytes);
 void gb_device_free(void *p);
 void *gb_host_alloc(size_t bytes); /* page-locked when possible */

@@ -162,6 +162,74 @@ __device__ __forceinline__ double2 cn_rhs(long i, long n, int bc, double2 cp, do
   return cs(cs(cs(cm(cp, p0), ca(cs(pm, two_p0), pfirst)), cm(c2, dif)), cm(c3y, dif));
 }
 
+// Potential factor on the elements i = i0, i0 + di, ... < n of one tile line
+// or column whose element i sits at base[i * es]; V of element i at
+// vbase + i * vstep, coordinates (ix, iy, iz) with the line's own axis
+// running along i.  No division per element; V loads batched by B.
+__device__ __forceinline__ void cn_pot_elems(double2 *base, int es, int i0, int di, int n, long vbase, long vstep,
+                                             long ix, long iy, long iz, const CnAxis &a, const gb_potential &pt) {
+  constexpr int B = 4;
+  for (int ib = i0; ib < n; ib += di * B) {
+    double2 v[B];
+#pragma unroll
+    for (int k = 0; k < B; k++) {
+      const int i = ib + k * di;
+      v[k] = make_double2(0.0, 0.0);
+      if (i < n) {
+        const long vi = vbase + i * vstep;
+        if (pt.kind == GB_POT_COMPLEX) v[k] = ((const double2 *) pt.v)[vi];
+        else if (pt.kind == GB_POT_REAL) v[k].x = ((const double *) pt.v)[vi];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < B; k++) {
+      const int i = ib + k * di;
+      if (i < n) {
+        double2 &r = base[i * es];
+        const long jx = a.axis == 0 ? i : ix, jy = a.axis == 1 ? i : iy, jz = a.axis == 2 ? i : iz;
+        r = cn_pot_with(r, v[k], jx, jy, jz, pt);
+      }
+    }
+  }
+}
+
+// Potential factor over a whole tile in shared memory.  Contiguous tiles
+// (lines along z, element (l, i) at sm[l * pitch + i]): one line per warp
+// at a time, lanes along the line.  Strided tiles (element (l, i) at
+// sm[i * pitch + l], pitch >= cols): one column per thread, `cols` columns
+// side by side, threads of equal column spaced along the rows.
+template <bool CONTIG>
+__device__ __forceinline__ void cn_tile_pot(double2 *sm, int pitch, int cols, int nl, long line0, long o, long col0,
+                                            const CnAxis &a, const gb_potential &pt) {
+  const int n = (int) a.n, nthr = (int) blockDim.x;
+  const long vrow = pt.vrow;
+  if constexpr (CONTIG) {
+    for (int l = (int) (threadIdx.x >> 5); l < nl; l += nthr >> 5) {
+      const long lid = line0 + l;
+      const long ix = lid / a.ny, iy = lid - ix * a.ny;
+      cn_pot_elems(sm + (long) l * pitch, 1, (int) (threadIdx.x & 31), 32, n, (ix * a.ny + iy) * vrow, 1, ix, iy, 0,
+                   a, pt);
+    }
+  } else {
+    const int l = (int) threadIdx.x % cols;
+    if (l >= nl) return;
+    const long q = col0 + l;
+    long ix = 0, iy = 0, iz = 0, vbase, vstep;
+    if (a.axis == 0) {
+      iy = q / a.nz;
+      iz = q - iy * a.nz;
+      vbase = iy * vrow + iz;
+      vstep = a.ny * vrow;
+    } else {
+      ix = o;
+      iz = q;
+      vbase = ix * a.ny * vrow + iz;
+      vstep = vrow;
+    }
+    cn_pot_elems(sm + l, pitch, (int) threadIdx.x / cols, nthr / cols, n, vbase, vstep, ix, iy, iz, a, pt);
+  }
+}
+
 // Segments per line in the fast kernel (= warps per CTA).
 constexpr int kSeg = 16;
 
@@ -176,16 +244,41 @@ template <bool CONTIG> __device__ __forceinline__ double2 &tile_at(double2 *sm, 
   else return sm[i * row + l];
 }
 
-// Fast path.  A CTA of 8 warps owns up to 32 lines (lane = line); warp s
-// owns segment s = [s S, (s+1) S) of every line, S = ceil(n / 8).  Both
+// Fast path.  A CTA of 16 warps owns up to 32 lines (lane = line); warp s
+// owns segment s = [s S, (s+1) S) of every line, S = ceil(n / 16) (at most
+// SMAX when SMAX > 0).  Both
 // Thomas recurrences are linear with line-independent coefficients:
 //   forward  v_i = b_i - m_i v_{i-1}
 //   backward x_i = rb_i v_i + Q_i x_{i+1},   Q_i = -rb_i c_i
 // so each warp runs the particular recurrence of its segment from a zero
-// carry-in, one warp chains the 8 segment carries per line, and every
+// carry-in, one warp chains the 16 segment carries per line, and every
 // element then adds (carry-in) x (homogeneous response), whose tables
 // H_i = prod(-m_j) and G_i = prod(Q_j) over the segment are precomputed.
-template <bool CONTIG> __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast(double2 *__restrict__ psi, CnAxis a) {
+// Loop k = 0 .. cnt - 1 (seg_loop_rev: downwards) over a segment; SMAX > 0
+// unrolls it for segments of at most SMAX points, so the table loads of
+// all steps issue ahead of the recurrence.
+template <int SMAX, class F> __device__ __forceinline__ void seg_loop(int cnt, F &&f) {
+  if constexpr (SMAX > 0) {
+#pragma unroll
+    for (int k = 0; k < SMAX; k++)
+      if (k < cnt) f(k);
+  } else {
+    for (int k = 0; k < cnt; k++) f(k);
+  }
+}
+
+template <int SMAX, class F> __device__ __forceinline__ void seg_loop_rev(int cnt, F &&f) {
+  if constexpr (SMAX > 0) {
+#pragma unroll
+    for (int k = SMAX - 1; k >= 0; k--)
+      if (k < cnt) f(k);
+  } else {
+    for (int k = cnt - 1; k >= 0; k--) f(k);
+  }
+}
+
+template <bool CONTIG, int SMAX>
+__global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast(double2 *__restrict__ psi, CnAxis a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ __align__(8) uint64_t bar;
   __shared__ double2 s_end[kSeg][32];
@@ -229,29 +322,16 @@ template <bool CONTIG> __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast
   }
 
   // ---- optional first potential half-step (all threads, element-parallel)
-  if (a.pre.kind != GB_POT_NONE || a.pre.g != 0.0) {
-    for (long e = tid; e < (long) nl * n; e += 32 * kSeg) {
-      long l, i;
-      if constexpr (CONTIG) {
-        l = e / n;
-        i = e - l * n;
-      } else {
-        i = e / nl;
-        l = e - i * nl;
-      }
-      long ix, iy, iz;
-      cn_decode(a, CONTIG ? line0 + l : o, i, col0 + l, ix, iy, iz);
-      double2 &r = tile_at<CONTIG>(sm, (int) l, i, row);
-      r = cn_pot(r, ix, iy, iz, a, a.pre);
-    }
-  }
+  if (a.pre.kind != GB_POT_NONE || a.pre.g != 0.0)
+    cn_tile_pot<CONTIG>(sm, (int) row, lpc, nl, line0, o, col0, a, a.pre);
   __syncthreads();
 
   const double2 *tm = a.tab, *trb = a.tab + n, *tz = a.tab + 2 * n, *tH = a.tab + 3 * n, *tQ = a.tab + 4 * n,
                 *tG = a.tab + 5 * n;
   const long S = (n + kSeg - 1) / kSeg;
   const long a0 = seg * S, e0 = (a0 + S < n) ? a0 + S : n;
-  const bool active = (lane < nl) && (a0 < e0);
+  const int cnt = a0 < e0 ? (int) (e0 - a0) : 0;
+  const bool active = (lane < nl) && (cnt > 0);
   const int bc = a.boundary;
 
   // ---- neighbours of the segment, read before anything is overwritten
@@ -270,23 +350,25 @@ template <bool CONTIG> __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast
   double2 u = zero;
   if (active) {
     double2 pm = p_before, p0 = tile_at<CONTIG>(sm, lane, a0, row);
-    for (long i = a0; i < e0; i++) {
-      const double2 pp = (i + 1 < e0) ? tile_at<CONTIG>(sm, lane, i + 1, row) : p_after;
+    seg_loop<SMAX>(cnt, [&](int k) {
+      const long i = a0 + k;
+      const double2 pp = (k + 1 < cnt) ? tile_at<CONTIG>(sm, lane, i + 1, row) : p_after;
       const double2 b = cn_rhs(i, n, bc, a.cp, a.c2, zero, pm, p0, pp, pfirst, plast);
-      u = (i == a0) ? b : cs(b, cm(tm[i], u));
+      u = (k == 0) ? b : cs(b, cm(__ldg(tm + i), u));
       tile_at<CONTIG>(sm, lane, i, row) = u;
       pm = p0;
       p0 = pp;
-    }
+    });
   }
   if (lane < nl) s_end[seg][lane] = u;
   __syncthreads();
   if (seg == 0 && lane < nl) {
     double2 vin = zero;
+#pragma unroll
     for (int s = 0; s < kSeg; s++) {
       const long as = s * S, es = (as + S < n) ? as + S : n;
       s_in[s][lane] = vin;
-      if (as < es) vin = ca(s_end[s][lane], cm(tH[es - 1], vin));
+      if (as < es) vin = ca(s_end[s][lane], cm(__ldg(tH + es - 1), vin));
     }
   }
   __syncthreads();
@@ -295,20 +377,22 @@ template <bool CONTIG> __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast
   double2 y = zero;
   if (active) {
     const double2 vin = s_in[seg][lane];
-    for (long i = e0 - 1; i >= a0; i--) {
-      const double2 v = ca(tile_at<CONTIG>(sm, lane, i, row), cm(tH[i], vin));
-      y = (i == e0 - 1) ? cm(trb[i], v) : ca(cm(trb[i], v), cm(tQ[i], y));
+    seg_loop_rev<SMAX>(cnt, [&](int k) {
+      const long i = a0 + k;
+      const double2 v = ca(tile_at<CONTIG>(sm, lane, i, row), cm(__ldg(tH + i), vin));
+      y = (k == cnt - 1) ? cm(__ldg(trb + i), v) : ca(cm(__ldg(trb + i), v), cm(__ldg(tQ + i), y));
       tile_at<CONTIG>(sm, lane, i, row) = y;
-    }
+    });
   }
   if (lane < nl) s_end[seg][lane] = y;
   __syncthreads();
   if (seg == 0 && lane < nl) {
     double2 xin = zero;
+#pragma unroll
     for (int s = kSeg - 1; s >= 0; s--) {
       const long as = s * S, es = (as + S < n) ? as + S : n;
       s_in[s][lane] = xin;
-      if (as < es) xin = ca(s_end[s][lane], cm(tG[as], xin));
+      if (as < es) xin = ca(s_end[s][lane], cm(__ldg(tG + as), xin));
     }
     if (bc == 3) {
       // Sherman-Morrison: fact = (x_0 + beta x_{n-1} / gamma) / den; the
@@ -319,21 +403,21 @@ template <bool CONTIG> __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast
   }
   __syncthreads();
 
-  // ---- backward fix-up, periodic correction, second potential half-step
-  const bool post = (a.post.kind != GB_POT_NONE || a.post.g != 0.0);
+  // ---- backward fix-up and periodic correction
   if (active) {
     const double2 xin = s_in[seg][lane];
     const double2 fact = (bc == 3) ? s_fact[lane] : zero;
-    for (long i = a0; i < e0; i++) {
-      double2 x = ca(tile_at<CONTIG>(sm, lane, i, row), cm(tG[i], xin));
-      if (bc == 3) x = cs(x, cm(fact, tz[i]));
-      if (post) {
-        long ix, iy, iz;
-        cn_decode(a, CONTIG ? line0 + lane : o, i, col0 + lane, ix, iy, iz);
-        x = cn_pot(x, ix, iy, iz, a, a.post);
-      }
+    seg_loop<SMAX>(cnt, [&](int k) {
+      const long i = a0 + k;
+      double2 x = ca(tile_at<CONTIG>(sm, lane, i, row), cm(__ldg(tG + i), xin));
+      if (bc == 3) x = cs(x, cm(fact, __ldg(tz + i)));
       tile_at<CONTIG>(sm, lane, i, row) = x;
-    }
+    });
+  }
+  // ---- optional second potential half-step (element-parallel)
+  if (a.post.kind != GB_POT_NONE || a.post.g != 0.0) {
+    __syncthreads();
+    cn_tile_pot<CONTIG>(sm, (int) row, lpc, nl, line0, o, col0, a, a.post);
   }
 
   // ---- tile store
@@ -491,70 +575,6 @@ __device__ __forceinline__ void cn_warp_line(double2 *sm, int pitch, int l, cons
 // thread keeps one line (contiguous) or one column (strided) and walks its
 // elements, so the grid coordinates of the line are decoded once; the V
 // values of a batch of elements are loaded before any phase is applied.
-template <bool CONTIG>
-__device__ __forceinline__ void cn_tile_pot(double2 *sm, int pitch, int nl, long line0, long o, long col0,
-                                            const CnAxis &a, const gb_potential &pt) {
-  constexpr int B = 4;
-  const int n = (int) a.n;
-  const long vrow = pt.vrow;
-  int l, i0, di;
-  long ix = 0, iy = 0, iz = 0, vbase = 0, vstep = 0;  // V index of element i: vbase + i * vstep
-  if constexpr (CONTIG) {
-    l = threadIdx.x >> 5;  // one line per warp
-    i0 = threadIdx.x & 31;
-    di = 32;
-    if (l >= nl) return;
-    const long lid = line0 + l;
-    ix = lid / a.ny;
-    iy = lid - ix * a.ny;
-    vbase = (ix * a.ny + iy) * vrow;
-    vstep = 1;
-  } else {
-    constexpr int TL = tile_lines<false>();
-    l = threadIdx.x % TL;  // one column per thread, TL columns side by side
-    i0 = threadIdx.x / TL;
-    di = kCnWarpThreads / TL;
-    if (l >= nl) return;
-    const long q = col0 + l;
-    if (a.axis == 0) {
-      iy = q / a.nz;
-      iz = q - iy * a.nz;
-      vbase = iy * vrow + iz;
-      vstep = a.ny * vrow;
-    } else {
-      ix = o;
-      iz = q;
-      vbase = ix * a.ny * vrow + iz;
-      vstep = vrow;
-    }
-  }
-  double2 *const base = CONTIG ? sm + l * pitch : sm + l;
-  const int es = CONTIG ? 1 : pitch;
-  for (int ib = i0; ib < n; ib += di * B) {
-    double2 v[B];
-#pragma unroll
-    for (int k = 0; k < B; k++) {
-      const int i = ib + k * di;
-      v[k] = make_double2(0.0, 0.0);
-      if (i < n) {
-        const long vi = vbase + i * vstep;
-        if (pt.kind == GB_POT_COMPLEX) v[k] = ((const double2 *) pt.v)[vi];
-        else if (pt.kind == GB_POT_REAL) v[k].x = ((const double *) pt.v)[vi];
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < B; k++) {
-      const int i = ib + k * di;
-      if (i < n) {
-        double2 &r = base[i * es];
-        const long jx = CONTIG ? ix : (a.axis == 0 ? i : ix), jy = CONTIG ? iy : (a.axis == 0 ? iy : i);
-        const long jz = CONTIG ? i : iz;
-        r = cn_pot_with(r, v[k], jx, jy, jz, pt);
-      }
-    }
-  }
-}
-
 struct CnTile {
   long line0, o, col0;
   int nl;
@@ -647,13 +667,13 @@ __global__ void __launch_bounds__(kCnWarpThreads, 2) k_cn_warp(double2 *__restri
     const CnTile c = cn_tile_of<CONTIG>(a, t, tpo);
     double2 *sm = buf(b);
     if (pre) {
-      cn_tile_pot<CONTIG>(sm, pitch, c.nl, c.line0, c.o, c.col0, a, a.pre);
+      cn_tile_pot<CONTIG>(sm, pitch, tile_lines<false>(), c.nl, c.line0, c.o, c.col0, a, a.pre);
       __syncthreads();
     }
     for (int l = warp; l < c.nl; l += kCnWarps) cn_warp_line<CONTIG, SMAX>(sm, pitch, l, a, lane);
     if (post) {
       __syncthreads();
-      cn_tile_pot<CONTIG>(sm, pitch, c.nl, c.line0, c.o, c.col0, a, a.post);
+      cn_tile_pot<CONTIG>(sm, pitch, tile_lines<false>(), c.nl, c.line0, c.o, c.col0, a, a.post);
     }
     fence_proxy_async_smem();
     __syncthreads();
@@ -998,6 +1018,17 @@ static int launch_cn_warp(void *psi, CnAxis &a, bool contig, int axis, cudaStrea
 // Warp-cooperative line solver on (1) or off (0, the default: the
 // segment-per-warp kernel, measured faster on B200 at 192^3: 0.447 against
 // 0.487 ms per step); -1 only queries.
+// The fast kernel unrolled for the segment length of lines of n points.
+using FastKernel = void (*)(double2 *, CnAxis);
+template <bool CONTIG> static FastKernel fast_kernel(long n) {
+  const long S = (n + kSeg - 1) / kSeg;
+  if (S <= 4) return k_cn_fast<CONTIG, 4>;
+  if (S <= 8) return k_cn_fast<CONTIG, 8>;
+  if (S <= 12) return k_cn_fast<CONTIG, 12>;
+  if (S <= 16) return k_cn_fast<CONTIG, 16>;
+  return k_cn_fast<CONTIG, 0>;
+}
+
 static int g_cn_warp_on = 0;
 extern "C" int gb_cn_warp_solver(int on) {
   const int old = g_cn_warp_on;
@@ -1101,8 +1132,8 @@ extern "C" int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, co
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&smpm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
         cudaFuncAttributes fa0, fa1;
-        cudaFuncGetAttributes(&fa0, k_cn_fast<true>);
-        cudaFuncGetAttributes(&fa1, k_cn_fast<false>);
+        cudaFuncGetAttributes(&fa0, k_cn_fast<true, 0>);
+        cudaFuncGetAttributes(&fa1, k_cn_fast<false, 0>);
         const size_t st_max = fa0.sharedSizeBytes > fa1.sharedSizeBytes ? fa0.sharedSizeBytes : fa1.sharedSizeBytes;
         const long b = (long) smpm / 2 - 1024 - (long) st_max;
         budget = b > 16 * 1024 ? (size_t) b : 16 * 1024;
@@ -1114,11 +1145,12 @@ extern "C" int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, co
         if (lpc < 1) return gb__set_error(1011, "cn: line too long for a shared-memory tile");
         a.lpc = (int) lpc;
         const size_t sm = (size_t) lpc * row * 16;
-        cudaFuncSetAttribute(k_cn_fast<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
+        const FastKernel kern = fast_kernel<true>(a.n);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
         const long nb = (a.outer + lpc - 1) / lpc;
         {
           const int slot = gb__pass_begin(15 + axis);
-          k_cn_fast<true><<<(unsigned) nb, 32 * kSeg, sm, st>>>((double2 *) psi, a);
+          kern<<<(unsigned) nb, 32 * kSeg, sm, st>>>((double2 *) psi, a);
           gb__pass_end(slot);
         }
       } else {
@@ -1128,12 +1160,13 @@ extern "C" int gb_cn_step(void *psi, const gb_geom *g, const gb_cn_params *p, co
         const long lpc = largest_pow2_divisor(a.inner, cap);
         a.lpc = (int) lpc;
         const size_t sm = (size_t) lpc * a.n * 16;
-        cudaFuncSetAttribute(k_cn_fast<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
+        const FastKernel kern = fast_kernel<false>(a.n);
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) sm);
         if (a.outer > 65535) return gb__set_error(1012, "cn: outer extent above 65535");
         dim3 grid((unsigned) (a.inner / lpc), (unsigned) a.outer);
         {
           const int slot = gb__pass_begin(15 + axis);
-          k_cn_fast<false><<<grid, 32 * kSeg, sm, st>>>((double2 *) psi, a);
+          kern<<<grid, 32 * kSeg, sm, st>>>((double2 *) psi, a);
           gb__pass_end(slot);
         }
       }

@@ -7,10 +7,10 @@
 // lands outside the grid again (the reference recurses without end there);
 // this implementation uses the single plane instead.
 //
-// Each output point is one thread.  The plane of threads in a block covers a
-// (BY x BZ) tile of (y, z) and walks along x, keeping the x-1, x, x+1 values
-// in registers, so every input element is read from HBM once; the y/z
-// neighbours come from the L1-resident tile rows.  Laplacian sums keep the
+// Each output column (j, k) is one thread of a CTA whose 8 x 32 (y, z) tile
+// marches along a chunk of x planes (k_fd below): x neighbours in registers,
+// y/z neighbours from a shared-memory plane with a one-point halo, so every
+// input element is read from HBM about once.  Laplacian sums keep the
 // reference's left-to-right order
 //   (-6 c + z+ + z- + y+ + y- + x+ + x-) / h^2     (src/cgrid_diff.c:330-335).
 #include <string.h>
@@ -75,71 +75,136 @@ __device__ __forceinline__ typename Elem<T, REAL>::V fetch(const typename Elem<T
   return src[(i * a.ny + j) * a.row + k];
 }
 
-template <typename T, bool REAL>
-__global__ void k_fd(int op, typename Elem<T, REAL>::V *__restrict__ dst, const typename Elem<T, REAL>::V *__restrict__ src,
-                     FdArgs a) {
+// Tiles: a CTA of 256 threads owns a (kFdTY x kFdTZ) = (8 x 32) tile of
+// (y, z) over kFdXC consecutive x planes and marches along x.  Each thread
+// keeps its own column's x-1, x and x+1 values in registers and loads the
+// x+2 plane one step ahead; the current plane's tile and its one-point y/z
+// halo sit in a double-buffered shared-memory plane, so the y/z neighbours
+// come from shared memory and every element is read from HBM about once
+// ((kFdXC + 2) / kFdXC planes per chunk, plus the halo rows from L2).  The
+// halo of plane x is loaded one step ahead as well: warp 0 the row y-1,
+// warp 1 the row y+8, warp 2 the columns z-1 (lanes 0-7) and z+32 (lanes
+// 8-15).
+constexpr int kFdTY = 8, kFdTZ = 32, kFdXC = 16, kFdThreads = kFdTY * kFdTZ;
+
+template <typename T, bool REAL> struct FdTile {
   using E = Elem<T, REAL>;
   using V = typename E::V;
-  const long k = blockIdx.x * (long) blockDim.x + threadIdx.x;
-  const long j = blockIdx.y;
-  if (k >= a.nz) return;
+  V c, xm, xp, xq;  // planes i, i-1, i+1, i+2 of this thread's column
+  V h, hn;          // this thread's halo point of planes i and i+1 (if it owns one)
+  long hj, hk;      // halo point (y, z), hj < 0: none
+  int hy, hz;       // its place in the shared plane
+
+  __device__ void init(const V *src, const FdArgs &a, long i0, long j, long k, int ty, int tz) {
+    const long j0 = j - ty, k0 = k - tz;
+    hj = -1;
+    hk = 0;
+    hy = hz = 0;
+    if (ty == 0) {
+      hj = j0 - 1, hk = k, hy = 0, hz = tz + 1;
+    } else if (ty == 1) {
+      hj = j0 + kFdTY, hk = k, hy = kFdTY + 1, hz = tz + 1;
+    } else if (ty == 2 && tz < 2 * kFdTY) {
+      const int r = tz & (kFdTY - 1);
+      hj = j0 + r, hk = tz < kFdTY ? k0 - 1 : k0 + kFdTZ, hy = r + 1, hz = tz < kFdTY ? 0 : kFdTZ + 1;
+    }
+    // every thread of the tile loads its column, also past the far edge of
+    // the grid (a partial tile): there fetch returns the boundary value the
+    // last row/column needs as its neighbour
+    xm = fetch<T, REAL>(src, i0 - 1, j, k, a);
+    c = fetch<T, REAL>(src, i0, j, k, a);
+    xp = fetch<T, REAL>(src, i0 + 1, j, k, a);
+    xq = E::zero();
+    h = hj >= 0 ? fetch<T, REAL>(src, i0, hj, hk, a) : E::zero();
+    hn = hj >= 0 ? fetch<T, REAL>(src, i0 + 1, hj, hk, a) : E::zero();
+  }
+};
+
+template <typename T, bool REAL>
+__global__ void __launch_bounds__(kFdThreads) k_fd(int op, typename Elem<T, REAL>::V *__restrict__ dst,
+                                                   const typename Elem<T, REAL>::V *__restrict__ src, FdArgs a) {
+  using E = Elem<T, REAL>;
+  using V = typename E::V;
+  __shared__ V sm[2][kFdTY + 2][kFdTZ + 2];
+  const int tz = threadIdx.x % kFdTZ, ty = threadIdx.x / kFdTZ;
+  const long k = blockIdx.x * (long) kFdTZ + tz, j = blockIdx.y * (long) kFdTY + ty;
+  const long i0 = blockIdx.z * (long) kFdXC;
+  const long i1 = i0 + kFdXC < a.nx ? i0 + kFdXC : a.nx;
+  const bool in = k < a.nz && j < a.ny;
   const T coef = (T) a.coef;
-  V xm = fetch<T, REAL>(src, -1, j, k, a);
-  V c = fetch<T, REAL>(src, 0, j, k, a);
-  for (long i = 0; i < a.nx; i++) {
-    const V xp = fetch<T, REAL>(src, i + 1, j, k, a);
+  FdTile<T, REAL> t;
+  t.init(src, a, i0, j, k, ty, tz);
+  V *out = dst + (i0 * a.ny + j) * a.row + k;
+  const long pstride = a.ny * a.row;
+  for (long i = i0; i < i1; i++) {
+    // the loads of plane i + 2 (column and halo) go out first
+    if (i + 2 <= i1) t.xq = fetch<T, REAL>(src, i + 2, j, k, a);
+    V hq = E::zero();
+    if (t.hj >= 0 && i + 2 < i1) hq = fetch<T, REAL>(src, i + 2, t.hj, t.hk, a);
+    const int b = (int) ((i - i0) & 1);
+    sm[b][ty + 1][tz + 1] = t.c;
+    if (t.hj >= 0) sm[b][t.hy][t.hz] = t.h;
+    __syncthreads();
+    const V zp = sm[b][ty + 1][tz + 2], zm = sm[b][ty + 1][tz];
+    const V yp = sm[b][ty + 2][tz + 1], ym = sm[b][ty][tz + 1];
     V r;
     switch (op) {
       case GB_FD_LAPLACE: {
-        V s = E::scale(c, (T) -6.0);
-        s = E::add(s, fetch<T, REAL>(src, i, j, k + 1, a));
-        s = E::add(s, fetch<T, REAL>(src, i, j, k - 1, a));
-        s = E::add(s, fetch<T, REAL>(src, i, j + 1, k, a));
-        s = E::add(s, fetch<T, REAL>(src, i, j - 1, k, a));
-        s = E::add(s, xp);
-        s = E::add(s, xm);
+        V s = E::scale(t.c, (T) -6.0);
+        s = E::add(s, zp);
+        s = E::add(s, zm);
+        s = E::add(s, yp);
+        s = E::add(s, ym);
+        s = E::add(s, t.xp);
+        s = E::add(s, t.xm);
         r = E::scale(s, coef);
       } break;
-      case GB_FD_LAPLACE_X: r = E::scale(E::add(E::add(E::scale(c, (T) -2.0), xp), xm), coef); break;
-      case GB_FD_LAPLACE_Y:
-        r = E::scale(E::add(E::add(E::scale(c, (T) -2.0), fetch<T, REAL>(src, i, j + 1, k, a)),
-                            fetch<T, REAL>(src, i, j - 1, k, a)),
-                     coef);
-        break;
-      case GB_FD_LAPLACE_Z:
-        r = E::scale(E::add(E::add(E::scale(c, (T) -2.0), fetch<T, REAL>(src, i, j, k + 1, a)),
-                            fetch<T, REAL>(src, i, j, k - 1, a)),
-                     coef);
-        break;
-      case GB_FD_GRADIENT_X: r = E::scale(E::sub(xp, xm), coef); break;
-      case GB_FD_GRADIENT_Y:
-        r = E::scale(E::sub(fetch<T, REAL>(src, i, j + 1, k, a), fetch<T, REAL>(src, i, j - 1, k, a)), coef);
-        break;
-      default:
-        r = E::scale(E::sub(fetch<T, REAL>(src, i, j, k + 1, a), fetch<T, REAL>(src, i, j, k - 1, a)), coef);
-        break;
+      case GB_FD_LAPLACE_X: r = E::scale(E::add(E::add(E::scale(t.c, (T) -2.0), t.xp), t.xm), coef); break;
+      case GB_FD_LAPLACE_Y: r = E::scale(E::add(E::add(E::scale(t.c, (T) -2.0), yp), ym), coef); break;
+      case GB_FD_LAPLACE_Z: r = E::scale(E::add(E::add(E::scale(t.c, (T) -2.0), zp), zm), coef); break;
+      case GB_FD_GRADIENT_X: r = E::scale(E::sub(t.xp, t.xm), coef); break;
+      case GB_FD_GRADIENT_Y: r = E::scale(E::sub(yp, ym), coef); break;
+      default: r = E::scale(E::sub(zp, zm), coef); break;
     }
-    dst[(i * a.ny + j) * a.row + k] = r;
-    xm = c;
-    c = xp;
+    if (in) out[(i - i0) * pstride] = r;
+    t.xm = t.c;
+    t.c = t.xp;
+    t.xp = t.xq;
+    t.h = t.hn;
+    t.hn = hq;
   }
 }
 
-// sum conj(psi) * Laplacian(psi) (unscaled by 1/h^2 until the end).
+// sum conj(psi) * Laplacian(psi) over the grid, the Laplacian summed in the
+// stencil kernel's order and scaled by 1/h^2 (a.coef) before the product.
+// Same tiles and march as k_fd; each CTA writes one partial (x, y) sum,
+// reduced in a fixed order, so the result is the same from run to run.
 template <typename T>
-__global__ void __launch_bounds__(256) k_fd_kinetic(const C2<T> *__restrict__ src, FdArgs a, double2 *partial) {
-  __shared__ double sb[16];
+__global__ void __launch_bounds__(kFdThreads) k_fd_kinetic(const C2<T> *__restrict__ src, FdArgs a,
+                                                           double2 *__restrict__ partial) {
+  using E = Elem<T, false>;
+  using V = C2<T>;
+  __shared__ V sm[2][kFdTY + 2][kFdTZ + 2];
+  __shared__ double sb[2 * kFdThreads / 32];
+  const int tz = threadIdx.x % kFdTZ, ty = threadIdx.x / kFdTZ;
+  const long k = blockIdx.x * (long) kFdTZ + tz, j = blockIdx.y * (long) kFdTY + ty;
+  const long i0 = blockIdx.z * (long) kFdXC;
+  const long i1 = i0 + kFdXC < a.nx ? i0 + kFdXC : a.nx;
+  const bool in = k < a.nz && j < a.ny;
+  FdTile<T, false> t;
+  t.init(src, a, i0, j, k, ty, tz);
   double sx = 0.0, sy = 0.0;
-  const long nyz = a.ny * a.nz;
-  for (long col = blockIdx.x * (long) blockDim.x + threadIdx.x; col < nyz; col += (long) gridDim.x * blockDim.x) {
-    const long j = col / a.nz, k = col - j * a.nz;
-    C2<T> xm = fetch<T, false>(src, -1, j, k, a);
-    C2<T> c = fetch<T, false>(src, 0, j, k, a);
-    for (long i = 0; i < a.nx; i++) {
-      const C2<T> xp = fetch<T, false>(src, i + 1, j, k, a);
-      double sr = -6.0 * (double) c.x, si = -6.0 * (double) c.y;
-      C2<T> nb[6] = {fetch<T, false>(src, i, j, k + 1, a), fetch<T, false>(src, i, j, k - 1, a),
-                     fetch<T, false>(src, i, j + 1, k, a), fetch<T, false>(src, i, j - 1, k, a), xp, xm};
+  for (long i = i0; i < i1; i++) {
+    if (i + 2 <= i1) t.xq = fetch<T, false>(src, i + 2, j, k, a);
+    V hq = E::zero();
+    if (t.hj >= 0 && i + 2 < i1) hq = fetch<T, false>(src, i + 2, t.hj, t.hk, a);
+    const int b = (int) ((i - i0) & 1);
+    sm[b][ty + 1][tz + 1] = t.c;
+    if (t.hj >= 0) sm[b][t.hy][t.hz] = t.h;
+    __syncthreads();
+    if (in) {
+      const V nb[6] = {sm[b][ty + 1][tz + 2], sm[b][ty + 1][tz], sm[b][ty + 2][tz + 1], sm[b][ty][tz + 1], t.xp, t.xm};
+      double sr = -6.0 * (double) t.c.x, si = -6.0 * (double) t.c.y;
 #pragma unroll
       for (int q = 0; q < 6; q++) {
         sr += (double) nb[q].x;
@@ -148,11 +213,44 @@ __global__ void __launch_bounds__(256) k_fd_kinetic(const C2<T> *__restrict__ sr
       sr *= a.coef;
       si *= a.coef;
       // conj(c) * (sr + i si)
-      sx += (double) c.x * sr + (double) c.y * si;
-      sy += (double) c.x * si - (double) c.y * sr;
-      xm = c;
-      c = xp;
+      sx += (double) t.c.x * sr + (double) t.c.y * si;
+      sy += (double) t.c.x * si - (double) t.c.y * sr;
     }
+    t.xm = t.c;
+    t.c = t.xp;
+    t.xp = t.xq;
+    t.h = t.hn;
+    t.hn = hq;
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    sx += __shfl_down_sync(0xffffffffu, sx, off);
+    sy += __shfl_down_sync(0xffffffffu, sy, off);
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) {
+    sb[2 * w] = sx;
+    sb[2 * w + 1] = sy;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double tx = 0.0, tyy = 0.0;
+    for (int q = 0; q < kFdThreads / 32; q++) {
+      tx += sb[2 * q];
+      tyy += sb[2 * q + 1];
+    }
+    partial[((long) blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x] = make_double2(tx, tyy);
+  }
+}
+
+// Sum of n partials by one CTA of 256 threads: strided per-thread sums,
+// then a fixed shuffle tree (deterministic).
+__global__ void __launch_bounds__(256) k_finish_fd(const double2 *__restrict__ p, long n, double2 *out) {
+  __shared__ double sb[16];
+  double sx = 0.0, sy = 0.0;
+  for (long i = threadIdx.x; i < n; i += 256) {
+    sx += p[i].x;
+    sy += p[i].y;
   }
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {
@@ -171,19 +269,16 @@ __global__ void __launch_bounds__(256) k_fd_kinetic(const C2<T> *__restrict__ sr
       tx += sb[2 * q];
       ty += sb[2 * q + 1];
     }
-    partial[blockIdx.x] = make_double2(tx, ty);
+    *out = make_double2(tx, ty);
   }
 }
 
-__global__ void k_finish_fd(const double2 *__restrict__ p, int n, double2 *out) {
-  if (threadIdx.x == 0 && blockIdx.x == 0) {
-    double sx = 0.0, sy = 0.0;
-    for (int i = 0; i < n; i++) {
-      sx += p[i].x;
-      sy += p[i].y;
-    }
-    *out = make_double2(sx, sy);
-  }
+// Launch grid of the tiled stencils: (z tiles, y tiles, x chunks).
+int fd_grid(const gb_geom *g, dim3 *grid) {
+  const long gz = (g->nz + kFdTZ - 1) / kFdTZ, gy = (g->ny + kFdTY - 1) / kFdTY, gx = (g->nx + kFdXC - 1) / kFdXC;
+  if (gy > 65535 || gx > 65535) return gb__set_error(1005, "fd: grid too large for the stencil tiling");
+  *grid = dim3((unsigned) gz, (unsigned) gy, (unsigned) gx);
+  return 0;
 }
 
 }  // namespace
@@ -199,16 +294,15 @@ extern "C" int gb_fd(int op, void *dst, const void *src, const gb_geom *g, int b
   a.out_re = out_re;
   a.out_im = out_im;
   a.coef = coef;
-  if (g->ny > 65535) return gb__set_error(1005, "fd: ny above 65535");
-  const int th = g->nz >= 128 ? 128 : (g->nz >= 32 ? 32 : (int) g->nz);
-  dim3 grid((unsigned) ((g->nz + th - 1) / th), (unsigned) g->ny);
+  dim3 grid;
+  if (fd_grid(g, &grid)) return gb_last_error();
   cudaStream_t st = gb__stream();
   if (is_real) {
-    if (g->prec == GB_FP32) k_fd<float, true><<<grid, th, 0, st>>>(op, (float *) dst, (const float *) src, a);
-    else k_fd<double, true><<<grid, th, 0, st>>>(op, (double *) dst, (const double *) src, a);
+    if (g->prec == GB_FP32) k_fd<float, true><<<grid, kFdThreads, 0, st>>>(op, (float *) dst, (const float *) src, a);
+    else k_fd<double, true><<<grid, kFdThreads, 0, st>>>(op, (double *) dst, (const double *) src, a);
   } else {
-    if (g->prec == GB_FP32) k_fd<float, false><<<grid, th, 0, st>>>(op, (float2 *) dst, (const float2 *) src, a);
-    else k_fd<double, false><<<grid, th, 0, st>>>(op, (double2 *) dst, (const double2 *) src, a);
+    if (g->prec == GB_FP32) k_fd<float, false><<<grid, kFdThreads, 0, st>>>(op, (float2 *) dst, (const float2 *) src, a);
+    else k_fd<double, false><<<grid, kFdThreads, 0, st>>>(op, (double2 *) dst, (const double2 *) src, a);
   }
   GB_CHECK_LAUNCH("fd stencil");
   return 0;
@@ -225,18 +319,17 @@ extern "C" int gb_fd_kinetic_sum(const void *psi, const gb_geom *g, int bc, doub
   a.out_re = out_re;
   a.out_im = out_im;
   a.coef = inv_h2;
-  const long nyz = g->ny * g->nz;
-  long nb = (nyz + 255) / 256;
-  if (nb > 148 * 8) nb = 148 * 8;
-  if (nb < 1) nb = 1;
+  dim3 grid;
+  if (fd_grid(g, &grid)) return gb_last_error();
+  const long nb = (long) grid.x * grid.y * grid.z;
   double2 *partial = (double2 *) gb__scratch(GB_SCR_PARTIAL, sizeof(double2) * (size_t) nb);
   double2 *res = (double2 *) gb__result_slot();
   if (!partial || !res) return gb_last_error();
   cudaStream_t st = gb__stream();
-  if (g->prec == GB_FP32) k_fd_kinetic<float><<<(unsigned) nb, 256, 0, st>>>((const float2 *) psi, a, partial);
-  else k_fd_kinetic<double><<<(unsigned) nb, 256, 0, st>>>((const double2 *) psi, a, partial);
+  if (g->prec == GB_FP32) k_fd_kinetic<float><<<grid, kFdThreads, 0, st>>>((const float2 *) psi, a, partial);
+  else k_fd_kinetic<double><<<grid, kFdThreads, 0, st>>>((const double2 *) psi, a, partial);
   GB_CHECK_LAUNCH("fd kinetic");
-  k_finish_fd<<<1, 32, 0, st>>>(partial, (int) nb, res);
+  k_finish_fd<<<1, 256, 0, st>>>(partial, nb, res);
   GB_CHECK_LAUNCH("fd kinetic finish");
   double2 h;
   int rc = gb__read_result(&h, sizeof(double2));

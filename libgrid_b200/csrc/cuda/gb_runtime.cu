@@ -9,6 +9,7 @@
 // demand and are released at gb_shutdown.
 #include <math.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <cudaTypedefs.h>
@@ -21,6 +22,19 @@ static cudaStream_t g_stream = nullptr;
 static int g_err = 0;
 static char g_err_where[160] = "";
 static long g_launches = 0;
+
+// Scratch buffers replaced while a captured graph is alive stay allocated
+// (the graph may hold their address) until the last graph is freed.
+static int g_graphs_live = 0;
+static void *g_retired[64];
+static int g_nretired = 0;
+
+static void free_retired(void) {
+  if (g_nretired) cudaStreamSynchronize(g_stream);
+  for (int i = 0; i < g_nretired; i++) cudaFree(g_retired[i]);
+  g_nretired = 0;
+}
+
 static cudaEvent_t g_events[16];
 static bool g_events_made = false;
 
@@ -111,6 +125,79 @@ extern "C" int gb_synchronize(void) {
 extern "C" void *gb_stream_handle(void) { return (void *) g_stream; }
 extern "C" long gb_launch_count(void) { return g_launches; }
 
+// CUDA graphs of library calls: gb_graph_begin starts capturing the library
+// stream, so the kernels and copies the following calls issue are recorded
+// instead of run; gb_graph_end instantiates them into an executable graph
+// that gb_graph_launch replays on the stream (the same kernels with the same
+// arguments and pointers).  Calls that read results back to the host must
+// not be captured; scratch buffers are best sized by one uncaptured run of
+// the same calls first (a capture must not free device memory).
+struct GbGraph {
+  cudaGraphExec_t exec;
+  long kernels;  // launches recorded, added to gb_launch_count per replay
+};
+static long g_capture_start = 0;
+
+extern "C" int gb_graph_begin(void) {
+  if (!g_stream) return gb__set_error(1080, "graph: library not initialised");
+  const cudaError_t e = cudaStreamBeginCapture(g_stream, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return gb__set_error((int) e, "graph: begin capture");
+  }
+  g_capture_start = g_launches;
+  return 0;
+}
+
+extern "C" int gb_graph_end(void **out) {
+  *out = nullptr;
+  cudaGraph_t gr = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(g_stream, &gr);
+  const long kernels = g_launches - g_capture_start;
+  g_launches = g_capture_start;
+  if (e != cudaSuccess || !gr) {
+    if (gr) cudaGraphDestroy(gr);
+    cudaGetLastError();
+    return gb__set_error(e != cudaSuccess ? (int) e : 1081, "graph: end capture");
+  }
+  cudaGraphExec_t ex = nullptr;
+  const cudaError_t ei = cudaGraphInstantiate(&ex, gr, 0);
+  cudaGraphDestroy(gr);
+  if (ei != cudaSuccess) {
+    cudaGetLastError();
+    return gb__set_error((int) ei, "graph: instantiate");
+  }
+  GbGraph *g = (GbGraph *) malloc(sizeof(GbGraph));
+  if (!g) {
+    cudaGraphExecDestroy(ex);
+    return gb__set_error(2, "graph: host allocation");
+  }
+  g->exec = ex;
+  g->kernels = kernels;
+  g_graphs_live++;
+  *out = g;
+  return 0;
+}
+
+extern "C" int gb_graph_launch(void *h) {
+  GbGraph *g = (GbGraph *) h;
+  if (!g) return gb__set_error(1082, "graph: null handle");
+  const cudaError_t e = cudaGraphLaunch(g->exec, g_stream);
+  if (e != cudaSuccess) return gb__set_error((int) e, "graph: launch");
+  g_launches += g->kernels;
+  return 0;
+}
+
+extern "C" int gb_graph_free(void *h) {
+  GbGraph *g = (GbGraph *) h;
+  if (g) {
+    cudaGraphExecDestroy(g->exec);
+    free(g);
+    if (--g_graphs_live == 0) free_retired();
+  }
+  return 0;
+}
+
 extern "C" void *gb_device_alloc(size_t bytes) {
   void *p = nullptr;
   cudaError_t e = cudaMalloc(&p, bytes ? bytes : 16);
@@ -191,8 +278,12 @@ void *gb__scratch(int slot, size_t bytes) {
   Scratch &s = g_scratch[slot];
   if (s.bytes >= bytes && s.p) return s.p;
   if (s.p) {
-    cudaStreamSynchronize(g_stream);
-    cudaFree(s.p);
+    if (g_graphs_live > 0 && g_nretired < 64) {
+      g_retired[g_nretired++] = s.p;
+    } else {
+      cudaStreamSynchronize(g_stream);
+      cudaFree(s.p);
+    }
   }
   s.p = nullptr;
   s.bytes = 0;

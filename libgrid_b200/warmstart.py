@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import sys
 import time
 
 import numpy as np
@@ -104,6 +105,14 @@ def _bind(lib):
     lib.gb_d2d.restype = I
     lib.gb_d2d.argtypes = [V, V, C.c_size_t]
     lib.gb_synchronize.restype = I
+    lib.gb_graph_begin.restype = I
+    lib.gb_graph_begin.argtypes = []
+    lib.gb_graph_end.restype = I
+    lib.gb_graph_end.argtypes = [C.POINTER(V)]
+    lib.gb_graph_launch.restype = I
+    lib.gb_graph_launch.argtypes = [V]
+    lib.gb_graph_free.restype = I
+    lib.gb_graph_free.argtypes = [V]
     lib.rgrid_product.restype = None
     lib.rgrid_product.argtypes = [V, V, V]
 
@@ -148,6 +157,7 @@ class DeviceUNet:
         for b in (self._m, self._v, self._g):
             _ok(self.lib.gb_unet_fill(b, off, 0.0), "fill")
         self.t = 0
+        self._graphs = {}
         # activations: a conv with two sources reads them as one contiguous block
         self.vol = [(n >> l) ** 3 for l in range(4)]
         place, off = {}, 0
@@ -173,6 +183,9 @@ class DeviceUNet:
         return p
 
     def free(self):
+        for h in self.__dict__.get("_graphs", {}).values():
+            self.lib.gb_graph_free(h)
+        self._graphs = {}
         for b in (self._p, self._pb, self._m, self._v, self._g, self._a, self._ga, self._tgt):
             self.lib.gb_device_free(b)
 
@@ -271,6 +284,60 @@ class DeviceUNet:
         c1, c2 = 1.0 / (1.0 - b1 ** self.t), 1.0 / (1.0 - b2 ** self.t)
         _ok(self.lib.gb_unet_adam(self._p, self._pb, self._m, self._v, self._g, self.nparam, lr, b1, b2, eps, c1, c2),
             "adam")
+
+    def _graph(self, key, build):
+        """The CUDA graph of the calls `build` makes, captured on first use
+        (after one uncaptured run that sizes the library's scratch buffers)
+        and cached under key."""
+        g = self._graphs.get(key)
+        if g is None:
+            build()
+            _ok(self.lib.gb_synchronize(), "sync")
+            _ok(self.lib.gb_graph_begin(), "graph begin")
+            try:
+                build()
+            finally:
+                h = C.c_void_p()
+                rc = self.lib.gb_graph_end(C.byref(h))
+            _ok(rc, "graph end")
+            g = self._graphs[key] = h
+        return g
+
+    def train_sample(self, x_dptr, y_dptr, scale):
+        """Forward, MSE gradient (times scale) and backward of one sample
+        whose input and target sit in device memory: two device copies into
+        the network's input and target slots, then one graph launch (the
+        captured forward, loss gradient and backward; weight gradients
+        accumulate)."""
+        g = self._graphs.get(("train", float(scale)))
+        if g is None:
+            raise RuntimeError("train_sample: no graph for loss scale %r (call prepare_training first)" % scale)
+        _ok(self.lib.gb_d2d(self._act("in"), x_dptr, 4 * self.chan["in"] * self.vol[0]), "d2d")
+        _ok(self.lib.gb_d2d(self._tgt, y_dptr, 4 * self.vol[0]), "d2d")
+        _ok(self.lib.gb_graph_launch(g), "graph launch")
+
+    def prepare_training(self, scales):
+        """Capture the training graphs of the given loss scales before the
+        first sample (their sizing runs' gradients are cleared)."""
+        for sc in scales:
+            def build(sc=sc):
+                self.forward()
+                self.loss_grad(self._tgt, sc)
+                self.backward()
+
+            self._graph(("train", float(sc)), build)
+        _ok(self.lib.gb_unet_fill(self._g, self.nparam, 0.0), "fill")
+
+    def forward_graph(self):
+        """Forward of the input already in the activation slab, as one
+        graph launch."""
+        _ok(self.lib.gb_graph_launch(self._graph(("fwd",), self.forward)), "graph launch")
+
+    def infer_device(self, x_dptr):
+        """Forward of one device-resident input (a graph launch); the output
+        stays in the activation slab ("out")."""
+        _ok(self.lib.gb_d2d(self._act("in"), x_dptr, 4 * self.chan["in"] * self.vol[0]), "d2d")
+        _ok(self.lib.gb_graph_launch(self._graph(("fwd",), self.forward)), "graph launch")
 
     def predict(self, x: np.ndarray) -> np.ndarray:
         self.set_input(x)
@@ -555,21 +622,20 @@ def train(net: DeviceUNet, ds: DeviceSet, epochs=60, batch=8, lr=2e-3, seed=0, l
     nb, vol = ds.count, net.vol[0]
     rng = np.random.default_rng(seed)
     last = float("nan")
+    # one captured graph (forward, loss gradient, backward) per minibatch
+    # length: the full batch and the remainder
+    net.prepare_training(sorted({2.0 / (vol * min(batch, nb - b0)) for b0 in range(0, nb, batch)}))
     for ep in range(epochs):
         order = rng.permutation(nb)
         for b0 in range(0, nb, batch):
             idx = order[b0 : b0 + batch]
             for i in idx:
-                net.set_input_device(ds.xp(i))
-                net.forward()
-                net.loss_grad(ds.yp(i), 2.0 / (vol * len(idx)))
-                net.backward()
+                net.train_sample(ds.xp(i), ds.yp(i), 2.0 / (vol * len(idx)))
             net.adam(lr * (0.5 * (1 + math.cos(math.pi * ep / epochs)) * 0.95 + 0.05))
         if log is not None or ep == epochs - 1:
             errs = []
             for i in range(min(nb, monitor)):
-                net.set_input_device(ds.xp(i))
-                net.forward()
+                net.infer_device(ds.xp(i))
                 y = np.empty(vol, np.float32)
                 _ok(net.lib.gb_d2h(y.ctypes.data, ds.yp(i), y.nbytes), "d2h")
                 errs.append(float(((net.activation("out")[0].ravel() - y) ** 2).mean()))
@@ -606,7 +672,7 @@ def evaluate(api, net: DeviceUNet, seeds, n=32, step=0.1, tol=1e-8, ref_tol=1e-1
             t_tf = time.perf_counter() - t0
             t0 = time.perf_counter()
             _, s = r.tf_features(net._act("in"))
-            net.forward()
+            net.forward_graph()
             r.set_guess(net._act("out"), s, 1e-6)
             e_n, st_n = r.relax(tol=tol)
             _ok(lib.gb_synchronize(), "sync")
@@ -621,23 +687,24 @@ def evaluate(api, net: DeviceUNet, seeds, n=32, step=0.1, tol=1e-8, ref_tol=1e-1
 
 
 def time_training_step(net: DeviceUNet, ds: DeviceSet, reps: int = 10):
-    """(forward ms, forward + loss + backward ms) per sample, CUDA events on
-    the library stream, after 3 warm-up repetitions."""
+    """(forward ms, forward + loss + backward ms) per sample as training and
+    inference run them (captured graphs replayed on the library stream),
+    CUDA events after 3 warm-up repetitions."""
     lib = net.lib
     lib.gb_event_record.restype = C.c_int
     lib.gb_event_record.argtypes = [C.c_int]
     lib.gb_event_elapsed_ms.restype = C.c_float
     lib.gb_event_elapsed_ms.argtypes = [C.c_int, C.c_int]
-    net.set_input_device(ds.xp(0))
+    net.prepare_training([2.0 / net.vol[0]])
     out = []
     for with_bwd in (False, True):
         for r in range(reps + 3):
             if r == 3:
                 _ok(lib.gb_event_record(0), "event")
-            net.forward()
             if with_bwd:
-                net.loss_grad(ds.yp(0))
-                net.backward()
+                net.train_sample(ds.xp(0), ds.yp(0), 2.0 / net.vol[0])
+            else:
+                net.infer_device(ds.xp(0))
         _ok(lib.gb_event_record(1), "event")
         _ok(lib.gb_synchronize(), "sync")
         out.append(lib.gb_event_elapsed_ms(0, 1) / reps)
@@ -664,20 +731,30 @@ def main(argv=None):
     ap.add_argument("--step", type=float, default=0.1)
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--quiet", action="store_true", help="no progress lines on stderr")
     a = ap.parse_args(argv)
+
+    def note(msg):
+        if not a.quiet:
+            print("[warmstart %.0fs] %s" % (time.perf_counter() - t_start, msg), file=sys.stderr, flush=True)
+
+    t_start = time.perf_counter()
     api = libgrid_b200.load()
     api.lib.cuda_enable(b"\x01", 0, None)
     t0 = time.perf_counter()
     ds, meta = make_dataset(api, range(1000, 1000 + a.train), a.n, a.step, tol=a.tol)
     t_data = time.perf_counter() - t0
+    note("%d ground states in %.1f s (mean %.0f steps)" % (a.train, t_data, np.mean([m["steps"] for m in meta])))
     net = DeviceUNet(api, a.n, cin=3, seed=0)
     try:
         t0 = time.perf_counter()
-        loss = train(net, ds, epochs=a.epochs, batch=a.batch, lr=a.lr)
+        loss = train(net, ds, epochs=a.epochs, batch=a.batch, lr=a.lr,
+                     log=None if a.quiet else (lambda ep, l: note("epoch %d loss %.3e" % (ep, l))))
         api.lib.gb_synchronize()
         t_train = time.perf_counter() - t0
         step_ms = time_training_step(net, ds)
         ds.free()
+        note("trained in %.1f s" % t_train)
         rows = evaluate(api, net, range(5000, 5000 + a.test), a.n, a.step, tol=a.tol)
     finally:
         net.free()
