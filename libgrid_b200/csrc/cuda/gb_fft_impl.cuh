@@ -648,8 +648,11 @@ int pipe_enabled();
 
 template <int N> __host__ __device__ constexpr int pipe_rows() { return N < 256 ? N : 256; }
 
+#ifndef GB_PIPE_MINB
+#define GB_PIPE_MINB 3
+#endif
 template <typename T, int N, int BZ, int... Ops>
-__global__ void __launch_bounds__((N / Sched<N>::P) * BZ, sizeof(T) == 8 ? 3 : 3)
+__global__ void __launch_bounds__((N / Sched<N>::P) * BZ, GB_PIPE_MINB)
     k_pass_strided_pipe(C2<T> *__restrict__ dst, unsigned inner, unsigned ncb, unsigned ntiles, PassArgs a,
                         const __grid_constant__ CUtensorMap tmap) {
   using T2 = C2<T>;

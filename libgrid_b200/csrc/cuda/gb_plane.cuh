@@ -24,6 +24,15 @@ namespace gbfft {
 
 template <int AX, int... Ops> struct Stage {};
 
+// Resident CTAs per SM the FP64 chains are compiled for (register caps of
+// 128 threads x 168 / 128 registers); overridable for tuning builds.
+#ifndef GB_CHAIN_POT_MINB
+#define GB_CHAIN_POT_MINB 3
+#endif
+#ifndef GB_CHAIN_MINB64
+#define GB_CHAIN_MINB64 4
+#endif
+
 template <typename T, int N> struct ChainCfg {
   static constexpr int P = Sched<N>::P;
   static constexpr int TL = N / P;
@@ -34,7 +43,7 @@ template <typename T, int N> struct ChainCfg {
   static constexpr int LINE = N + (N >> SH);
   static constexpr int SM_Z = W * LINE, SM_Y = N * W;  // exchange elements
   static constexpr int SM_X = SM_Z > SM_Y ? SM_Z : SM_Y;
-  static constexpr int MINB = sizeof(T) == 8 ? 4 : 3;
+  static constexpr int MINB = sizeof(T) == 8 ? GB_CHAIN_MINB64 : 3;
 };
 
 struct ChainArgs {
@@ -108,7 +117,7 @@ __device__ __forceinline__ void chain_tile(Stage<AX, Ops...>, C2<T> *__restrict_
 // the potential op (two transforms and the phase) gets 3 in FP64, so it
 // does not spill.
 template <typename T, int N, class... Stages> constexpr int chain_minb() {
-  return (sizeof(T) == 8 && (stage_has_pot(Stages{}) || ...)) ? 3 : ChainCfg<T, N>::MINB;
+  return (sizeof(T) == 8 && (stage_has_pot(Stages{}) || ...)) ? GB_CHAIN_POT_MINB : ChainCfg<T, N>::MINB;
 }
 
 template <typename T, int N, class... Stages>
