@@ -78,7 +78,7 @@ __device__ __forceinline__ typename Elem<T, REAL>::V fetch(const typename Elem<T
 // Tiles: a CTA of 256 threads owns a (kFdTY x kFdTZ) = (8 x 32) tile of
 // (y, z) over kFdXC consecutive x planes and marches along x.  Each thread
 // keeps its own column's x-1, x and x+1 values in registers and loads the
-// x+2 plane one step ahead; the current plane's tile and its one-point y/z
+// x+4 plane four steps ahead; the current plane's tile and its one-point y/z
 // halo sit in a double-buffered shared-memory plane, so the y/z neighbours
 // come from shared memory and every element is read from HBM about once
 // ((kFdXC + 2) / kFdXC planes per chunk, plus the halo rows from L2).  The
@@ -86,20 +86,22 @@ __device__ __forceinline__ typename Elem<T, REAL>::V fetch(const typename Elem<T
 // warp 1 the row y+8, warp 2 the columns z-1 (lanes 0-7) and z+32 (lanes
 // 8-15).
 constexpr int kFdTY = 8, kFdTZ = 32, kFdXC = 16, kFdThreads = kFdTY * kFdTZ;
+constexpr int kFdPD = 4;  // planes loaded ahead of the one being computed
 
 template <typename T, bool REAL> struct FdTile {
   using E = Elem<T, REAL>;
   using V = typename E::V;
-  V c, xm, xp, xq;  // planes i, i-1, i+1, i+2 of this thread's column
-  V h, hn;          // this thread's halo point of planes i and i+1 (if it owns one)
-  long hj, hk;      // halo point (y, z), hj < 0: none
-  int hy, hz;       // its place in the shared plane
+  V col[kFdPD + 2];  // this thread's column, planes i-1, i, ..., i+kFdPD
+  V hal[kFdPD + 1];  // its halo point (if it owns one), planes i, ..., i+kFdPD
+  long hj, hk;       // halo point (y, z); may lie outside the grid
+  int hy, hz;        // its place in the shared plane
+  bool has_h;        // whether this thread owns a halo point
 
   __device__ void init(const V *src, const FdArgs &a, long i0, long j, long k, int ty, int tz) {
     const long j0 = j - ty, k0 = k - tz;
-    hj = -1;
-    hk = 0;
+    hj = hk = 0;
     hy = hz = 0;
+    has_h = ty < 2 || (ty == 2 && tz < 2 * kFdTY);
     if (ty == 0) {
       hj = j0 - 1, hk = k, hy = 0, hz = tz + 1;
     } else if (ty == 1) {
@@ -111,17 +113,30 @@ template <typename T, bool REAL> struct FdTile {
     // every thread of the tile loads its column, also past the far edge of
     // the grid (a partial tile): there fetch returns the boundary value the
     // last row/column needs as its neighbour
-    xm = fetch<T, REAL>(src, i0 - 1, j, k, a);
-    c = fetch<T, REAL>(src, i0, j, k, a);
-    xp = fetch<T, REAL>(src, i0 + 1, j, k, a);
-    xq = E::zero();
-    h = hj >= 0 ? fetch<T, REAL>(src, i0, hj, hk, a) : E::zero();
-    hn = hj >= 0 ? fetch<T, REAL>(src, i0 + 1, hj, hk, a) : E::zero();
+#pragma unroll
+    for (int q = 0; q <= kFdPD; q++) col[q] = fetch<T, REAL>(src, i0 - 1 + q, j, k, a);
+    col[kFdPD + 1] = E::zero();
+#pragma unroll
+    for (int q = 0; q < kFdPD; q++) hal[q] = has_h ? fetch<T, REAL>(src, i0 + q, hj, hk, a) : E::zero();
+    hal[kFdPD] = E::zero();
+  }
+
+  // loads of plane i + kFdPD (column and halo), issued at the top of step i
+  __device__ __forceinline__ void prefetch(const V *src, const FdArgs &a, long i, long i1, long j, long k) {
+    if (i + kFdPD <= i1) col[kFdPD + 1] = fetch<T, REAL>(src, i + kFdPD, j, k, a);
+    if (has_h && i + kFdPD < i1) hal[kFdPD] = fetch<T, REAL>(src, i + kFdPD, hj, hk, a);
+  }
+
+  __device__ __forceinline__ void shift() {
+#pragma unroll
+    for (int q = 0; q <= kFdPD; q++) col[q] = col[q + 1];
+#pragma unroll
+    for (int q = 0; q < kFdPD; q++) hal[q] = hal[q + 1];
   }
 };
 
 template <typename T, bool REAL>
-__global__ void __launch_bounds__(kFdThreads) k_fd(int op, typename Elem<T, REAL>::V *__restrict__ dst,
+__global__ void __launch_bounds__(kFdThreads, 3) k_fd(int op, typename Elem<T, REAL>::V *__restrict__ dst,
                                                    const typename Elem<T, REAL>::V *__restrict__ src, FdArgs a) {
   using E = Elem<T, REAL>;
   using V = typename E::V;
@@ -137,41 +152,35 @@ __global__ void __launch_bounds__(kFdThreads) k_fd(int op, typename Elem<T, REAL
   V *out = dst + (i0 * a.ny + j) * a.row + k;
   const long pstride = a.ny * a.row;
   for (long i = i0; i < i1; i++) {
-    // the loads of plane i + 2 (column and halo) go out first
-    if (i + 2 <= i1) t.xq = fetch<T, REAL>(src, i + 2, j, k, a);
-    V hq = E::zero();
-    if (t.hj >= 0 && i + 2 < i1) hq = fetch<T, REAL>(src, i + 2, t.hj, t.hk, a);
+    t.prefetch(src, a, i, i1, j, k);
     const int b = (int) ((i - i0) & 1);
-    sm[b][ty + 1][tz + 1] = t.c;
-    if (t.hj >= 0) sm[b][t.hy][t.hz] = t.h;
+    const V c = t.col[1], xm = t.col[0], xp = t.col[2];
+    sm[b][ty + 1][tz + 1] = c;
+    if (t.has_h) sm[b][t.hy][t.hz] = t.hal[0];
     __syncthreads();
     const V zp = sm[b][ty + 1][tz + 2], zm = sm[b][ty + 1][tz];
     const V yp = sm[b][ty + 2][tz + 1], ym = sm[b][ty][tz + 1];
     V r;
     switch (op) {
       case GB_FD_LAPLACE: {
-        V s = E::scale(t.c, (T) -6.0);
+        V s = E::scale(c, (T) -6.0);
         s = E::add(s, zp);
         s = E::add(s, zm);
         s = E::add(s, yp);
         s = E::add(s, ym);
-        s = E::add(s, t.xp);
-        s = E::add(s, t.xm);
+        s = E::add(s, xp);
+        s = E::add(s, xm);
         r = E::scale(s, coef);
       } break;
-      case GB_FD_LAPLACE_X: r = E::scale(E::add(E::add(E::scale(t.c, (T) -2.0), t.xp), t.xm), coef); break;
-      case GB_FD_LAPLACE_Y: r = E::scale(E::add(E::add(E::scale(t.c, (T) -2.0), yp), ym), coef); break;
-      case GB_FD_LAPLACE_Z: r = E::scale(E::add(E::add(E::scale(t.c, (T) -2.0), zp), zm), coef); break;
-      case GB_FD_GRADIENT_X: r = E::scale(E::sub(t.xp, t.xm), coef); break;
+      case GB_FD_LAPLACE_X: r = E::scale(E::add(E::add(E::scale(c, (T) -2.0), xp), xm), coef); break;
+      case GB_FD_LAPLACE_Y: r = E::scale(E::add(E::add(E::scale(c, (T) -2.0), yp), ym), coef); break;
+      case GB_FD_LAPLACE_Z: r = E::scale(E::add(E::add(E::scale(c, (T) -2.0), zp), zm), coef); break;
+      case GB_FD_GRADIENT_X: r = E::scale(E::sub(xp, xm), coef); break;
       case GB_FD_GRADIENT_Y: r = E::scale(E::sub(yp, ym), coef); break;
       default: r = E::scale(E::sub(zp, zm), coef); break;
     }
     if (in) out[(i - i0) * pstride] = r;
-    t.xm = t.c;
-    t.c = t.xp;
-    t.xp = t.xq;
-    t.h = t.hn;
-    t.hn = hq;
+    t.shift();
   }
 }
 
@@ -180,7 +189,7 @@ __global__ void __launch_bounds__(kFdThreads) k_fd(int op, typename Elem<T, REAL
 // Same tiles and march as k_fd; each CTA writes one partial (x, y) sum,
 // reduced in a fixed order, so the result is the same from run to run.
 template <typename T>
-__global__ void __launch_bounds__(kFdThreads) k_fd_kinetic(const C2<T> *__restrict__ src, FdArgs a,
+__global__ void __launch_bounds__(kFdThreads, 3) k_fd_kinetic(const C2<T> *__restrict__ src, FdArgs a,
                                                            double2 *__restrict__ partial) {
   using E = Elem<T, false>;
   using V = C2<T>;
@@ -195,16 +204,16 @@ __global__ void __launch_bounds__(kFdThreads) k_fd_kinetic(const C2<T> *__restri
   t.init(src, a, i0, j, k, ty, tz);
   double sx = 0.0, sy = 0.0;
   for (long i = i0; i < i1; i++) {
-    if (i + 2 <= i1) t.xq = fetch<T, false>(src, i + 2, j, k, a);
-    V hq = E::zero();
-    if (t.hj >= 0 && i + 2 < i1) hq = fetch<T, false>(src, i + 2, t.hj, t.hk, a);
+    t.prefetch(src, a, i, i1, j, k);
     const int b = (int) ((i - i0) & 1);
-    sm[b][ty + 1][tz + 1] = t.c;
-    if (t.hj >= 0) sm[b][t.hy][t.hz] = t.h;
+    const V c = t.col[1];
+    sm[b][ty + 1][tz + 1] = c;
+    if (t.has_h) sm[b][t.hy][t.hz] = t.hal[0];
     __syncthreads();
     if (in) {
-      const V nb[6] = {sm[b][ty + 1][tz + 2], sm[b][ty + 1][tz], sm[b][ty + 2][tz + 1], sm[b][ty][tz + 1], t.xp, t.xm};
-      double sr = -6.0 * (double) t.c.x, si = -6.0 * (double) t.c.y;
+      const V nb[6] = {sm[b][ty + 1][tz + 2], sm[b][ty + 1][tz], sm[b][ty + 2][tz + 1], sm[b][ty][tz + 1], t.col[2],
+                       t.col[0]};
+      double sr = -6.0 * (double) c.x, si = -6.0 * (double) c.y;
 #pragma unroll
       for (int q = 0; q < 6; q++) {
         sr += (double) nb[q].x;
@@ -213,14 +222,10 @@ __global__ void __launch_bounds__(kFdThreads) k_fd_kinetic(const C2<T> *__restri
       sr *= a.coef;
       si *= a.coef;
       // conj(c) * (sr + i si)
-      sx += (double) t.c.x * sr + (double) t.c.y * si;
-      sy += (double) t.c.x * si - (double) t.c.y * sr;
+      sx += (double) c.x * sr + (double) c.y * si;
+      sy += (double) c.x * si - (double) c.y * sr;
     }
-    t.xm = t.c;
-    t.c = t.xp;
-    t.xp = t.xq;
-    t.h = t.hn;
-    t.hn = hq;
+    t.shift();
   }
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {

@@ -27,8 +27,10 @@
 //   gw[co][ci][t] += sum_q gy[co][q] x[ci][q + off(t)].
 // A CTA stages gy of a voxel block (bf16, [co][q]) and three x-shifted copies
 // of the x halo block (dx = -1, 0, 1, bf16, [ci][row][x]), so every tap's
-// operand rows are 16-byte aligned for ldmatrix.  Warps split the taps; the
-// partial sums of each block go to scratch and a fixed-order pass adds them
+// operand rows are 16-byte aligned for ldmatrix.  Warps split the taps.  A
+// resident wave of CTAs loops over the voxel blocks (CTA b takes blocks b,
+// b + grid, ...) with the accumulators in registers; each CTA's partial
+// sums go to scratch and a fixed-order pass (one warp per weight) adds them
 // to gw (deterministic, no atomics).
 //
 // Operands are rounded to bf16 (round to nearest even) and accumulated in
@@ -110,6 +112,7 @@ __device__ __forceinline__ uint32_t pack_bf16x2(float a, float b) {
 constexpr int kTcThreads = 256;  // two warpgroups: staging, epilogue
 constexpr int kTcM = 128;
 constexpr int kTcN = 16;  // output channels per CTA
+constexpr int kStageG = 4;  // staging items whose loads are issued together
 
 struct TcConv {
   const float *x;     // [cx][d][h][w] FP32
@@ -159,31 +162,47 @@ __global__ void __launch_bounds__(kTcThreads) k_conv3_tc(TcConv p) {
   const int nb16 = p.nmma * 2 * (kTcN / 8) * 8;  // 16-byte units
   const uint4 *bsrc = p.bp + (size_t) blockIdx.y * nb16;
   for (int i = tid; i < nb16; i += kTcThreads) ((uint4 *) b_sm)[i] = bsrc[i];
-  // A operand: the zero-padded halo block, bf16 channel-chunk planes; one
-  // staged row (chunk c, zs, ys) per warp at a time, lanes along x, the
-  // eight channel loads of a position issued together
-  const int rows_per_plane = (p.tz + 2) * (p.ty + 2);
-  for (int row = warp; row < p.c8 * rows_per_plane; row += kTcThreads / 32) {
-    const int c = row / rows_per_plane, rr = row - c * rows_per_plane;
-    const int zs = rr / (p.ty + 2), ys = rr - zs * (p.ty + 2);
-    const int z = z0 + zs - 1, y = y0 + ys - 1;
-    const bool inrow = z >= 0 && z < p.d && y >= 0 && y < p.h;
-    const long vrow = ((long) z * p.h + y) * p.w;
-    uint4 *prow = (uint4 *) (a_sm + (size_t) c * plane_bytes) + p.guard + zs * p.sz + ys * p.sy;
-    for (int xs = lane; xs < p.sy; xs += 32) {
-      const int x = xs - 1;
-      float v[8];
+  // A operand: the zero-padded halo block, bf16 channel-chunk planes.  The
+  // work items are (staged row, 32-position chunk of the row), lanes along
+  // x; a warp takes every 8th item and issues the loads of kStageG items
+  // (8 channels each) before packing and storing any of them, so that many
+  // loads are in flight per lane instead of one row chunk at a time.
+  {
+    constexpr int G = kStageG, NW = kTcThreads / 32;
+    const int rows_per_plane = (p.tz + 2) * (p.ty + 2);
+    const int xch = (p.sy + 31) >> 5;
+    const int nitems = p.c8 * rows_per_plane * xch;
+    for (int i0 = warp; i0 < nitems; i0 += G * NW) {
+      float v[G][8];
+      int dpos[G];
 #pragma unroll
-      for (int e = 0; e < 8; e++) v[e] = 0.f;
-      if (inrow && x >= 0 && x < p.w) {
+      for (int g = 0; g < G; g++) {
+        const int it = i0 + g * NW;
+        dpos[g] = -1;
 #pragma unroll
-        for (int e = 0; e < 8; e++) {
-          const int ch = c * 8 + e;
-          if (ch < p.cx) v[e] = __ldg(p.x + (size_t) ch * vol + vrow + x);
+        for (int e = 0; e < 8; e++) v[g][e] = 0.f;
+        if (it < nitems) {
+          const int row = it / xch, xc = it - row * xch;
+          const int c = row / rows_per_plane, rr = row - c * rows_per_plane;
+          const int zs = rr / (p.ty + 2), ys = rr - zs * (p.ty + 2);
+          const int xs = xc * 32 + lane;
+          if (xs < p.sy) {
+            dpos[g] = c * p.plane_rows + p.guard + zs * p.sz + ys * p.sy + xs;
+            const int z = z0 + zs - 1, y = y0 + ys - 1, x = xs - 1;
+            if (z >= 0 && z < p.d && y >= 0 && y < p.h && x >= 0 && x < p.w) {
+              const float *src = p.x + ((long) z * p.h + y) * p.w + x;
+#pragma unroll
+              for (int e = 0; e < 8; e++)
+                if (c * 8 + e < p.cx) v[g][e] = __ldg(src + (size_t) (c * 8 + e) * vol);
+            }
+          }
         }
       }
-      prow[xs] = make_uint4(pack_bf16x2(v[0], v[1]), pack_bf16x2(v[2], v[3]), pack_bf16x2(v[4], v[5]),
-                            pack_bf16x2(v[6], v[7]));
+#pragma unroll
+      for (int g = 0; g < G; g++)
+        if (dpos[g] >= 0)
+          ((uint4 *) a_sm)[dpos[g]] = make_uint4(pack_bf16x2(v[g][0], v[g][1]), pack_bf16x2(v[g][2], v[g][3]),
+                                                 pack_bf16x2(v[g][4], v[g][5]), pack_bf16x2(v[g][6], v[g][7]));
     }
   }
   fence_proxy_async_smem();
@@ -294,10 +313,11 @@ __global__ void k_pack_b(const __nv_bfloat16 *__restrict__ w, __nv_bfloat16 *__r
 constexpr int kWgThreads = 256;  // 8 warps, warp w takes taps w, w + 8, ...
 constexpr int kWgTaps = 4;       // ceil(27 / 8)
 constexpr int kWgCo16 = 4;       // up to 64 output channels
+constexpr int kWgXB = 8;         // staging loads issued together per lane
 
 struct TcWgrad {
   const float *x, *gy;
-  float *part;  // [block][cz][co][8][27] partial sums; bias partials after them
+  float *part;  // [cta][cz][co][8][27] partial sums; bias partials [cta][co] after them
   int cin, cout, d, h, w;
   int tz, ty;
   int co16;     // output channels / 16, rounded up
@@ -333,24 +353,47 @@ __global__ void __launch_bounds__(kWgThreads) k_conv3_wgrad_mma(TcWgrad p) {
   __nv_bfloat16 *xs = gys + (size_t) 16 * p.co16 * p.qp;                   // [3][8][rows][w]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int nby = p.h / p.ty;
-  const int blk = blockIdx.x, cz = blockIdx.y;
-  const int z0 = (blk / nby) * p.tz, y0 = (blk % nby) * p.ty;
+  const int cz = blockIdx.y;
   const long vol = (long) p.d * p.h * p.w;
   const int nq = p.tz * p.ty * p.w;
+  // accumulators persist over the voxel blocks blockIdx.x, + gridDim.x, ...
+  float acc[kWgTaps][kWgCo16][4];
+#pragma unroll
+  for (int a = 0; a < kWgTaps; a++)
+#pragma unroll
+    for (int b = 0; b < kWgCo16; b++)
+#pragma unroll
+      for (int c = 0; c < 4; c++) acc[a][b][c] = 0.f;
+  float bacc = 0.f;  // bias partial of output channel tid (tid < cout)
+  for (int blk = blockIdx.x; blk < p.nblk; blk += gridDim.x) {
+  const int z0 = (blk / nby) * p.tz, y0 = (blk % nby) * p.ty;
   // gy of the block, bf16 [co][q] (rows past cout are zero); one row
   // (co, zi, yi) per warp at a time, lanes along x; the warp also sums the
   // row (FP32, unrounded) for the bias gradient
   const int bz = p.tz * p.ty;
   __shared__ float brow[64 * 16];  // [co][zi ty + yi] row sums (co < 64, tz ty <= 16)
+  // (the loads of up to kWgXB 32-wide chunks of a row are issued before
+  // their stores, and the row sum adds the chunks in x order per lane)
   for (int row = warp; row < 16 * p.co16 * bz; row += kWgThreads / 32) {
     const int co = row / bz, rr = row - co * bz, zi = rr / p.ty, yi = rr - zi * p.ty;
     const float *src = p.gy + (size_t) co * vol + ((long) (z0 + zi) * p.h + (y0 + yi)) * p.w;
     __nv_bfloat16 *dst = gys + (size_t) co * p.qp + (size_t) rr * p.w;
     float s = 0.f;
-    for (int x = lane; x < p.w; x += 32) {
-      const float v = co < p.cout ? __ldg(src + x) : 0.f;
-      dst[x] = __float2bfloat16_rn(v);
-      s += v;
+    for (int xb = 0; xb < p.w; xb += 32 * kWgXB) {
+      float v[kWgXB];
+#pragma unroll
+      for (int j = 0; j < kWgXB; j++) {
+        const int x = xb + 32 * j + lane;
+        v[j] = (co < p.cout && x < p.w) ? __ldg(src + x) : 0.f;
+      }
+#pragma unroll
+      for (int j = 0; j < kWgXB; j++) {
+        const int x = xb + 32 * j + lane;
+        if (x < p.w) {
+          dst[x] = __float2bfloat16_rn(v[j]);
+          s += v[j];
+        }
+      }
     }
     if (p.dobias && cz == 0 && co < p.cout) {
       for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -359,36 +402,50 @@ __global__ void __launch_bounds__(kWgThreads) k_conv3_wgrad_mma(TcWgrad p) {
   }
   // three x-shifted copies of the x halo block for this chunk of 8 channels:
   // copy cp holds x[. + cp - 1]; each input value is loaded once and stored
-  // into the three copies
+  // into the three copies.  Items (row, 32-wide chunk), every 8th to a warp,
+  // kWgXB items' loads issued together.
   const int srows = (p.tz + 2) * (p.ty + 2);
-  for (int row = warp; row < 8 * srows; row += kWgThreads / 32) {
-    const int c = row / srows, r = row - c * srows;
-    const int zs = r / (p.ty + 2), ys = r - zs * (p.ty + 2);
-    const int z = z0 + zs - 1, y = y0 + ys - 1, ci = cz * 8 + c;
-    const bool inrow = ci < p.cin && z >= 0 && z < p.d && y >= 0 && y < p.h;
-    const float *src = p.x + (size_t) ci * vol + ((long) z * p.h + y) * p.w;
-    __nv_bfloat16 *d0 = xs + (size_t) c * p.xpp + (size_t) r * p.xrp;
-    __nv_bfloat16 *d1 = d0 + p.xcp, *d2 = d0 + 2 * (size_t) p.xcp;
-    const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
-    for (int x = lane; x < p.w; x += 32) {
-      const __nv_bfloat16 v = __float2bfloat16_rn(inrow ? __ldg(src + x) : 0.f);
-      d1[x] = v;
-      if (x + 1 < p.w) d0[x + 1] = v;
-      if (x >= 1) d2[x - 1] = v;
+  const int xch = (p.w + 31) >> 5;
+  const int nitems = 8 * srows * xch;
+  const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
+  for (int i0 = warp; i0 < nitems; i0 += kWgXB * (kWgThreads / 32)) {
+    float v[kWgXB];
+    int dofs[kWgXB], xx[kWgXB];
+#pragma unroll
+    for (int g = 0; g < kWgXB; g++) {
+      const int it = i0 + g * (kWgThreads / 32);
+      v[g] = 0.f;
+      dofs[g] = -1;
+      xx[g] = 0;
+      if (it < nitems) {
+        const int row = it / xch, xc = it - row * xch;
+        const int c = row / srows, r = row - c * srows;
+        const int zs = r / (p.ty + 2), ys = r - zs * (p.ty + 2);
+        const int z = z0 + zs - 1, y = y0 + ys - 1, ci = cz * 8 + c;
+        const int x = xc * 32 + lane;
+        if (x < p.w) {
+          dofs[g] = c * p.xpp + r * p.xrp;
+          xx[g] = x;
+          if (ci < p.cin && z >= 0 && z < p.d && y >= 0 && y < p.h)
+            v[g] = __ldg(p.x + (size_t) ci * vol + ((long) z * p.h + y) * p.w + x);
+        }
+      }
     }
-    if (lane == 0) {
-      d0[0] = zero;
-      d2[p.w - 1] = zero;
+#pragma unroll
+    for (int g = 0; g < kWgXB; g++) {
+      if (dofs[g] < 0) continue;
+      __nv_bfloat16 *d0 = xs + dofs[g];
+      __nv_bfloat16 *d1 = d0 + p.xcp, *d2 = d0 + 2 * (size_t) p.xcp;
+      const int x = xx[g];
+      const __nv_bfloat16 b = __float2bfloat16_rn(v[g]);
+      d1[x] = b;
+      if (x + 1 < p.w) d0[x + 1] = b;
+      if (x >= 1) d2[x - 1] = b;
+      if (x == 0) d0[0] = zero;
+      if (x == p.w - 1) d2[p.w - 1] = zero;
     }
   }
   __syncthreads();
-  float acc[kWgTaps][kWgCo16][4];
-#pragma unroll
-  for (int a = 0; a < kWgTaps; a++)
-#pragma unroll
-    for (int b = 0; b < kWgCo16; b++)
-#pragma unroll
-      for (int c = 0; c < 4; c++) acc[a][b][c] = 0.f;
   const uint32_t gys_u = smem_u32(gys), xs_u = smem_u32(xs);
   // ldmatrix row addresses: A (x4) lanes 0-15 rows 0-15 at k 0, lanes 16-31
   // rows 0-15 at k 8; B (x2) lanes 0-7 rows (channels) at k 0, 8-15 at k 8
@@ -417,8 +474,13 @@ __global__ void __launch_bounds__(kWgThreads) k_conv3_wgrad_mma(TcWgrad p) {
       }
     }
   }
+  // bias: this block's row sums of gy, in row order
+  if (p.dobias && cz == 0 && tid < p.cout)
+    for (int rr = 0; rr < bz; rr++) bacc += brow[tid * 16 + rr];
+  __syncthreads();  // the next block's staging overwrites the buffers
+  }
   // partials: D[m = co][n = ci]; thread holds rows lane/4 (+8), columns 2 (lane%4) (+1)
-  const size_t blkoff = ((size_t) blk * p.ncz + cz) * (size_t) p.cout * 8 * 27;
+  const size_t blkoff = ((size_t) blockIdx.x * p.ncz + cz) * (size_t) p.cout * 8 * 27;
 #pragma unroll
   for (int k = 0; k < kWgTaps; k++) {
     const int t = warp + 8 * k;
@@ -433,34 +495,38 @@ __global__ void __launch_bounds__(kWgThreads) k_conv3_wgrad_mma(TcWgrad p) {
       }
     }
   }
-  // bias partials (the first channel chunk's CTAs): the block's row sums
-  // of gy in row order
-  if (p.dobias && cz == 0 && tid < p.cout) {
-    float s = 0.f;
-    for (int rr = 0; rr < bz; rr++) s += brow[tid * 16 + rr];
-    p.part[(size_t) p.nblk * p.ncz * p.cout * 8 * 27 + (size_t) blk * p.cout + tid] = s;
-  }
+  // bias partials (the first channel chunk's CTAs)
+  if (p.dobias && cz == 0 && tid < p.cout)
+    p.part[(size_t) gridDim.x * p.ncz * p.cout * 8 * 27 + (size_t) blockIdx.x * p.cout + tid] = bacc;
 }
 
-// gw[co][ci][t] += sum over blocks (block order) of the partials
+// gw[co][ci][t] += sum over the CTAs' partials: one warp per weight, lanes
+// take every 32nd partial in CTA order, then a fixed shuffle tree (the same
+// sum on every run).
 __global__ void k_wgrad_reduce(const float *__restrict__ part, float *__restrict__ gw, float *__restrict__ gbias,
-                               int cin, int cout, int nblk, int ncz, int dobias) {
+                               int cin, int cout, int nparts, int ncz, int dobias) {
   const long nw = (long) cout * cin * 27;
-  const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  const long i = ((long) blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  float s = 0.f;
   if (i < nw) {
     const int t = (int) (i % 27);
     const long rest = i / 27;
     const int ci = (int) (rest % cin), co = (int) (rest / cin);
     const int cz = ci / 8, n = ci % 8;
-    float s = 0.f;
-    for (int b = 0; b < nblk; b++) s += part[(((size_t) b * ncz + cz) * cout + co) * 8 * 27 + (size_t) n * 27 + t];
-    gw[i] += s;
+    for (int b = lane; b < nparts; b += 32) s += part[(((size_t) b * ncz + cz) * cout + co) * 8 * 27 + (size_t) n * 27 + t];
   } else if (dobias && i < nw + cout) {
     const int co = (int) (i - nw);
-    float s = 0.f;
-    const float *bp = part + (size_t) nblk * ncz * cout * 8 * 27;
-    for (int b = 0; b < nblk; b++) s += bp[(size_t) b * cout + co];
-    gbias[co] += s;
+    const float *bp = part + (size_t) nparts * ncz * cout * 8 * 27;
+    for (int b = lane; b < nparts; b += 32) s += bp[(size_t) b * cout + co];
+  } else {
+    return;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) {
+    if (i < nw) gw[i] += s;
+    else gbias[i - nw] += s;
   }
 }
 
@@ -596,20 +662,37 @@ int run_wgrad_mma(const float *x, const float *gy, float *gw, float *gbias, int 
   }
   if (!found) return gb__set_error(1105, "unet weight gradient: no block plan fits");
   p.nblk = (d / p.tz) * (h / p.ty);
-  const size_t nwp = (size_t) p.nblk * p.ncz * cout * 8 * 27;
-  const size_t nparts = nwp + (p.dobias ? (size_t) p.nblk * cout : 0);
-  p.part = (float *) gb__scratch(GB_SCR_UNET, nparts * sizeof(float));
-  if (!p.part) return gb_last_error();
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_conv3_wgrad_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
     attr = true;
   }
+  // CTAs per channel chunk: one resident wave over all chunks, each CTA
+  // looping over its share of the voxel blocks
+  int nsm = 148, per = 1;
+  {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_conv3_wgrad_mma, kWgThreads, smem) != cudaSuccess ||
+        per < 1) {
+      cudaGetLastError();
+      per = 1;
+    }
+  }
+  int nctas = (per * nsm + p.ncz - 1) / p.ncz;
+  if (nctas > p.nblk) nctas = p.nblk;
+  if (nctas < 1) nctas = 1;
+  const size_t nwp = (size_t) nctas * p.ncz * cout * 8 * 27;
+  const size_t nparts = nwp + (p.dobias ? (size_t) nctas * cout : 0);
+  p.part = (float *) gb__scratch(GB_SCR_UNET, nparts * sizeof(float));
+  if (!p.part) return gb_last_error();
   cudaStream_t st = gb__stream();
-  k_conv3_wgrad_mma<<<dim3((unsigned) p.nblk, (unsigned) p.ncz), kWgThreads, smem, st>>>(p);
+  k_conv3_wgrad_mma<<<dim3((unsigned) nctas, (unsigned) p.ncz), kWgThreads, smem, st>>>(p);
   GB_CHECK_LAUNCH("unet weight gradient");
   const long nw = (long) cout * cin * 27 + (p.dobias ? cout : 0);
-  k_wgrad_reduce<<<(unsigned) ((nw + 255) / 256), 256, 0, st>>>(p.part, gw, gbias, cin, cout, p.nblk, p.ncz, p.dobias);
+  k_wgrad_reduce<<<(unsigned) ((nw * 32 + 255) / 256), 256, 0, st>>>(p.part, gw, gbias, cin, cout, nctas, p.ncz,
+                                                                       p.dobias);
   GB_CHECK_LAUNCH("unet weight gradient reduce");
   return 0;
 }
