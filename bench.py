@@ -76,7 +76,8 @@ KIND_NAMES[18] = "zy_fwd_chain"
 KIND_NAMES[19] = "z_inv_pot_fwd_y_fwd_chain"
 KIND_NAMES[20] = "yz_inv_chain"
 KIND_NAMES[21] = "y_inv_z_inv_pot_fwd_y_fwd_chain"
-NUM_KINDS = 22
+KIND_NAMES[22] = "z_inv_pot_y_fwd_z_fwd_chain"
+NUM_KINDS = 23
 
 
 def measured_traffic(kind, n):

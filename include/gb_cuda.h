@@ -156,9 +156,11 @@ int gb_pass_pipeline(int on);
  * that works plane by plane, so the intermediate result stays in L2 (grids
  * with nx >= 2 and ny = nz = 256).  on = 1 enables, 2 also chains the y INV
  * pass in front of the FP64 potential chain (y INV | z INV.V.FWD | y FWD in
- * one launch: five launches per step), 0 disables, -1 only queries; returns
- * the previous setting.  All schedules compute the same values.  (No
- * reference counterpart.) */
+ * one launch: five launches per step), 3 runs the FP64 real-time step with a
+ * real V_ext as y INV | [z INV, V.y FWD, z FWD] (the potential applied in
+ * the y stage), 0 disables, -1 only queries; returns the previous setting.
+ * All schedules compute the same values up to rounding.  (No reference
+ * counterpart.) */
 int gb_plane_passes(int on);
 /* Ticket lag of the plane-chained passes, in percent of one resident wave of
  * tiles (default 200): the second stage of a plane is issued that far behind

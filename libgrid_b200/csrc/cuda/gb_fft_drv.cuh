@@ -73,7 +73,8 @@ template <typename T> bool plane_ok(const gb_geom *g) {
 }
 
 // Timing kinds of the chains: 18 [z FWD, y FWD], 19 [z INV.V.FWD (or
-// INV.FWD), y FWD], 20 [y INV, z INV], 21 [y INV, z INV.V.FWD, y FWD].
+// INV.FWD), y FWD], 20 [y INV, z INV], 21 [y INV, z INV.V.FWD, y FWD],
+// 22 [z INV, V.y FWD, z FWD].
 template <typename T, class... Stages>
 int plane_chain(const gb_geom *g, void *psi, const PassArgs &a, int kind, Stages...) {
   ChainArgs c;
@@ -99,6 +100,14 @@ int plane_chain(const gb_geom *g, void *psi, const PassArgs &a, int kind, Stages
 // chain is slower than the two passes, and all three stay line passes.
 template <typename T> int plane_mid(const gb_geom *g, void *psi, const PassArgs &a, bool has_pot) {
   if constexpr (sizeof(T) == 8) {
+    // schedule 3 (real-time steps with a real V_ext): y INV | [z INV, V.y FWD, z FWD]
+    // (kind 22), the potential applied in the y stage before its forward
+    // transform, so no stage carries two transforms
+    if (plane_enabled() == 3 && has_pot && a.pot.kind == GB_POT_REAL && !a.pot.absorb && a.pot.c_re == 0.0) {
+      const int rc = pass<T>(g, 1, psi, psi, a, OpL<OP_INV>{});
+      if (rc) return rc;
+      return plane_chain<T>(g, psi, a, 22, Stage<2, OP_INV>{}, Stage<1, OP_POT_RP, OP_FWD>{}, Stage<2, OP_FWD>{});
+    }
     // schedule 2: the y INV pass joins the chain as its first stage (kind 21)
     if (plane_enabled() == 2) {
       if (has_pot && a.pot.kind == GB_POT_REAL && !a.pot.absorb && a.pot.c_re == 0.0)

@@ -54,6 +54,12 @@ struct ChainArgs {
   unsigned wait_limit;  // polls before a dependency wait gives up
 };
 
+// a stage that carries the potential op between two transforms (the
+// register-heaviest stage)
+template <int AX, int... Ops> __host__ __device__ constexpr bool stage_heavy(Stage<AX, Ops...>) {
+  return ((Ops == OP_POT || Ops == OP_POT_RP) || ...) && (((Ops == OP_FWD || Ops == OP_INV) ? 1 : 0) + ...) >= 2;
+}
+
 template <int AX, int... Ops> __host__ __device__ constexpr bool stage_has_pot(Stage<AX, Ops...>) {
   return ((Ops == OP_POT || Ops == OP_POT_RP) || ...);
 }
@@ -113,11 +119,11 @@ __device__ __forceinline__ void chain_tile(Stage<AX, Ops...>, C2<T> *__restrict_
   }
 }
 
-// Resident CTAs per SM for the register bound: a chain whose stage carries
-// the potential op (two transforms and the phase) gets 3 in FP64, so it
+// Resident CTAs per SM for the register bound: a chain with a stage that
+// carries the potential op between two transforms gets 3 in FP64, so it
 // does not spill.
 template <typename T, int N, class... Stages> constexpr int chain_minb() {
-  return (sizeof(T) == 8 && (stage_has_pot(Stages{}) || ...)) ? GB_CHAIN_POT_MINB : ChainCfg<T, N>::MINB;
+  return (sizeof(T) == 8 && (stage_heavy(Stages{}) || ...)) ? GB_CHAIN_POT_MINB : ChainCfg<T, N>::MINB;
 }
 
 template <typename T, int N, class... Stages>

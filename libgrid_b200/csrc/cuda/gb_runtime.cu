@@ -494,7 +494,7 @@ int plane_enabled() { return g_plane_on; }
 }  // namespace gbfft
 extern "C" int gb_plane_passes(int on) {
   const int old = g_plane_on;
-  if (on >= 0) g_plane_on = on > 2 ? 2 : on;
+  if (on >= 0) g_plane_on = on > 3 ? 3 : on;
   return old;
 }
 
