@@ -281,8 +281,8 @@ template <bool CONTIG, int SMAX>
 __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast(double2 *__restrict__ psi, CnAxis a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ __align__(8) uint64_t bar;
-  __shared__ double2 s_end[kSeg][32];
-  __shared__ double2 s_in[kSeg][32];
+  // segment end values, replaced in place by the segments' carries
+  __shared__ double2 s_car[kSeg][32];
   __shared__ double2 s_fact[32];
   double2 *sm = (double2 *) smraw;
   const int tid = threadIdx.x, lane = tid & 31, seg = tid >> 5;
@@ -360,15 +360,16 @@ __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast(double2 *__restrict__ 
       p0 = pp;
     });
   }
-  if (lane < nl) s_end[seg][lane] = u;
+  if (lane < nl) s_car[seg][lane] = u;
   __syncthreads();
   if (seg == 0 && lane < nl) {
     double2 vin = zero;
 #pragma unroll
     for (int s = 0; s < kSeg; s++) {
       const long as = s * S, es = (as + S < n) ? as + S : n;
-      s_in[s][lane] = vin;
-      if (as < es) vin = ca(s_end[s][lane], cm(__ldg(tH + es - 1), vin));
+      const double2 e = s_car[s][lane];
+      s_car[s][lane] = vin;
+      if (as < es) vin = ca(e, cm(__ldg(tH + es - 1), vin));
     }
   }
   __syncthreads();
@@ -376,7 +377,7 @@ __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast(double2 *__restrict__ 
   // ---- forward fix-up fused with the backward particular recurrence
   double2 y = zero;
   if (active) {
-    const double2 vin = s_in[seg][lane];
+    const double2 vin = s_car[seg][lane];
     seg_loop_rev<SMAX>(cnt, [&](int k) {
       const long i = a0 + k;
       const double2 v = ca(tile_at<CONTIG>(sm, lane, i, row), cm(__ldg(tH + i), vin));
@@ -384,15 +385,16 @@ __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast(double2 *__restrict__ 
       tile_at<CONTIG>(sm, lane, i, row) = y;
     });
   }
-  if (lane < nl) s_end[seg][lane] = y;
+  if (lane < nl) s_car[seg][lane] = y;
   __syncthreads();
   if (seg == 0 && lane < nl) {
     double2 xin = zero;
 #pragma unroll
     for (int s = kSeg - 1; s >= 0; s--) {
       const long as = s * S, es = (as + S < n) ? as + S : n;
-      s_in[s][lane] = xin;
-      if (as < es) xin = ca(s_end[s][lane], cm(__ldg(tG + as), xin));
+      const double2 e = s_car[s][lane];
+      s_car[s][lane] = xin;
+      if (as < es) xin = ca(e, cm(__ldg(tG + as), xin));
     }
     if (bc == 3) {
       // Sherman-Morrison: fact = (x_0 + beta x_{n-1} / gamma) / den; the
@@ -405,7 +407,7 @@ __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast(double2 *__restrict__ 
 
   // ---- backward fix-up and periodic correction
   if (active) {
-    const double2 xin = s_in[seg][lane];
+    const double2 xin = s_car[seg][lane];
     const double2 fact = (bc == 3) ? s_fact[lane] : zero;
     seg_loop<SMAX>(cnt, [&](int k) {
       const long i = a0 + k;
@@ -430,7 +432,9 @@ __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast(double2 *__restrict__ 
       bulk_s2g(psi + o * n * a.inner + i * a.inner + col0, sm + i * row, (unsigned) (nl * 16));
   }
   bulk_commit();
-  bulk_wait_all();
+  // the CTA may leave once the stores have read shared memory; their global
+  // writes complete with the grid
+  bulk_wait_read_all();
 }
 
 // ---------------------------------------------------------------------------
@@ -680,7 +684,9 @@ __global__ void __launch_bounds__(kCnWarpThreads, 2) k_cn_warp(double2 *__restri
     cn_tile_copy<CONTIG, false>(psi, sm, pitch, c, a, nullptr, tid);
     bulk_commit();
   }
-  bulk_wait_all();
+  // the CTA may leave once the stores have read shared memory; their global
+  // writes complete with the grid
+  bulk_wait_read_all();
 }
 
 // General path: one thread per line, element (line, i) of a workspace array
