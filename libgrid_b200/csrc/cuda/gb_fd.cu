@@ -78,15 +78,16 @@ __device__ __forceinline__ typename Elem<T, REAL>::V fetch(const typename Elem<T
 // Tiles: a CTA of 256 threads owns a (kFdTY x kFdTZ) = (8 x 32) tile of
 // (y, z) over kFdXC consecutive x planes and marches along x.  Each thread
 // keeps its own column's x-1, x and x+1 values in registers and loads the
-// x+4 plane four steps ahead; the current plane's tile and its one-point y/z
+// plane kFdPD steps ahead; the current plane's tile and its one-point y/z
 // halo sit in a double-buffered shared-memory plane, so the y/z neighbours
 // come from shared memory and every element is read from HBM about once
 // ((kFdXC + 2) / kFdXC planes per chunk, plus the halo rows from L2).  The
-// halo of plane x is loaded one step ahead as well: warp 0 the row y-1,
+// halo points are loaded kFdPD steps ahead as well: warp 0 the row y-1,
 // warp 1 the row y+8, warp 2 the columns z-1 (lanes 0-7) and z+32 (lanes
-// 8-15).
+// 8-15).  Measured at 256^3: two planes ahead at four CTAs per SM beat four
+// planes ahead at three.
 constexpr int kFdTY = 8, kFdTZ = 32, kFdXC = 16, kFdThreads = kFdTY * kFdTZ;
-constexpr int kFdPD = 4;  // planes loaded ahead of the one being computed
+constexpr int kFdPD = 2;  // planes loaded ahead of the one being computed
 
 template <typename T, bool REAL> struct FdTile {
   using E = Elem<T, REAL>;
@@ -136,7 +137,7 @@ template <typename T, bool REAL> struct FdTile {
 };
 
 template <typename T, bool REAL>
-__global__ void __launch_bounds__(kFdThreads, 3) k_fd(int op, typename Elem<T, REAL>::V *__restrict__ dst,
+__global__ void __launch_bounds__(kFdThreads, 4) k_fd(int op, typename Elem<T, REAL>::V *__restrict__ dst,
                                                    const typename Elem<T, REAL>::V *__restrict__ src, FdArgs a) {
   using E = Elem<T, REAL>;
   using V = typename E::V;
@@ -189,7 +190,7 @@ __global__ void __launch_bounds__(kFdThreads, 3) k_fd(int op, typename Elem<T, R
 // Same tiles and march as k_fd; each CTA writes one partial (x, y) sum,
 // reduced in a fixed order, so the result is the same from run to run.
 template <typename T>
-__global__ void __launch_bounds__(kFdThreads, 3) k_fd_kinetic(const C2<T> *__restrict__ src, FdArgs a,
+__global__ void __launch_bounds__(kFdThreads, 4) k_fd_kinetic(const C2<T> *__restrict__ src, FdArgs a,
                                                            double2 *__restrict__ partial) {
   using E = Elem<T, false>;
   using V = C2<T>;
