@@ -78,25 +78,24 @@ __device__ __forceinline__ typename Elem<T, REAL>::V fetch(const typename Elem<T
 // Tiles: a CTA of 256 threads owns a (kFdTY x kFdTZ) = (8 x 32) tile of
 // (y, z) over kFdXC consecutive x planes and marches along x.  Each thread
 // keeps its own column's x-1, x and x+1 values in registers and loads the
-// plane kFdPD steps ahead; the current plane's tile and its one-point y/z
+// x+2 plane two steps ahead; the current plane's tile and its one-point y/z
 // halo sit in a double-buffered shared-memory plane, so the y/z neighbours
 // come from shared memory and every element is read from HBM about once
 // ((kFdXC + 2) / kFdXC planes per chunk, plus the halo rows from L2).  The
-// halo points are loaded kFdPD steps ahead as well: warp 0 the row y-1,
+// halo points are loaded two steps ahead as well: warp 0 the row y-1,
 // warp 1 the row y+8, warp 2 the columns z-1 (lanes 0-7) and z+32 (lanes
 // 8-15).  Measured at 256^3: two planes ahead at four CTAs per SM beat four
 // planes ahead at three.
 constexpr int kFdTY = 8, kFdTZ = 32, kFdXC = 16, kFdThreads = kFdTY * kFdTZ;
-constexpr int kFdPD = 2;  // planes loaded ahead of the one being computed
 
 template <typename T, bool REAL> struct FdTile {
   using E = Elem<T, REAL>;
   using V = typename E::V;
-  V col[kFdPD + 2];  // this thread's column, planes i-1, i, ..., i+kFdPD
-  V hal[kFdPD + 1];  // its halo point (if it owns one), planes i, ..., i+kFdPD
-  long hj, hk;       // halo point (y, z); may lie outside the grid
-  int hy, hz;        // its place in the shared plane
-  bool has_h;        // whether this thread owns a halo point
+  V xm, c, xp, xq;  // this thread's column, planes i-1, i, i+1, i+2
+  V h, hn;          // its halo point (if it owns one), planes i and i+1
+  long hj, hk;      // halo point (y, z); may lie outside the grid
+  int hy, hz;       // its place in the shared plane
+  bool has_h;       // whether this thread owns a halo point
 
   __device__ void init(const V *src, const FdArgs &a, long i0, long j, long k, int ty, int tz) {
     const long j0 = j - ty, k0 = k - tz;
@@ -114,25 +113,27 @@ template <typename T, bool REAL> struct FdTile {
     // every thread of the tile loads its column, also past the far edge of
     // the grid (a partial tile): there fetch returns the boundary value the
     // last row/column needs as its neighbour
-#pragma unroll
-    for (int q = 0; q <= kFdPD; q++) col[q] = fetch<T, REAL>(src, i0 - 1 + q, j, k, a);
-    col[kFdPD + 1] = E::zero();
-#pragma unroll
-    for (int q = 0; q < kFdPD; q++) hal[q] = has_h ? fetch<T, REAL>(src, i0 + q, hj, hk, a) : E::zero();
-    hal[kFdPD] = E::zero();
+    xm = fetch<T, REAL>(src, i0 - 1, j, k, a);
+    c = fetch<T, REAL>(src, i0, j, k, a);
+    xp = fetch<T, REAL>(src, i0 + 1, j, k, a);
+    xq = E::zero();
+    h = has_h ? fetch<T, REAL>(src, i0, hj, hk, a) : E::zero();
+    hn = has_h ? fetch<T, REAL>(src, i0 + 1, hj, hk, a) : E::zero();
   }
 
-  // loads of plane i + kFdPD (column and halo), issued at the top of step i
-  __device__ __forceinline__ void prefetch(const V *src, const FdArgs &a, long i, long i1, long j, long k) {
-    if (i + kFdPD <= i1) col[kFdPD + 1] = fetch<T, REAL>(src, i + kFdPD, j, k, a);
-    if (has_h && i + kFdPD < i1) hal[kFdPD] = fetch<T, REAL>(src, i + kFdPD, hj, hk, a);
+  // loads of plane i + 2 (column and halo), issued at the top of step i;
+  // returns the halo value for the shift
+  __device__ __forceinline__ V prefetch(const V *src, const FdArgs &a, long i, long i1, long j, long k) {
+    if (i + 2 <= i1) xq = fetch<T, REAL>(src, i + 2, j, k, a);
+    return (has_h && i + 2 < i1) ? fetch<T, REAL>(src, i + 2, hj, hk, a) : E::zero();
   }
 
-  __device__ __forceinline__ void shift() {
-#pragma unroll
-    for (int q = 0; q <= kFdPD; q++) col[q] = col[q + 1];
-#pragma unroll
-    for (int q = 0; q < kFdPD; q++) hal[q] = hal[q + 1];
+  __device__ __forceinline__ void shift(V hq) {
+    xm = c;
+    c = xp;
+    xp = xq;
+    h = hn;
+    hn = hq;
   }
 };
 
@@ -153,11 +154,11 @@ __global__ void __launch_bounds__(kFdThreads, 4) k_fd(int op, typename Elem<T, R
   V *out = dst + (i0 * a.ny + j) * a.row + k;
   const long pstride = a.ny * a.row;
   for (long i = i0; i < i1; i++) {
-    t.prefetch(src, a, i, i1, j, k);
+    const V hq = t.prefetch(src, a, i, i1, j, k);
     const int b = (int) ((i - i0) & 1);
-    const V c = t.col[1], xm = t.col[0], xp = t.col[2];
+    const V c = t.c, xm = t.xm, xp = t.xp;
     sm[b][ty + 1][tz + 1] = c;
-    if (t.has_h) sm[b][t.hy][t.hz] = t.hal[0];
+    if (t.has_h) sm[b][t.hy][t.hz] = t.h;
     __syncthreads();
     const V zp = sm[b][ty + 1][tz + 2], zm = sm[b][ty + 1][tz];
     const V yp = sm[b][ty + 2][tz + 1], ym = sm[b][ty][tz + 1];
@@ -181,7 +182,7 @@ __global__ void __launch_bounds__(kFdThreads, 4) k_fd(int op, typename Elem<T, R
       default: r = E::scale(E::sub(zp, zm), coef); break;
     }
     if (in) out[(i - i0) * pstride] = r;
-    t.shift();
+    t.shift(hq);
   }
 }
 
@@ -190,7 +191,7 @@ __global__ void __launch_bounds__(kFdThreads, 4) k_fd(int op, typename Elem<T, R
 // Same tiles and march as k_fd; each CTA writes one partial (x, y) sum,
 // reduced in a fixed order, so the result is the same from run to run.
 template <typename T>
-__global__ void __launch_bounds__(kFdThreads, 4) k_fd_kinetic(const C2<T> *__restrict__ src, FdArgs a,
+__global__ void __launch_bounds__(kFdThreads) k_fd_kinetic(const C2<T> *__restrict__ src, FdArgs a,
                                                            double2 *__restrict__ partial) {
   using E = Elem<T, false>;
   using V = C2<T>;
@@ -205,15 +206,14 @@ __global__ void __launch_bounds__(kFdThreads, 4) k_fd_kinetic(const C2<T> *__res
   t.init(src, a, i0, j, k, ty, tz);
   double sx = 0.0, sy = 0.0;
   for (long i = i0; i < i1; i++) {
-    t.prefetch(src, a, i, i1, j, k);
+    const V hq = t.prefetch(src, a, i, i1, j, k);
     const int b = (int) ((i - i0) & 1);
-    const V c = t.col[1];
+    const V c = t.c;
     sm[b][ty + 1][tz + 1] = c;
-    if (t.has_h) sm[b][t.hy][t.hz] = t.hal[0];
+    if (t.has_h) sm[b][t.hy][t.hz] = t.h;
     __syncthreads();
     if (in) {
-      const V nb[6] = {sm[b][ty + 1][tz + 2], sm[b][ty + 1][tz], sm[b][ty + 2][tz + 1], sm[b][ty][tz + 1], t.col[2],
-                       t.col[0]};
+      const V nb[6] = {sm[b][ty + 1][tz + 2], sm[b][ty + 1][tz], sm[b][ty + 2][tz + 1], sm[b][ty][tz + 1], t.xp, t.xm};
       double sr = -6.0 * (double) c.x, si = -6.0 * (double) c.y;
 #pragma unroll
       for (int q = 0; q < 6; q++) {
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(kFdThreads, 4) k_fd_kinetic(const C2<T> *__res
       sx += (double) c.x * sr + (double) c.y * si;
       sy += (double) c.x * si - (double) c.y * sr;
     }
-    t.shift();
+    t.shift(hq);
   }
 #pragma unroll
   for (int off = 16; off > 0; off >>= 1) {

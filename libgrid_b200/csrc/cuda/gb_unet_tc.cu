@@ -313,7 +313,7 @@ __global__ void k_pack_b(const __nv_bfloat16 *__restrict__ w, __nv_bfloat16 *__r
 constexpr int kWgThreads = 256;  // 8 warps, warp w takes taps w, w + 8, ...
 constexpr int kWgTaps = 4;       // ceil(27 / 8)
 constexpr int kWgCo16 = 4;       // up to 64 output channels
-constexpr int kWgXB = 8;         // staging loads issued together per lane
+constexpr int kWgXB = 4;         // 32-wide chunks of a staged row loaded together
 
 struct TcWgrad {
   const float *x, *gy;
@@ -347,7 +347,7 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1
 }
 
 // grid: (voxel blocks, input-channel chunks of 8)
-__global__ void __launch_bounds__(kWgThreads) k_conv3_wgrad_mma(TcWgrad p) {
+__global__ void __launch_bounds__(kWgThreads, 2) k_conv3_wgrad_mma(TcWgrad p) {
   extern __shared__ __align__(128) unsigned char smraw[];
   __nv_bfloat16 *gys = (__nv_bfloat16 *) smraw;                           // [16 co16][qp]
   __nv_bfloat16 *xs = gys + (size_t) 16 * p.co16 * p.qp;                   // [3][8][rows][w]
@@ -367,82 +367,120 @@ __global__ void __launch_bounds__(kWgThreads) k_conv3_wgrad_mma(TcWgrad p) {
   float bacc = 0.f;  // bias partial of output channel tid (tid < cout)
   for (int blk = blockIdx.x; blk < p.nblk; blk += gridDim.x) {
   const int z0 = (blk / nby) * p.tz, y0 = (blk % nby) * p.ty;
-  // gy of the block, bf16 [co][q] (rows past cout are zero); one row
-  // (co, zi, yi) per warp at a time, lanes along x; the warp also sums the
-  // row (FP32, unrounded) for the bias gradient
+  // gy of the block, bf16 [co][q] (rows past cout are zero), rows
+  // (co, zi, yi) with lanes along x; the warp also sums each row (FP32,
+  // unrounded) for the bias gradient
   const int bz = p.tz * p.ty;
   __shared__ float brow[64 * 16];  // [co][zi ty + yi] row sums (co < 64, tz ty <= 16)
-  // (the loads of up to kWgXB 32-wide chunks of a row are issued before
-  // their stores, and the row sum adds the chunks in x order per lane)
-  for (int row = warp; row < 16 * p.co16 * bz; row += kWgThreads / 32) {
-    const int co = row / bz, rr = row - co * bz, zi = rr / p.ty, yi = rr - zi * p.ty;
-    const float *src = p.gy + (size_t) co * vol + ((long) (z0 + zi) * p.h + (y0 + yi)) * p.w;
-    __nv_bfloat16 *dst = gys + (size_t) co * p.qp + (size_t) rr * p.w;
-    float s = 0.f;
-    for (int xb = 0; xb < p.w; xb += 32 * kWgXB) {
-      float v[kWgXB];
+  // (a warp takes two rows at a time and issues the loads of both rows'
+  // chunks, up to kWgXB per row, before any store; the row sum adds the
+  // chunks in x order per lane).  Rows of channels past cout stay zero:
+  // they are written by the CTA's first block only.
+  {
+    constexpr int NW = kWgThreads / 32, RB = 2;
+    const int nrows = (blk == (int) blockIdx.x ? 16 * p.co16 : p.cout) * bz;
+    for (int r0 = warp; r0 < nrows; r0 += RB * NW) {
+      const float *src[RB];
+      __nv_bfloat16 *dst[RB];
+      bool ok[RB], live[RB];
+      int cos[RB], rrs[RB];
 #pragma unroll
-      for (int j = 0; j < kWgXB; j++) {
-        const int x = xb + 32 * j + lane;
-        v[j] = (co < p.cout && x < p.w) ? __ldg(src + x) : 0.f;
+      for (int q = 0; q < RB; q++) {
+        const int row = r0 + q * NW;
+        ok[q] = row < nrows;
+        const int co = ok[q] ? row / bz : 0, rr = ok[q] ? row - co * bz : 0, zi = rr / p.ty, yi = rr - zi * p.ty;
+        cos[q] = co;
+        rrs[q] = rr;
+        live[q] = ok[q] && co < p.cout;
+        src[q] = live[q] ? p.gy + (size_t) co * vol + ((long) (z0 + zi) * p.h + (y0 + yi)) * p.w : p.gy;
+        dst[q] = gys + (size_t) co * p.qp + (size_t) rr * p.w;
       }
+      float sum[RB] = {};
+      for (int xb = 0; xb < p.w; xb += 32 * kWgXB) {
+        float v[RB][kWgXB];
 #pragma unroll
-      for (int j = 0; j < kWgXB; j++) {
-        const int x = xb + 32 * j + lane;
-        if (x < p.w) {
-          dst[x] = __float2bfloat16_rn(v[j]);
-          s += v[j];
+        for (int q = 0; q < RB; q++)
+#pragma unroll
+          for (int j = 0; j < kWgXB; j++) {
+            const int x = xb + 32 * j + lane;
+            v[q][j] = (live[q] && x < p.w) ? __ldg(src[q] + x) : 0.f;
+          }
+#pragma unroll
+        for (int q = 0; q < RB; q++) {
+          if (!ok[q]) continue;
+#pragma unroll
+          for (int j = 0; j < kWgXB; j++) {
+            const int x = xb + 32 * j + lane;
+            if (x < p.w) {
+              dst[q][x] = __float2bfloat16_rn(v[q][j]);
+              sum[q] += v[q][j];
+            }
+          }
         }
       }
-    }
-    if (p.dobias && cz == 0 && co < p.cout) {
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-      if (lane == 0) brow[co * 16 + rr] = s;
+      if (p.dobias && cz == 0) {
+#pragma unroll
+        for (int q = 0; q < RB; q++) {
+          float t = sum[q];
+          for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+          if (lane == 0 && live[q]) brow[cos[q] * 16 + rrs[q]] = t;
+        }
+      }
     }
   }
   // three x-shifted copies of the x halo block for this chunk of 8 channels:
   // copy cp holds x[. + cp - 1]; each input value is loaded once and stored
-  // into the three copies.  Items (row, 32-wide chunk), every 8th to a warp,
-  // kWgXB items' loads issued together.
-  const int srows = (p.tz + 2) * (p.ty + 2);
-  const int xch = (p.w + 31) >> 5;
-  const int nitems = 8 * srows * xch;
-  const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
-  for (int i0 = warp; i0 < nitems; i0 += kWgXB * (kWgThreads / 32)) {
-    float v[kWgXB];
-    int dofs[kWgXB], xx[kWgXB];
+  // into the three copies.  A warp takes two staged rows at a time (rows
+  // warp, warp + 8, ...), lanes along x, and issues the loads of both rows'
+  // chunks (up to kWgXB per row) before any store.
+  {
+    constexpr int NW = kWgThreads / 32, RB = 2;
+    const int srows = (p.tz + 2) * (p.ty + 2);
+    const int nrows = 8 * srows;
+    const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
+    for (int r0 = warp; r0 < nrows; r0 += RB * NW) {
+      const float *src[RB];
+      __nv_bfloat16 *dst[RB];
+      bool ok[RB], inrow[RB];
 #pragma unroll
-    for (int g = 0; g < kWgXB; g++) {
-      const int it = i0 + g * (kWgThreads / 32);
-      v[g] = 0.f;
-      dofs[g] = -1;
-      xx[g] = 0;
-      if (it < nitems) {
-        const int row = it / xch, xc = it - row * xch;
-        const int c = row / srows, r = row - c * srows;
+      for (int q = 0; q < RB; q++) {
+        const int row = r0 + q * NW;
+        ok[q] = row < nrows;
+        const int c = ok[q] ? row / srows : 0, r = ok[q] ? row - c * srows : 0;
         const int zs = r / (p.ty + 2), ys = r - zs * (p.ty + 2);
         const int z = z0 + zs - 1, y = y0 + ys - 1, ci = cz * 8 + c;
-        const int x = xc * 32 + lane;
-        if (x < p.w) {
-          dofs[g] = c * p.xpp + r * p.xrp;
-          xx[g] = x;
-          if (ci < p.cin && z >= 0 && z < p.d && y >= 0 && y < p.h)
-            v[g] = __ldg(p.x + (size_t) ci * vol + ((long) z * p.h + y) * p.w + x);
+        inrow[q] = ok[q] && ci < p.cin && z >= 0 && z < p.d && y >= 0 && y < p.h;
+        src[q] = inrow[q] ? p.x + (size_t) ci * vol + ((long) z * p.h + y) * p.w : p.x;
+        dst[q] = xs + (size_t) c * p.xpp + (size_t) r * p.xrp;
+      }
+      for (int xb = 0; xb < p.w; xb += 32 * kWgXB) {
+        float v[RB][kWgXB];
+#pragma unroll
+        for (int q = 0; q < RB; q++)
+#pragma unroll
+          for (int j = 0; j < kWgXB; j++) {
+            const int x = xb + 32 * j + lane;
+            v[q][j] = (inrow[q] && x < p.w) ? __ldg(src[q] + x) : 0.f;
+          }
+#pragma unroll
+        for (int q = 0; q < RB; q++) {
+          if (!ok[q]) continue;
+          __nv_bfloat16 *d0 = dst[q];
+          __nv_bfloat16 *d1 = d0 + p.xcp, *d2 = d0 + 2 * (size_t) p.xcp;
+#pragma unroll
+          for (int j = 0; j < kWgXB; j++) {
+            const int x = xb + 32 * j + lane;
+            if (x < p.w) {
+              const __nv_bfloat16 b = __float2bfloat16_rn(v[q][j]);
+              d1[x] = b;
+              if (x + 1 < p.w) d0[x + 1] = b;
+              if (x >= 1) d2[x - 1] = b;
+              if (x == 0) d0[0] = zero;
+              if (x == p.w - 1) d2[p.w - 1] = zero;
+            }
+          }
         }
       }
-    }
-#pragma unroll
-    for (int g = 0; g < kWgXB; g++) {
-      if (dofs[g] < 0) continue;
-      __nv_bfloat16 *d0 = xs + dofs[g];
-      __nv_bfloat16 *d1 = d0 + p.xcp, *d2 = d0 + 2 * (size_t) p.xcp;
-      const int x = xx[g];
-      const __nv_bfloat16 b = __float2bfloat16_rn(v[g]);
-      d1[x] = b;
-      if (x + 1 < p.w) d0[x + 1] = b;
-      if (x >= 1) d2[x - 1] = b;
-      if (x == 0) d0[0] = zero;
-      if (x == p.w - 1) d2[p.w - 1] = zero;
     }
   }
   __syncthreads();
@@ -638,27 +676,31 @@ int run_wgrad_mma(const float *x, const float *gy, float *gw, float *gbias, int 
   p.co16 = (cout + 15) / 16;
   p.ncz = (cin + 7) / 8;
   p.dobias = gbias != nullptr;
-  // voxel block: tz x ty x w with tz ty w a multiple of 16 and the staging
-  // within 160 KB
+  // voxel block: tz x ty x w with tz ty w a multiple of 16; the largest
+  // block whose staging lets two CTAs share an SM (<= 108 KB), else the
+  // largest within 160 KB
   const int cand[4][2] = {{2, 2}, {2, 1}, {1, 2}, {1, 1}};
+  const size_t caps[2] = {108 * 1024, 160 * 1024};
   bool found = false;
   size_t smem = 0;
-  for (auto &c : cand) {
-    const int tz = c[0], ty = c[1];
-    if (tz > d || ty > h || d % tz || h % ty || (tz * ty * wd) % 16) continue;
-    const int nq = tz * ty * wd;
-    const int qp = nq + 8;
-    const int xpp = (tz + 2) * (ty + 2) * wd + 8;
-    smem = ((size_t) 16 * p.co16 * qp + (size_t) 3 * 8 * xpp) * 2;
-    if (smem > 160 * 1024) continue;
-    p.tz = tz;
-    p.ty = ty;
-    p.qp = qp;
-    p.xrp = wd;
-    p.xpp = xpp;
-    p.xcp = 8 * xpp;
-    found = true;
-    break;
+  for (int pass = 0; pass < 2 && !found; pass++) {
+    for (auto &c : cand) {
+      const int tz = c[0], ty = c[1];
+      if (tz > d || ty > h || d % tz || h % ty || (tz * ty * wd) % 16) continue;
+      const int nq = tz * ty * wd;
+      const int qp = nq + 8;
+      const int xpp = (tz + 2) * (ty + 2) * wd + 8;
+      smem = ((size_t) 16 * p.co16 * qp + (size_t) 3 * 8 * xpp) * 2;
+      if (smem > caps[pass]) continue;
+      p.tz = tz;
+      p.ty = ty;
+      p.qp = qp;
+      p.xrp = wd;
+      p.xpp = xpp;
+      p.xcp = 8 * xpp;
+      found = true;
+      break;
+    }
   }
   if (!found) return gb__set_error(1105, "unet weight gradient: no block plan fits");
   p.nblk = (d / p.tz) * (h / p.ty);
