@@ -410,7 +410,8 @@ void gb_batch_free(gb_batch *b);
  * (src/grid_wf.c:379-556, 681-700, 215-221) and starts from whatever guess
  * the caller maps in; these kernels only produce that guess.
  *
- * Activations are FP32 [C][D][H][W] (one sample per call), weights bf16
+ * Activations are FP32 [C][D][H][W] (one sample, or nb samples stacked along
+ * the depth axis for the *_nb convolutions), weights bf16
  * [Cout][Cin][27] (3x3x3 taps, zero padding, tap t = 9(dz+1)+3(dy+1)+(dx+1)),
  * accumulation FP32.  Gradient buffers accumulate (+=); gb_unet_adam clears
  * them.  All calls are asynchronous on the library stream.
@@ -423,6 +424,19 @@ int gb_unet_conv3_bwd_data(const float *gy, const uint16_t *w, float *gx, int ci
 /* gw += dL/dw, gb += dL/db (gb may be NULL). */
 int gb_unet_conv3_bwd_weight(const float *x, const float *gy, float *gw, float *gb, int cin, int cout, int d, int h,
                              int wd);
+/* The same three convolutions over nb samples in one call: activations
+ * [C][nb*d][h][wd], sample s in planes [s*d, (s+1)*d) of every channel, with
+ * no depth neighbours across samples (the weight and bias gradients sum
+ * over all samples).  Pooling, upsampling, the ReLU mask and the MSE
+ * gradient need no variant: give them depth nb*d or n = nb times the
+ * sample's size.  Batches fill the GPU on the coarse levels of small
+ * grids. */
+int gb_unet_conv3_fwd_nb(const float *x, const uint16_t *w, const float *b, float *y, int cin, int cout, int nb, int d,
+                         int h, int wd, int relu);
+int gb_unet_conv3_bwd_data_nb(const float *gy, const uint16_t *w, float *gx, int cin, int cout, int nb, int d, int h,
+                              int wd);
+int gb_unet_conv3_bwd_weight_nb(const float *x, const float *gy, float *gw, float *gb, int cin, int cout, int nb, int d,
+                                int h, int wd);
 /* gy[i] = 0 where y[i] <= 0 (y is the ReLU output). */
 int gb_unet_relu_bwd(float *gy, const float *y, long n);
 /* 2x2x2 average pooling and its gradient (gx += ...); d, h, wd = input

@@ -69,10 +69,11 @@ template <typename T> int gb__ksq_sum_t(const void *psi, void *work, const gb_ge
 // Tensor-core U-Net convolutions (gb_unet_tc.cu): return -1 when the path is
 // off or the shape has no plan (the caller runs the SIMT kernel), else a
 // status.  mode 0: y = conv(x) (+ bias, ReLU); mode 1: y = data gradient of
-// x = gy.
-int gb__unet_conv_tc(const float *x, const uint16_t *w, const float *b, float *y, int cin, int cout, int d, int h,
-                     int wd, int relu, int mode);
-int gb__unet_wgrad_tc(const float *x, const float *gy, float *gw, float *gb, int cin, int cout, int d, int h, int wd);
+// x = gy.  nb samples of d planes each are stacked along the depth axis.
+int gb__unet_conv_tc(const float *x, const uint16_t *w, const float *b, float *y, int cin, int cout, int nb, int d,
+                     int h, int wd, int relu, int mode);
+int gb__unet_wgrad_tc(const float *x, const float *gy, float *gw, float *gb, int cin, int cout, int nb, int d, int h,
+                      int wd);
 
 // Deterministic sum of n partials into out (FP64), on the library stream.
 int gb__sum_partials(const double *partial, long n, double *out_host);

@@ -6,7 +6,10 @@
 // every M steps).  The plain imaginary-time propagation still decides the
 // converged state.
 //
-// Layout: activations FP32 [C][D][H][W], one sample per call; weights bf16
+// Layout: activations FP32 [C][D][H][W]; the *_nb convolutions take nb
+// samples stacked along the depth axis ([C][nb D][H][W], depth neighbours
+// never crossing samples), and pooling, upsampling and the pointwise kernels
+// take the stacked depth as it is; weights bf16
 // [Cout][Cin][27] (3x3x3 taps, zero padding), FP32 master weights and FP32
 // gradient accumulators [Cout][Cin][27] owned by the caller.  All
 // accumulation is FP32 in a fixed order, so every kernel is deterministic.
@@ -39,7 +42,7 @@ constexpr size_t kMaxStage = 48 * 1024 - kSplit * 4 * (kThreads / kSplit) * size
 template <int S>
 __global__ void __launch_bounds__(kThreads) k_conv3_fwd(const float *__restrict__ x, const __nv_bfloat16 *__restrict__ w,
                                                         const float *__restrict__ b, float *__restrict__ y, int cin,
-                                                        int cout, int d, int h, int wd, int relu) {
+                                                        int cout, int d, int h, int wd, int dp, int relu) {
   constexpr int VB = kThreads / S;  // voxels per block
   extern __shared__ float ws[];     // [kCoGroup][cin][27]
   const int co0 = blockIdx.y * kCoGroup;
@@ -56,12 +59,13 @@ __global__ void __launch_bounds__(kThreads) k_conv3_fwd(const float *__restrict_
   for (int j = 0; j < kCoGroup; j++) acc[j] = 0.f;
   if (valid) {
     const int ix = (int) (p % wd), iy = (int) ((p / wd) % h), iz = (int) (p / ((long) wd * h));
+    const int zl = iz % dp;  // plane within its sample
     for (int ci = sl; ci < cin; ci += S) {
       const float *xc = x + (size_t) ci * vol;
       const float *wc = ws + ci * 27;
       for (int dz = -1; dz <= 1; dz++) {
         const int z = iz + dz;
-        if (z < 0 || z >= d) continue;
+        if (zl + dz < 0 || zl + dz >= dp) continue;
         for (int dy = -1; dy <= 1; dy++) {
           const int yy = iy + dy;
           if (yy < 0 || yy >= h) continue;
@@ -106,7 +110,7 @@ __global__ void __launch_bounds__(kThreads) k_conv3_fwd(const float *__restrict_
 template <int S>
 __global__ void __launch_bounds__(kThreads) k_conv3_bwd_data(const float *__restrict__ gy,
                                                              const __nv_bfloat16 *__restrict__ w, float *__restrict__ gx,
-                                                             int cin, int cout, int d, int h, int wd) {
+                                                             int cin, int cout, int d, int h, int wd, int dp) {
   constexpr int VB = kThreads / S;
   extern __shared__ float ws[];  // [kCiGroup][cout][27]
   const int ci0 = blockIdx.y * kCiGroup;
@@ -125,12 +129,13 @@ __global__ void __launch_bounds__(kThreads) k_conv3_bwd_data(const float *__rest
   for (int j = 0; j < kCiGroup; j++) acc[j] = 0.f;
   if (valid) {
     const int ix = (int) (q % wd), iy = (int) ((q / wd) % h), iz = (int) (q / ((long) wd * h));
+    const int zl = iz % dp;  // plane within its sample
     for (int co = sl; co < cout; co += S) {
       const float *gc = gy + (size_t) co * vol;
       const float *wc = ws + co * 27;
       for (int dz = -1; dz <= 1; dz++) {
         const int z = iz - dz;
-        if (z < 0 || z >= d) continue;
+        if (zl - dz < 0 || zl - dz >= dp) continue;
         for (int dy = -1; dy <= 1; dy++) {
           const int yy = iy - dy;
           if (yy < 0 || yy >= h) continue;
@@ -179,7 +184,7 @@ constexpr int kWCo = 4;
 __global__ void __launch_bounds__(kWThreads) k_conv3_bwd_weight(const float *__restrict__ x, const float *__restrict__ gy,
                                                                 float *__restrict__ gw, float *__restrict__ gbias,
                                                                 float *__restrict__ part, int cin, int cout, int d, int h,
-                                                                int wd, long chunk, int nchunk) {
+                                                                int wd, int dp, long chunk, int nchunk) {
   __shared__ float red[kWThreads / 32][kWCo * 28];  // 27 taps, then the bias sum, per output channel
   const int ci = blockIdx.x, co0 = blockIdx.y * kWCo, c = blockIdx.z;
   const int nco = min(kWCo, cout - co0);
@@ -203,10 +208,11 @@ __global__ void __launch_bounds__(kWThreads) k_conv3_bwd_weight(const float *__r
       for (int j = 0; j < kWCo; j++) bs[j] += g[j];
     }
     const int ix = (int) (p % wd), iy = (int) ((p / wd) % h), iz = (int) (p / ((long) wd * h));
+    const int zl = iz % dp;  // plane within its sample
 #pragma unroll
     for (int t = 0; t < 27; t++) {
       const int z = iz + t / 9 - 1, yy = iy + (t / 3) % 3 - 1, xx = ix + t % 3 - 1;
-      const bool in = z >= 0 && z < d && yy >= 0 && yy < h && xx >= 0 && xx < wd;
+      const bool in = zl + t / 9 - 1 >= 0 && zl + t / 9 - 1 < dp && yy >= 0 && yy < h && xx >= 0 && xx < wd;
       const float v = in ? xc[((long) z * h + yy) * wd + xx] : 0.f;
 #pragma unroll
       for (int j = 0; j < kWCo; j++) acc[j][t] = fmaf(g[j], v, acc[j][t]);
@@ -410,50 +416,63 @@ inline int shape_ok(const char *where, long a, long b, long c, long d) {
 
 }  // namespace
 
-extern "C" int gb_unet_conv3_fwd(const float *x, const uint16_t *w, const float *b, float *y, int cin, int cout, int d,
-                                 int h, int wd, int relu) {
-  if (shape_ok("gb_unet_conv3_fwd: bad shape", cin, cout, (long) d * h, wd)) return 1101;
-  const int tc = gb__unet_conv_tc(x, w, b, y, cin, cout, d, h, wd, relu, 0);
+extern "C" int gb_unet_conv3_fwd_nb(const float *x, const uint16_t *w, const float *b, float *y, int cin, int cout, int nb,
+                                    int d, int h, int wd, int relu) {
+  if (shape_ok("gb_unet_conv3_fwd: bad shape", cin, cout, (long) nb * d * h, wd)) return 1101;
+  const int tc = gb__unet_conv_tc(x, w, b, y, cin, cout, nb, d, h, wd, relu, 0);
   if (tc >= 0) return tc;
   const size_t smem = (size_t) kCoGroup * cin * 27 * sizeof(float);
   if (smem > kMaxStage) return gb__set_error(1102, "gb_unet_conv3_fwd: too many input channels for the weight stage");
-  const long vol = (long) d * h * wd;
+  const int dt = nb * d;  // all samples' planes
+  const long vol = (long) dt * h * wd;
   const unsigned gy = (cout + kCoGroup - 1) / kCoGroup;
   if (vol <= kSplitVolume)
     k_conv3_fwd<kSplit><<<dim3((unsigned) ((vol + kThreads / kSplit - 1) / (kThreads / kSplit)), gy), kThreads, smem,
-                          gb__stream()>>>(x, (const __nv_bfloat16 *) w, b, y, cin, cout, d, h, wd, relu);
+                          gb__stream()>>>(x, (const __nv_bfloat16 *) w, b, y, cin, cout, dt, h, wd, d, relu);
   else
     k_conv3_fwd<1><<<dim3(blocks_for(vol), gy), kThreads, smem, gb__stream()>>>(x, (const __nv_bfloat16 *) w, b, y, cin,
-                                                                               cout, d, h, wd, relu);
+                                                                               cout, dt, h, wd, d, relu);
   GB_CHECK_LAUNCH("gb_unet_conv3_fwd");
+  return 0;
+}
+
+extern "C" int gb_unet_conv3_fwd(const float *x, const uint16_t *w, const float *b, float *y, int cin, int cout, int d,
+                                 int h, int wd, int relu) {
+  return gb_unet_conv3_fwd_nb(x, w, b, y, cin, cout, 1, d, h, wd, relu);
+}
+
+extern "C" int gb_unet_conv3_bwd_data_nb(const float *gy, const uint16_t *w, float *gx, int cin, int cout, int nb, int d,
+                                         int h, int wd) {
+  if (shape_ok("gb_unet_conv3_bwd_data: bad shape", cin, cout, (long) nb * d * h, wd)) return 1101;
+  const int tc = gb__unet_conv_tc(gy, w, nullptr, gx, cin, cout, nb, d, h, wd, 0, 1);
+  if (tc >= 0) return tc;
+  const size_t smem = (size_t) kCiGroup * cout * 27 * sizeof(float);
+  if (smem > kMaxStage) return gb__set_error(1102, "gb_unet_conv3_bwd_data: too many output channels for the weight stage");
+  const int dt = nb * d;
+  const long vol = (long) dt * h * wd;
+  const unsigned gyd = (cin + kCiGroup - 1) / kCiGroup;
+  if (vol <= kSplitVolume)
+    k_conv3_bwd_data<kSplit><<<dim3((unsigned) ((vol + kThreads / kSplit - 1) / (kThreads / kSplit)), gyd), kThreads,
+                               smem, gb__stream()>>>(gy, (const __nv_bfloat16 *) w, gx, cin, cout, dt, h, wd, d);
+  else
+    k_conv3_bwd_data<1><<<dim3(blocks_for(vol), gyd), kThreads, smem, gb__stream()>>>(gy, (const __nv_bfloat16 *) w, gx,
+                                                                                     cin, cout, dt, h, wd, d);
+  GB_CHECK_LAUNCH("gb_unet_conv3_bwd_data");
   return 0;
 }
 
 extern "C" int gb_unet_conv3_bwd_data(const float *gy, const uint16_t *w, float *gx, int cin, int cout, int d, int h,
                                       int wd) {
-  if (shape_ok("gb_unet_conv3_bwd_data: bad shape", cin, cout, (long) d * h, wd)) return 1101;
-  const int tc = gb__unet_conv_tc(gy, w, nullptr, gx, cin, cout, d, h, wd, 0, 1);
-  if (tc >= 0) return tc;
-  const size_t smem = (size_t) kCiGroup * cout * 27 * sizeof(float);
-  if (smem > kMaxStage) return gb__set_error(1102, "gb_unet_conv3_bwd_data: too many output channels for the weight stage");
-  const long vol = (long) d * h * wd;
-  const unsigned gyd = (cin + kCiGroup - 1) / kCiGroup;
-  if (vol <= kSplitVolume)
-    k_conv3_bwd_data<kSplit><<<dim3((unsigned) ((vol + kThreads / kSplit - 1) / (kThreads / kSplit)), gyd), kThreads,
-                               smem, gb__stream()>>>(gy, (const __nv_bfloat16 *) w, gx, cin, cout, d, h, wd);
-  else
-    k_conv3_bwd_data<1><<<dim3(blocks_for(vol), gyd), kThreads, smem, gb__stream()>>>(gy, (const __nv_bfloat16 *) w, gx,
-                                                                                     cin, cout, d, h, wd);
-  GB_CHECK_LAUNCH("gb_unet_conv3_bwd_data");
-  return 0;
+  return gb_unet_conv3_bwd_data_nb(gy, w, gx, cin, cout, 1, d, h, wd);
 }
 
-extern "C" int gb_unet_conv3_bwd_weight(const float *x, const float *gy, float *gw, float *gb, int cin, int cout, int d,
-                                        int h, int wd) {
-  if (shape_ok("gb_unet_conv3_bwd_weight: bad shape", cin, cout, (long) d * h, wd)) return 1101;
-  const int tc = gb__unet_wgrad_tc(x, gy, gw, gb, cin, cout, d, h, wd);
+extern "C" int gb_unet_conv3_bwd_weight_nb(const float *x, const float *gy, float *gw, float *gb, int cin, int cout,
+                                           int nb, int d, int h, int wd) {
+  if (shape_ok("gb_unet_conv3_bwd_weight: bad shape", cin, cout, (long) nb * d * h, wd)) return 1101;
+  const int tc = gb__unet_wgrad_tc(x, gy, gw, gb, cin, cout, nb, d, h, wd);
   if (tc >= 0) return tc;
-  const long vol = (long) d * h * wd;
+  const int dt = nb * d;
+  const long vol = (long) dt * h * wd;
   // Voxel chunks of at least 2048 (at most 16 chunks): enough CTAs at 32^3,
   // one chunk (no partials) at 8^3 and below.
   const int nchunk = (int) std::min<long>(16, std::max<long>(1, vol / 2048));
@@ -465,7 +484,7 @@ extern "C" int gb_unet_conv3_bwd_weight(const float *x, const float *gy, float *
     if (!part) return gb_last_error();
   }
   k_conv3_bwd_weight<<<dim3(cin, (cout + kWCo - 1) / kWCo, nchunk), kWThreads, 0, gb__stream()>>>(x, gy, gw, gb, part, cin,
-                                                                                               cout, d, h, wd, chunk,
+                                                                                               cout, dt, h, wd, d, chunk,
                                                                                                nchunk);
   GB_CHECK_LAUNCH("gb_unet_conv3_bwd_weight");
   if (part) {
@@ -477,6 +496,11 @@ extern "C" int gb_unet_conv3_bwd_weight(const float *x, const float *gy, float *
     }
   }
   return 0;
+}
+
+extern "C" int gb_unet_conv3_bwd_weight(const float *x, const float *gy, float *gw, float *gb, int cin, int cout, int d,
+                                        int h, int wd) {
+  return gb_unet_conv3_bwd_weight_nb(x, gy, gw, gb, cin, cout, 1, d, h, wd);
 }
 
 extern "C" int gb_unet_relu_bwd(float *gy, const float *y, long n) {

@@ -121,7 +121,8 @@ struct TcConv {
   const uint4 *bp;    // packed B: per 16-channel chunk, nmma * 4 core matrices
   int *err;
   int cx, ny;         // input channels (K side), output channels (N side)
-  int d, h, w;
+  int d, h, w;        // d: all samples' planes (nb x dp)
+  int dp;             // planes per sample (depth neighbours never cross samples)
   int relu;
   int tz, ty;         // output block: tz x ty x w voxels
   int c8, np, nmma;   // channel chunks, N per CTA (16), MMAs per M-tile
@@ -145,6 +146,7 @@ __global__ void __launch_bounds__(kTcThreads) k_conv3_tc(TcConv p) {
   const int nby = p.h / p.ty;
   const int z0 = (blockIdx.x / nby) * p.tz, y0 = (blockIdx.x % nby) * p.ty;
   const int n0 = blockIdx.y * kTcN;  // first output channel of this CTA
+  const int zlo = (z0 / p.dp) * p.dp;  // first plane of this block's sample
   const long vol = (long) p.d * p.h * p.w;
   const uint32_t plane_bytes = (uint32_t) p.plane_rows * 16u;
   unsigned char *a_sm = smraw;
@@ -189,7 +191,7 @@ __global__ void __launch_bounds__(kTcThreads) k_conv3_tc(TcConv p) {
           if (xs < p.sy) {
             dpos[g] = c * p.plane_rows + p.guard + zs * p.sz + ys * p.sy + xs;
             const int z = z0 + zs - 1, y = y0 + ys - 1, x = xs - 1;
-            if (z >= 0 && z < p.d && y >= 0 && y < p.h && x >= 0 && x < p.w) {
+            if (z >= zlo && z < zlo + p.dp && y >= 0 && y < p.h && x >= 0 && x < p.w) {
               const float *src = p.x + ((long) z * p.h + y) * p.w + x;
 #pragma unroll
               for (int e = 0; e < 8; e++)
@@ -318,7 +320,8 @@ constexpr int kWgXB = 4;         // 32-wide chunks of a staged row loaded togeth
 struct TcWgrad {
   const float *x, *gy;
   float *part;  // [cta][cz][co][8][27] partial sums; bias partials [cta][co] after them
-  int cin, cout, d, h, w;
+  int cin, cout, d, h, w;  // d: all samples' planes (nb x dp)
+  int dp;                  // planes per sample
   int tz, ty;
   int co16;     // output channels / 16, rounded up
   int nblk, ncz;
@@ -449,7 +452,8 @@ __global__ void __launch_bounds__(kWgThreads, 2) k_conv3_wgrad_mma(TcWgrad p) {
         const int c = ok[q] ? row / srows : 0, r = ok[q] ? row - c * srows : 0;
         const int zs = r / (p.ty + 2), ys = r - zs * (p.ty + 2);
         const int z = z0 + zs - 1, y = y0 + ys - 1, ci = cz * 8 + c;
-        inrow[q] = ok[q] && ci < p.cin && z >= 0 && z < p.d && y >= 0 && y < p.h;
+        const int zlo = (z0 / p.dp) * p.dp;
+        inrow[q] = ok[q] && ci < p.cin && z >= zlo && z < zlo + p.dp && y >= 0 && y < p.h;
         src[q] = inrow[q] ? p.x + (size_t) ci * vol + ((long) z * p.h + y) * p.w : p.x;
         dst[q] = xs + (size_t) c * p.xpp + (size_t) r * p.xrp;
       }
@@ -615,9 +619,10 @@ bool tc_plan(int cx, int ny, int d, int h, int w, TcPlan &pl) {
   return false;
 }
 
-int run_conv_tc(const float *x, const uint16_t *w, const float *bias, float *y, int cin, int cout, int d, int h, int wd,
-                int relu, int mode) {
-  // mode 0: y[cout] = conv(x[cin]); mode 1: y = gx[cin] from x = gy[cout]
+int run_conv_tc(const float *x, const uint16_t *w, const float *bias, float *y, int cin, int cout, int nb, int d, int h,
+                int wd, int relu, int mode) {
+  // mode 0: y[cout] = conv(x[cin]); mode 1: y = gx[cin] from x = gy[cout];
+  // nb samples of d planes each, stacked along the depth axis
   const int cx = mode == 0 ? cin : cout, ny = mode == 0 ? cout : cin;
   TcPlan pl;
   if (!tc_plan(cx, ny, d, h, wd, pl)) return gb__set_error(1104, "unet tensor-core conv: no block plan fits");
@@ -637,7 +642,8 @@ int run_conv_tc(const float *x, const uint16_t *w, const float *bias, float *y, 
   p.err = err;
   p.cx = cx;
   p.ny = ny;
-  p.d = d;
+  p.d = nb * d;
+  p.dp = d;
   p.h = h;
   p.w = wd;
   p.relu = relu;
@@ -658,19 +664,21 @@ int run_conv_tc(const float *x, const uint16_t *w, const float *bias, float *y, 
     cudaFuncSetAttribute(k_conv3_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) (200 * 1024 + 1024));
     attr = 200 * 1024 + 1024;
   }
-  const dim3 grid((unsigned) ((d / pl.tz) * (h / pl.ty)), (unsigned) pl.nch);
+  const dim3 grid((unsigned) ((nb * d / pl.tz) * (h / pl.ty)), (unsigned) pl.nch);
   k_conv3_tc<<<grid, kTcThreads, pl.smem, st>>>(p);
   GB_CHECK_LAUNCH("unet tensor-core conv");
   return 0;
 }
 
-int run_wgrad_mma(const float *x, const float *gy, float *gw, float *gbias, int cin, int cout, int d, int h, int wd) {
+int run_wgrad_mma(const float *x, const float *gy, float *gw, float *gbias, int cin, int cout, int nb, int d, int h,
+                  int wd) {
   TcWgrad p;
   p.x = x;
   p.gy = gy;
   p.cin = cin;
   p.cout = cout;
-  p.d = d;
+  p.d = nb * d;
+  p.dp = d;
   p.h = h;
   p.w = wd;
   p.co16 = (cout + 15) / 16;
@@ -703,7 +711,7 @@ int run_wgrad_mma(const float *x, const float *gy, float *gw, float *gbias, int 
     }
   }
   if (!found) return gb__set_error(1105, "unet weight gradient: no block plan fits");
-  p.nblk = (d / p.tz) * (h / p.ty);
+  p.nblk = (nb * d / p.tz) * (h / p.ty);
   static bool attr = false;
   if (!attr) {
     cudaFuncSetAttribute(k_conv3_wgrad_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
@@ -751,15 +759,16 @@ extern "C" int gb_unet_tensor_cores(int on) {
 
 // Entry points used by gb_unet.cu when the tensor-core path is on; return
 // -1 when the shape has no tensor-core plan (the caller then runs SIMT).
-int gb__unet_conv_tc(const float *x, const uint16_t *w, const float *b, float *y, int cin, int cout, int d, int h,
-                     int wd, int relu, int mode) {
+int gb__unet_conv_tc(const float *x, const uint16_t *w, const float *b, float *y, int cin, int cout, int nb, int d,
+                     int h, int wd, int relu, int mode) {
   if (!g_tc_on) return -1;
   TcPlan pl;
   if (!tc_plan(mode == 0 ? cin : cout, mode == 0 ? cout : cin, d, h, wd, pl)) return -1;
-  return run_conv_tc(x, w, b, y, cin, cout, d, h, wd, relu, mode);
+  return run_conv_tc(x, w, b, y, cin, cout, nb, d, h, wd, relu, mode);
 }
 
-int gb__unet_wgrad_tc(const float *x, const float *gy, float *gw, float *gb, int cin, int cout, int d, int h, int wd) {
+int gb__unet_wgrad_tc(const float *x, const float *gy, float *gw, float *gb, int cin, int cout, int nb, int d, int h,
+                      int wd) {
   if (!g_tc_on || cout > 16 * kWgCo16 || wd < 16 || wd % 16) return -1;
-  return run_wgrad_mma(x, gy, gw, gb, cin, cout, d, h, wd);
+  return run_wgrad_mma(x, gy, gw, gb, cin, cout, nb, d, h, wd);
 }

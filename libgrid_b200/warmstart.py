@@ -80,6 +80,9 @@ def _bind(lib):
         "gb_unet_conv3_fwd": [V, V, V, V, I, I, I, I, I, I],
         "gb_unet_conv3_bwd_data": [V, V, V, I, I, I, I, I],
         "gb_unet_conv3_bwd_weight": [V, V, V, V, I, I, I, I, I],
+        "gb_unet_conv3_fwd_nb": [V, V, V, V, I, I, I, I, I, I, I],
+        "gb_unet_conv3_bwd_data_nb": [V, V, V, I, I, I, I, I, I],
+        "gb_unet_conv3_bwd_weight_nb": [V, V, V, V, I, I, I, I, I, I],
         "gb_unet_relu_bwd": [V, V, L],
         "gb_unet_pool2_fwd": [V, V, I, I, I, I],
         "gb_unet_pool2_bwd": [V, V, I, I, I, I],
@@ -125,12 +128,17 @@ def _ok(rc, what):
 class DeviceUNet:
     """The U-Net on the device: parameter slabs (FP32 master, bf16 copy,
     Adam moments, gradient), one activation slab and one gradient slab with
-    the same offsets.  Everything runs on the library stream."""
+    the same offsets.  With batch = nb > 1 every activation holds nb samples
+    stacked along the depth axis ([C][nb n][n][n]) and each layer is one
+    launch over all of them (gb_unet_conv3_*_nb), which fills the GPU on the
+    coarse levels.  Everything runs on the library stream."""
 
-    def __init__(self, api, n: int, cin: int = 3, seed: int = 0, ch=C_LEVELS):
+    def __init__(self, api, n: int, cin: int = 3, seed: int = 0, ch=C_LEVELS, batch: int = 1):
         if n % 8:
             raise ValueError("grid extent must be a multiple of 8 (three poolings)")
-        self.api, self.lib, self.n = api, api.lib, n
+        if batch < 1:
+            raise ValueError("batch must be at least 1")
+        self.api, self.lib, self.n, self.nb = api, api.lib, n, batch
         _bind(self.lib)
         self.spec, self.chan = unet_spec(cin, ch)
         # parameters
@@ -158,23 +166,25 @@ class DeviceUNet:
             _ok(self.lib.gb_unet_fill(b, off, 0.0), "fill")
         self.t = 0
         self._graphs = {}
-        # activations: a conv with two sources reads them as one contiguous block
+        # activations: a conv with two sources reads them as one contiguous
+        # block; every channel holds nb samples
         self.vol = [(n >> l) ** 3 for l in range(4)]
+        nb = self.nb
         place, off = {}, 0
         for op in self.spec:
             if op[0] == "conv" and len(op[1]) == 2:
                 a, b = op[1]
                 place[a] = off
-                place[b] = off + self.chan[a] * self.vol[_LEVEL[a]]
-                off += (self.chan[a] + self.chan[b]) * self.vol[_LEVEL[a]]
+                place[b] = off + self.chan[a] * self.vol[_LEVEL[a]] * nb
+                off += (self.chan[a] + self.chan[b]) * self.vol[_LEVEL[a]] * nb
         for name, c in self.chan.items():
             if name not in place:
                 place[name] = off
-                off += c * self.vol[_LEVEL[name]]
+                off += c * self.vol[_LEVEL[name]] * nb
         self.place, self.nact = place, off
         self._a = self._alloc(4 * off)
         self._ga = self._alloc(4 * off)
-        self._tgt = self._alloc(4 * self.vol[0])
+        self._tgt = self._alloc(4 * self.vol[0] * nb)
 
     def _alloc(self, nbytes):
         p = self.lib.gb_device_alloc(nbytes)
@@ -216,40 +226,52 @@ class DeviceUNet:
 
     def set_input(self, x: np.ndarray):
         x = np.ascontiguousarray(x, np.float32)
-        assert x.shape == (self.chan["in"], self.n, self.n, self.n)
+        assert self.nb == 1 and x.shape == (self.chan["in"], self.n, self.n, self.n)
         _ok(self.lib.gb_h2d(self._act("in"), x.ctypes.data, x.nbytes), "h2d")
 
     def set_input_device(self, dptr):
-        """Input already on the device (cin x n^3 float32)."""
-        _ok(self.lib.gb_d2d(self._act("in"), dptr, 4 * self.chan["in"] * self.vol[0]), "d2d")
+        """Input already on the device (cin x n^3 float32), into sample 0."""
+        self.load_slot(0, dptr)
+
+    def load_slot(self, b, x_dptr, y_dptr=None):
+        """Copy one sample's input (cin x n^3) and optionally its target
+        (n^3), both in device memory, into batch slot b."""
+        v, nb = self.vol[0], self.nb
+        base = self._act("in")
+        for c in range(self.chan["in"]):
+            _ok(self.lib.gb_d2d(base + 4 * (c * nb + b) * v, x_dptr + 4 * c * v, 4 * v), "d2d")
+        if y_dptr is not None:
+            _ok(self.lib.gb_d2d(self._tgt + 4 * b * v, y_dptr, 4 * v), "d2d")
 
     def activation(self, name: str) -> np.ndarray:
+        """An activation, [C][m][m][m] (batch 1) or [C][nb][m][m][m]."""
         lv = _LEVEL[name]
         m = self.n >> lv
-        out = np.empty((self.chan[name], m, m, m), np.float32)
+        shape = (self.chan[name], m, m, m) if self.nb == 1 else (self.chan[name], self.nb, m, m, m)
+        out = np.empty(shape, np.float32)
         _ok(self.lib.gb_d2h(out.ctypes.data, self._act(name), out.nbytes), "d2h")
         _ok(self.lib.gb_synchronize(), "sync")
         return out
 
     def forward(self):
-        lib = self.lib
+        lib, nb = self.lib, self.nb
         for op in self.spec:
             kind, srcs, out = op[0], op[1], op[2]
             m = self.n >> _LEVEL[srcs[0]]
             cin = sum(self.chan[s] for s in srcs)
             if kind == "conv":
                 o, co, ci = self.layers[op[3]]
-                _ok(lib.gb_unet_conv3_fwd(self._act(srcs[0]), self._pb + 2 * o, self._p + 4 * (o + co * ci * 27),
-                                          self._act(out), ci, co, m, m, m, int(op[4])), "conv3_fwd")
+                _ok(lib.gb_unet_conv3_fwd_nb(self._act(srcs[0]), self._pb + 2 * o, self._p + 4 * (o + co * ci * 27),
+                                             self._act(out), ci, co, nb, m, m, m, int(op[4])), "conv3_fwd")
             elif kind == "pool":
-                _ok(lib.gb_unet_pool2_fwd(self._act(srcs[0]), self._act(out), cin, m, m, m), "pool2_fwd")
+                _ok(lib.gb_unet_pool2_fwd(self._act(srcs[0]), self._act(out), cin, nb * m, m, m), "pool2_fwd")
             else:
-                _ok(lib.gb_unet_up2_fwd(self._act(srcs[0]), self._act(out), cin, m, m, m), "up2_fwd")
+                _ok(lib.gb_unet_up2_fwd(self._act(srcs[0]), self._act(out), cin, nb * m, m, m), "up2_fwd")
 
     def backward(self):
         """Accumulate parameter gradients of the loss whose gradient with
         respect to the output is already in the gradient slab."""
-        lib = self.lib
+        lib, nb = self.lib, self.nb
         ga = self._ga
         for op in reversed(self.spec):
             kind, srcs, out = op[0], op[1], op[2]
@@ -258,21 +280,28 @@ class DeviceUNet:
             if kind == "conv":
                 o, co, ci = self.layers[op[3]]
                 if op[4]:
-                    _ok(lib.gb_unet_relu_bwd(self._act(out, ga), self._act(out), co * m ** 3), "relu_bwd")
-                _ok(lib.gb_unet_conv3_bwd_weight(self._act(srcs[0]), self._act(out, ga), self._g + 4 * o,
-                                                 self._g + 4 * (o + co * ci * 27), ci, co, m, m, m), "bwd_weight")
+                    _ok(lib.gb_unet_relu_bwd(self._act(out, ga), self._act(out), co * nb * m ** 3), "relu_bwd")
+                _ok(lib.gb_unet_conv3_bwd_weight_nb(self._act(srcs[0]), self._act(out, ga), self._g + 4 * o,
+                                                    self._g + 4 * (o + co * ci * 27), ci, co, nb, m, m, m),
+                    "bwd_weight")
                 if srcs[0] != "in":
-                    _ok(lib.gb_unet_conv3_bwd_data(self._act(out, ga), self._pb + 2 * o, self._act(srcs[0], ga),
-                                                   ci, co, m, m, m), "bwd_data")
+                    _ok(lib.gb_unet_conv3_bwd_data_nb(self._act(out, ga), self._pb + 2 * o, self._act(srcs[0], ga),
+                                                      ci, co, nb, m, m, m), "bwd_data")
             elif kind == "pool":
-                _ok(lib.gb_unet_pool2_bwd(self._act(out, ga), self._act(srcs[0], ga), cin, m, m, m), "pool2_bwd")
+                _ok(lib.gb_unet_pool2_bwd(self._act(out, ga), self._act(srcs[0], ga), cin, nb * m, m, m), "pool2_bwd")
             else:
-                _ok(lib.gb_unet_up2_bwd(self._act(out, ga), self._act(srcs[0], ga), cin, m, m, m), "up2_bwd")
+                _ok(lib.gb_unet_up2_bwd(self._act(out, ga), self._act(srcs[0], ga), cin, nb * m, m, m), "up2_bwd")
 
-    def loss_grad(self, tgt_dptr, scale=None):
-        n = self.vol[0]
-        s = 2.0 / n if scale is None else scale
-        _ok(self.lib.gb_unet_mse_grad(self._act("out"), tgt_dptr, self._act("out", self._ga), n, s), "mse_grad")
+    def loss_grad(self, tgt_dptr, scale=None, count=None):
+        """Output gradient of the MSE loss for the first `count` samples
+        (default all nb) against targets at tgt_dptr ([count][n^3]); the
+        other slots get a zero gradient, so they add nothing."""
+        v, nb = self.vol[0], self.nb
+        count = nb if count is None else count
+        s = 2.0 / v if scale is None else scale
+        _ok(self.lib.gb_unet_mse_grad(self._act("out"), tgt_dptr, self._act("out", self._ga), count * v, s), "mse_grad")
+        if count < nb:
+            _ok(self.lib.gb_unet_fill(self._act("out", self._ga) + 4 * count * v, (nb - count) * v, 0.0), "fill")
 
     def set_target(self, tgt: np.ndarray):
         t = np.ascontiguousarray(tgt, np.float32)
@@ -305,28 +334,49 @@ class DeviceUNet:
 
     def train_sample(self, x_dptr, y_dptr, scale):
         """Forward, MSE gradient (times scale) and backward of one sample
-        whose input and target sit in device memory: two device copies into
-        the network's input and target slots, then one graph launch (the
-        captured forward, loss gradient and backward; weight gradients
-        accumulate)."""
-        g = self._graphs.get(("train", float(scale)))
+        whose input and target sit in device memory (batch-1 network): two
+        device copies into the network's input and target slots, then one
+        graph launch (the captured forward, loss gradient and backward;
+        weight gradients accumulate)."""
+        self.train_batch([x_dptr], [y_dptr], scale)
+
+    def train_batch(self, x_dptrs, y_dptrs, scale):
+        """The same for up to nb samples at once: each sample is copied into
+        its batch slot, then one graph launch runs forward, loss gradient and
+        backward over the batch (slots past the given samples get a zero
+        output gradient)."""
+        count = len(x_dptrs)
+        if not 1 <= count <= self.nb:
+            raise ValueError("train_batch: %d samples for a batch of %d" % (count, self.nb))
+        g = self._graphs.get(("train", float(scale), count))
         if g is None:
-            raise RuntimeError("train_sample: no graph for loss scale %r (call prepare_training first)" % scale)
-        _ok(self.lib.gb_d2d(self._act("in"), x_dptr, 4 * self.chan["in"] * self.vol[0]), "d2d")
-        _ok(self.lib.gb_d2d(self._tgt, y_dptr, 4 * self.vol[0]), "d2d")
+            raise RuntimeError("train_batch: no graph for loss scale %r and %d samples (call prepare_training first)"
+                               % (scale, count))
+        for b, (xp, yp) in enumerate(zip(x_dptrs, y_dptrs)):
+            self.load_slot(b, xp, yp)
         _ok(self.lib.gb_graph_launch(g), "graph launch")
 
-    def prepare_training(self, scales):
-        """Capture the training graphs of the given loss scales before the
-        first sample (their sizing runs' gradients are cleared)."""
-        for sc in scales:
-            def build(sc=sc):
+    def prepare_training(self, scales, counts=None):
+        """Capture the training graphs of the given loss scales (and batch
+        fills, default a full batch) before the first sample; their sizing
+        runs' gradients are cleared."""
+        counts = [self.nb] * len(scales) if counts is None else counts
+        for sc, cnt in zip(scales, counts):
+            def build(sc=sc, cnt=cnt):
                 self.forward()
-                self.loss_grad(self._tgt, sc)
+                self.loss_grad(self._tgt, sc, cnt)
                 self.backward()
 
-            self._graph(("train", float(sc)), build)
+            self._graph(("train", float(sc), int(cnt)), build)
         _ok(self.lib.gb_unet_fill(self._g, self.nparam, 0.0), "fill")
+
+    def clone(self, batch: int = 1):
+        """A network of the same shape and parameters with another batch
+        size (e.g. batch 1 for inference after batched training)."""
+        other = DeviceUNet(self.api, self.n, cin=self.chan["in"], seed=0, batch=batch)
+        _ok(self.lib.gb_d2d(other._p, self._p, 4 * self.nparam), "d2d")
+        _ok(self.lib.gb_d2d(other._pb, self._pb, 2 * self.nparam), "d2d")
+        return other
 
     def forward_graph(self):
         """Forward of the input already in the activation slab, as one
@@ -334,9 +384,9 @@ class DeviceUNet:
         _ok(self.lib.gb_graph_launch(self._graph(("fwd",), self.forward)), "graph launch")
 
     def infer_device(self, x_dptr):
-        """Forward of one device-resident input (a graph launch); the output
-        stays in the activation slab ("out")."""
-        _ok(self.lib.gb_d2d(self._act("in"), x_dptr, 4 * self.chan["in"] * self.vol[0]), "d2d")
+        """Forward of one device-resident input in batch slot 0 (a graph
+        launch); the output stays in the activation slab ("out")."""
+        self.load_slot(0, x_dptr)
         _ok(self.lib.gb_graph_launch(self._graph(("fwd",), self.forward)), "graph launch")
 
     def predict(self, x: np.ndarray) -> np.ndarray:
@@ -622,15 +672,24 @@ def train(net: DeviceUNet, ds: DeviceSet, epochs=60, batch=8, lr=2e-3, seed=0, l
     nb, vol = ds.count, net.vol[0]
     rng = np.random.default_rng(seed)
     last = float("nan")
+    if net.nb > 1:
+        batch = net.nb  # a batched network takes whole minibatches per launch
     # one captured graph (forward, loss gradient, backward) per minibatch
     # length: the full batch and the remainder
-    net.prepare_training(sorted({2.0 / (vol * min(batch, nb - b0)) for b0 in range(0, nb, batch)}))
+    lens = sorted({min(batch, nb - b0) for b0 in range(0, nb, batch)})
+    if net.nb > 1:
+        net.prepare_training([2.0 / (vol * L) for L in lens], lens)
+    else:
+        net.prepare_training([2.0 / (vol * L) for L in lens])
     for ep in range(epochs):
         order = rng.permutation(nb)
         for b0 in range(0, nb, batch):
             idx = order[b0 : b0 + batch]
-            for i in idx:
-                net.train_sample(ds.xp(i), ds.yp(i), 2.0 / (vol * len(idx)))
+            if net.nb > 1:
+                net.train_batch([ds.xp(i) for i in idx], [ds.yp(i) for i in idx], 2.0 / (vol * len(idx)))
+            else:
+                for i in idx:
+                    net.train_sample(ds.xp(i), ds.yp(i), 2.0 / (vol * len(idx)))
             net.adam(lr * (0.5 * (1 + math.cos(math.pi * ep / epochs)) * 0.95 + 0.05))
         if log is not None or ep == epochs - 1:
             errs = []
@@ -638,7 +697,7 @@ def train(net: DeviceUNet, ds: DeviceSet, epochs=60, batch=8, lr=2e-3, seed=0, l
                 net.infer_device(ds.xp(i))
                 y = np.empty(vol, np.float32)
                 _ok(net.lib.gb_d2h(y.ctypes.data, ds.yp(i), y.nbytes), "d2h")
-                errs.append(float(((net.activation("out")[0].ravel() - y) ** 2).mean()))
+                errs.append(float(((net.activation("out")[0].reshape(net.nb, -1)[0] - y) ** 2).mean()))
             last = float(np.mean(errs))
             if log is not None:
                 log(ep, last)
@@ -688,26 +747,31 @@ def evaluate(api, net: DeviceUNet, seeds, n=32, step=0.1, tol=1e-8, ref_tol=1e-1
 
 def time_training_step(net: DeviceUNet, ds: DeviceSet, reps: int = 10):
     """(forward ms, forward + loss + backward ms) per sample as training and
-    inference run them (captured graphs replayed on the library stream),
-    CUDA events after 3 warm-up repetitions."""
+    inference run them (captured graphs replayed on the library stream; a
+    batched network runs nb samples per launch and the time is divided by
+    nb), CUDA events after 3 warm-up repetitions."""
     lib = net.lib
     lib.gb_event_record.restype = C.c_int
     lib.gb_event_record.argtypes = [C.c_int]
     lib.gb_event_elapsed_ms.restype = C.c_float
     lib.gb_event_elapsed_ms.argtypes = [C.c_int, C.c_int]
-    net.prepare_training([2.0 / net.vol[0]])
+    nb, v = net.nb, net.vol[0]
+    net.prepare_training([2.0 / (v * nb)], [nb])
+    xs, ys = [ds.xp(0)] * nb, [ds.yp(0)] * nb
     out = []
     for with_bwd in (False, True):
         for r in range(reps + 3):
             if r == 3:
                 _ok(lib.gb_event_record(0), "event")
             if with_bwd:
-                net.train_sample(ds.xp(0), ds.yp(0), 2.0 / net.vol[0])
+                net.train_batch(xs, ys, 2.0 / (v * nb))
             else:
-                net.infer_device(ds.xp(0))
+                for b in range(nb):
+                    net.load_slot(b, xs[b])
+                net.forward_graph()
         _ok(lib.gb_event_record(1), "event")
         _ok(lib.gb_synchronize(), "sync")
-        out.append(lib.gb_event_elapsed_ms(0, 1) / reps)
+        out.append(lib.gb_event_elapsed_ms(0, 1) / reps / nb)
     _ok(lib.gb_unet_fill(net._g, net.nparam, 0.0), "fill")  # drop the timing runs' gradients
     return out
 
@@ -732,6 +796,8 @@ def main(argv=None):
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--out", default=None)
     ap.add_argument("--quiet", action="store_true", help="no progress lines on stderr")
+    ap.add_argument("--per-sample", action="store_true",
+                    help="train one sample per launch (default: the whole minibatch per launch)")
     a = ap.parse_args(argv)
 
     def note(msg):
@@ -745,7 +811,8 @@ def main(argv=None):
     ds, meta = make_dataset(api, range(1000, 1000 + a.train), a.n, a.step, tol=a.tol)
     t_data = time.perf_counter() - t0
     note("%d ground states in %.1f s (mean %.0f steps)" % (a.train, t_data, np.mean([m["steps"] for m in meta])))
-    net = DeviceUNet(api, a.n, cin=3, seed=0)
+    net = DeviceUNet(api, a.n, cin=3, seed=0, batch=1 if a.per_sample else a.batch)
+    inf = None
     try:
         t0 = time.perf_counter()
         loss = train(net, ds, epochs=a.epochs, batch=a.batch, lr=a.lr,
@@ -755,8 +822,11 @@ def main(argv=None):
         step_ms = time_training_step(net, ds)
         ds.free()
         note("trained in %.1f s" % t_train)
-        rows = evaluate(api, net, range(5000, 5000 + a.test), a.n, a.step, tol=a.tol)
+        inf = net.clone(1) if net.nb > 1 else net  # inference one potential at a time
+        rows = evaluate(api, inf, range(5000, 5000 + a.test), a.n, a.step, tol=a.tol)
     finally:
+        if inf is not None and inf is not net:
+            inf.free()
         net.free()
     mean = lambda k: float(np.mean([r[k] for r in rows]))
     rep = dict(
@@ -764,7 +834,8 @@ def main(argv=None):
         % (a.n, a.step, a.train, a.test),
         stopping="energy read every 10 steps; stop when the geometric estimate of the remaining distance to "
         "the limit and the last 10-step decrement are below %.0e Ha" % (a.tol / 2),
-        params=int(net.nparam), epochs=a.epochs, train_loss=loss, data_seconds=t_data, train_seconds=t_train,
+        params=int(net.nparam), epochs=a.epochs, batch=a.batch, samples_per_launch=net.nb, train_loss=loss,
+        data_seconds=t_data, train_seconds=t_train,
         forward_ms=step_ms[0], forward_backward_ms=step_ms[1],
         data_steps_mean=float(np.mean([m["steps"] for m in meta])),
         steps_gauss=mean("steps_gauss"), steps_tf=mean("steps_tf"), steps_net=mean("steps_net"),

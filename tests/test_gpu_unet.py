@@ -288,3 +288,45 @@ def test_graph_training_step_matches_eager(b200, lib, engine):
     finally:
         dev.free()
         net.free()
+
+
+def test_batched_network_matches_per_sample(b200, lib, engine):
+    """A batch-4 network (samples stacked along depth, one launch per layer)
+    fed 3 samples gives each sample's output as the batch-1 network does,
+    and the same summed weight and bias gradients up to the FP32 summation
+    order (the fourth slot gets a zero output gradient); no depth neighbour
+    crosses a sample boundary."""
+    rng = np.random.default_rng(41)
+    n = 16
+    xs = rng.standard_normal((3, 3, n, n, n)).astype(np.float32)
+    ys = np.abs(rng.standard_normal((3, n, n, n))).astype(np.float32)
+    scale = 2.0 / (3 * n**3)
+    one = ws.DeviceUNet(b200, n, cin=3, seed=9)
+    four = ws.DeviceUNet(b200, n, cin=3, seed=9, batch=4)
+    dev = Dev(lib)
+    try:
+        dx = [dev.put(x) for x in xs]
+        dy = [dev.put(y) for y in ys]
+        one.prepare_training([scale])
+        outs = []
+        for i in range(3):
+            one.train_sample(dx[i], dy[i], scale)
+            outs.append(one.activation("out")[0])
+        g_one = one.get("g")
+        four.prepare_training([scale], [3])
+        four.train_batch(dx, dy, scale)
+        g_four = four.get("g")
+        out4 = four.activation("out")[0]  # [4][n][n][n]
+        for i in range(3):
+            assert _rel(out4[i], outs[i].astype(np.float64)) < 1e-6, i
+        assert _rel(g_four, g_one.astype(np.float64)) < 1e-5
+        inf = four.clone(1)
+        try:
+            inf.infer_device(dx[1])
+            assert _rel(inf.activation("out")[0], outs[1].astype(np.float64)) < 1e-6
+        finally:
+            inf.free()
+    finally:
+        dev.free()
+        one.free()
+        four.free()
