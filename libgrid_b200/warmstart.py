@@ -8,10 +8,8 @@ judge and only replaces the guess: a small 3-D convolutional U-Net, run and
 trained entirely by this library's own device kernels (gb_unet_* in
 csrc/cuda/gb_unet.cu: bf16 weights, FP32 activations and accumulation, Adam on
 FP32 master weights), maps the external potential, the coupling g and the
-Thomas-Fermi profile to the ground-state amplitude: it predicts the
-correction to its Thomas-Fermi input channel, and the guess is that channel
-plus the prediction.  Training data are ground states produced by the plain
-imaginary-time propagator of this library.
+Thomas-Fermi profile to the ground-state amplitude.  Training data are ground
+states produced by the plain imaginary-time propagator of this library.
 
 Workload (seeded, reduced from the 128^3 family so that data generation and
 training fit a short run): 32^3 grid, step 0.1 bohr, mass 4 amu,
@@ -640,9 +638,8 @@ class DeviceSet:
 def make_dataset(api, seeds, n=32, step=0.1, tol=1e-8):
     """Ground states of the seeded potentials, relaxed by the plain
     imaginary-time loop from the Thomas-Fermi profile; features and targets
-    (the ground-state amplitude minus the Thomas-Fermi input channel, both in
-    units of the Thomas-Fermi maximum) stay on the device.  Returns
-    (DeviceSet, meta)."""
+    (the ground-state amplitude in units of the Thomas-Fermi maximum) stay on
+    the device.  Returns (DeviceSet, meta)."""
     seeds = list(seeds)
     r = Relaxer(api, n, step)
     ds = DeviceSet(r.lib, len(seeds), n**3)
@@ -654,8 +651,6 @@ def make_dataset(api, seeds, n=32, step=0.1, tol=1e-8):
             r.set_guess(ds.xp(i) + 4 * 2 * r.vol, s)
             e, steps = r.relax(tol=tol)
             r.target(ds.yp(i), s)
-            # the network learns the correction to its Thomas-Fermi input channel
-            _ok(r.lib.gb_unet_axpy(ds.yp(i), ds.xp(i) + 4 * 2 * r.vol, -1.0, r.vol), "axpy")
             meta.append(dict(seed=sd, g=g, energy=e, steps=steps, scale=s))
         _ok(r.lib.gb_synchronize(), "sync")
     finally:
@@ -739,8 +734,6 @@ def evaluate(api, net: DeviceUNet, seeds, n=32, step=0.1, tol=1e-8, ref_tol=1e-1
             t0 = time.perf_counter()
             _, s = r.tf_features(net._act("in"))
             net.forward_graph()
-            # guess = Thomas-Fermi channel + predicted correction
-            _ok(lib.gb_unet_axpy(net._act("out"), net._act("in") + 4 * 2 * r.vol, 1.0, r.vol), "axpy")
             r.set_guess(net._act("out"), s, 1e-6)
             e_n, st_n = r.relax(tol=tol)
             _ok(lib.gb_synchronize(), "sync")
