@@ -113,6 +113,7 @@ constexpr int kTcThreads = 256;  // two warpgroups: staging, epilogue
 constexpr int kTcM = 128;
 constexpr int kTcN = 16;  // output channels per CTA
 constexpr int kStageG = 4;  // staging items whose loads are issued together
+constexpr int kTcMaxMma = 256;  // MMAs per M-tile (K = 27 taps x channels / 16)
 
 struct TcConv {
   const float *x;     // [cx][d][h][w] FP32
@@ -151,6 +152,21 @@ __global__ void __launch_bounds__(kTcThreads) k_conv3_tc(TcConv p) {
   const uint32_t plane_bytes = (uint32_t) p.plane_rows * 16u;
   unsigned char *a_sm = smraw;
   unsigned char *b_sm = smraw + (size_t) p.c8 * plane_bytes;
+  // A descriptor of MMA j for the first M-tile (m0 = sz): K-chunks 2j and
+  // 2j + 1 (tap, channel chunk), their distance as the leading-byte offset
+  __shared__ uint64_t s_ad[kTcMaxMma];
+  {
+    const uint32_t ab = smem_u32(a_sm);
+    const int nkc = 27 * p.c8;
+    for (int j = threadIdx.x; j < p.nmma; j += kTcThreads) {
+      const int k1 = 2 * j, k2 = (2 * j + 1 < nkc) ? 2 * j + 1 : 2 * j;
+      const uint32_t a1 =
+          ab + (uint32_t) (k1 / 27) * plane_bytes + (uint32_t) (p.guard + p.sz + tap_off(k1 % 27, p.sy, p.sz)) * 16u;
+      const uint32_t a2 =
+          ab + (uint32_t) (k2 / 27) * plane_bytes + (uint32_t) (p.guard + p.sz + tap_off(k2 % 27, p.sy, p.sz)) * 16u;
+      s_ad[j] = smem_desc(a1, a2 - a1, 128u);
+    }
+  }
 
   if (warp == 0) {
     tmem_alloc(&tslot, (uint32_t) p.ncols);
@@ -212,26 +228,22 @@ __global__ void __launch_bounds__(kTcThreads) k_conv3_tc(TcConv p) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = tslot;
-  const uint32_t a_base = smem_u32(a_sm), b_base = smem_u32(b_sm);
+  const uint32_t b_base = smem_u32(b_sm);
   const uint32_t idesc = idesc_bf16(kTcM, p.np);
-  const int nk = 27 * p.c8;  // K-chunks of 8 channels
   bool ok = true;
 
   for (int b0 = 0, batch = 0; b0 < p.ntile; b0 += p.tb, batch++) {
     const int nt = min(p.tb, p.ntile - b0);
     if (tid == 0) {
+      // tile k of the batch starts (b0 + k) * kTcM positions (16-byte units)
+      // after the first tile: added to the start-address field of the
+      // tabled A descriptors (the sum stays inside shared memory, below the
+      // field's 14-bit range); B of MMA j starts j * 2 * np units after B's
+      const uint64_t bd0 = smem_desc(b_base, 16u * (uint32_t) p.np, 128u);
       for (int k = 0; k < nt; k++) {
-        const int m0 = p.sz + (b0 + k) * kTcM;  // first staged position of the tile
-        for (int j = 0; j < p.nmma; j++) {
-          const int k1 = 2 * j, k2 = (2 * j + 1 < nk) ? 2 * j + 1 : 2 * j;
-          const uint32_t a1 = a_base + (uint32_t) (k1 / 27) * plane_bytes +
-                              (uint32_t) (p.guard + m0 + tap_off(k1 % 27, p.sy, p.sz)) * 16u;
-          const uint32_t a2 = a_base + (uint32_t) (k2 / 27) * plane_bytes +
-                              (uint32_t) (p.guard + m0 + tap_off(k2 % 27, p.sy, p.sz)) * 16u;
-          const uint64_t ad = smem_desc(a1, a2 - a1, 128u);
-          const uint64_t bd = smem_desc(b_base + (uint32_t) j * 32u * (uint32_t) p.np, 16u * (uint32_t) p.np, 128u);
-          tc_mma(tmem + (uint32_t) (k * p.np), ad, bd, idesc, j > 0 ? 1u : 0u);
-        }
+        const uint64_t moff = (uint64_t) ((b0 + k) * kTcM);
+        for (int j = 0; j < p.nmma; j++)
+          tc_mma(tmem + (uint32_t) (k * p.np), s_ad[j] + moff, bd0 + (uint64_t) (j * 2 * p.np), idesc, j > 0 ? 1u : 0u);
       }
       tc_commit(&bar);
     }
@@ -592,6 +604,7 @@ bool tc_plan(int cx, int ny, int d, int h, int w, TcPlan &pl) {
   pl.np = kTcN;
   pl.nch = (ny + kTcN - 1) / kTcN;
   pl.nmma = (27 * pl.c8 + 1) / 2;
+  if (pl.nmma > kTcMaxMma) return false;
   const size_t bbytes = (size_t) pl.nmma * 32 * pl.np;
   const int cand[5][2] = {{4, 4}, {4, 2}, {2, 2}, {2, 1}, {1, 1}};
   for (auto &c : cand) {
