@@ -502,26 +502,33 @@ __global__ void __launch_bounds__(kWgThreads, 2) k_conv3_wgrad_mma(TcWgrad p) {
   __syncthreads();
   const uint32_t gys_u = smem_u32(gys), xs_u = smem_u32(xs);
   // ldmatrix row addresses: A (x4) lanes 0-15 rows 0-15 at k 0, lanes 16-31
-  // rows 0-15 at k 8; B (x2) lanes 0-7 rows (channels) at k 0, 8-15 at k 8
+  // rows 0-15 at k 8; B (x2) lanes 0-7 rows (channels) at k 0, 8-15 at k 8.
+  // The byte offsets that depend only on the lane and the warp's taps are
+  // formed once per block; a q-step adds its row and x position.
   const int arow = lane & 15, acol = (lane >> 4) * 8;
   const int bch = lane & 7, bcol = ((lane >> 3) & 1) * 8;
+  const uint32_t a_lane = gys_u + (uint32_t) (arow * p.qp + acol) * 2u;
+  uint32_t b_tap[kWgTaps];
+#pragma unroll
+  for (int k = 0; k < kWgTaps; k++) {
+    const int t = min(warp + 8 * k, 26);
+    const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
+    b_tap[k] = xs_u + (uint32_t) ((dx + 1) * p.xcp + bch * p.xpp + ((1 + dz) * (p.ty + 2) + (1 + dy)) * p.xrp + bcol) *
+                          2u;
+  }
   for (int q0 = 0; q0 < nq; q0 += 16) {
     const int x0 = q0 % p.w, yz = q0 / p.w, yi = yz % p.ty, zi = yz / p.ty;
+    const uint32_t q_off = (uint32_t) ((zi * (p.ty + 2) + yi) * p.xrp + x0) * 2u;
     uint32_t a[kWgCo16][4];
 #pragma unroll
     for (int g = 0; g < kWgCo16; g++)
       if (g < p.co16)
-        ldsm_x4(gys_u + (uint32_t) (((size_t) (g * 16 + arow) * p.qp + q0 + acol) * 2), a[g][0], a[g][1], a[g][2],
-                a[g][3]);
+        ldsm_x4(a_lane + (uint32_t) (g * 16 * p.qp + q0) * 2u, a[g][0], a[g][1], a[g][2], a[g][3]);
 #pragma unroll
     for (int k = 0; k < kWgTaps; k++) {
-      const int t = warp + 8 * k;
-      if (t < 27) {
-        const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-        const int r = (zi + 1 + dz) * (p.ty + 2) + (yi + 1 + dy);
+      if (warp + 8 * k < 27) {
         uint32_t b0, b1;
-        ldsm_x2(xs_u + (uint32_t) (((size_t) (dx + 1) * p.xcp + (size_t) bch * p.xpp + (size_t) r * p.xrp + x0 + bcol) * 2),
-                b0, b1);
+        ldsm_x2(b_tap[k] + q_off, b0, b1);
 #pragma unroll
         for (int g = 0; g < kWgCo16; g++)
           if (g < p.co16) mma_bf16(acc[k][g], a[g][0], a[g][1], a[g][2], a[g][3], b0, b1);
