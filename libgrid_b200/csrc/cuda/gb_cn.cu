@@ -96,13 +96,6 @@ __device__ __forceinline__ double cn_absorb(long i, long j, long k, const CnAxis
   return t > 1.0 ? 1.0 : t;
 }
 
-// V at (ix, iy, iz) as (re, im); zero without a potential grid.
-__device__ __forceinline__ double2 cn_pot_v(long ix, long iy, long iz, const CnAxis &a, const gb_potential &pt) {
-  const long vidx = (ix * a.ny + iy) * pt.vrow + iz;
-  if (pt.kind == GB_POT_COMPLEX) return ((const double2 *) pt.v)[vidx];
-  if (pt.kind == GB_POT_REAL) return make_double2(((const double *) pt.v)[vidx], 0.0);
-  return make_double2(0.0, 0.0);
-}
 
 // psi * exp(c (cons + V + g |psi|^2)) (src/grid_wf.c:586-598), V given
 __device__ __forceinline__ double2 cn_pot_with(double2 x, double2 v, long ix, long iy, long iz,
@@ -132,10 +125,6 @@ __device__ __forceinline__ double2 cn_pot_with(double2 x, double2 v, long ix, lo
     c *= m;
   }
   return cm(x, make_double2(c, s));
-}
-
-__device__ __forceinline__ double2 cn_pot(double2 x, long ix, long iy, long iz, const CnAxis &a, const gb_potential &pt) {
-  return cn_pot_with(x, cn_pot_v(ix, iy, iz, a, pt), ix, iy, iz, pt);
 }
 
 // Right-hand side row i of a line (src/grid_wf_cn.c:139-201 and the y/z
@@ -177,8 +166,11 @@ __device__ __forceinline__ void cn_pot_elems(double2 *base, int es, int i0, int 
       v[k] = make_double2(0.0, 0.0);
       if (i < n) {
         const long vi = vbase + i * vstep;
-        if (pt.kind == GB_POT_COMPLEX) v[k] = ((const double2 *) pt.v)[vi];
-        else if (pt.kind == GB_POT_REAL) v[k].x = ((const double *) pt.v)[vi];
+        // streaming loads: V is read once per sweep, and evict-first keeps
+        // the solver's coefficient tables in the small L1 left beside the
+        // shared-memory tiles
+        if (pt.kind == GB_POT_COMPLEX) v[k] = __ldcs((const double2 *) pt.v + vi);
+        else if (pt.kind == GB_POT_REAL) v[k].x = __ldcs((const double *) pt.v + vi);
       }
     }
 #pragma unroll
@@ -474,9 +466,6 @@ __host__ __device__ inline long warp_pitch(bool contig, long n) {
 // Offsets of the scan tables behind the six per-element tables.
 __host__ __device__ inline long warp_scan_off(long n) { return 6 * n; }
 
-__device__ __forceinline__ double2 shfl_idx2(double2 v, int src) {
-  return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
-}
 __device__ __forceinline__ double2 shfl_up2(double2 v, int d) {
   return make_double2(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d));
 }
