@@ -456,8 +456,6 @@ int gb_unet_adam(float *w, uint16_t *wb, float *m, float *v, float *g, long n, f
 int gb_unet_to_bf16(const float *w, uint16_t *wb, long n);
 /* p[0..n) = v. */
 int gb_unet_fill(float *p, long n, float v);
-/* y += a x over n floats (residual targets and guesses). */
-int gb_unet_axpy(float *y, const float *x, float a, long n);
 /* Convolution engine: 1 (the default) runs the forward and data-gradient
  * convolutions as tcgen05 implicit GEMMs (bf16 operands in shared memory,
  * FP32 accumulators in tensor memory) and the weight gradient on mma.sync

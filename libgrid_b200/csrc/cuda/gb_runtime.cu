@@ -278,7 +278,13 @@ void *gb__scratch(int slot, size_t bytes) {
   Scratch &s = g_scratch[slot];
   if (s.bytes >= bytes && s.p) return s.p;
   if (s.p) {
-    if (g_graphs_live > 0 && g_nretired < 64) {
+    if (g_graphs_live > 0) {
+      // a live graph may hold this buffer's address: keep it until the last
+      // graph is freed (a bounded list; beyond it the call fails instead)
+      if (g_nretired >= 64) {
+        gb__set_error(2, "scratch: too many buffers replaced while CUDA graphs are alive");
+        return nullptr;
+      }
       g_retired[g_nretired++] = s.p;
     } else {
       cudaStreamSynchronize(g_stream);

@@ -341,11 +341,6 @@ __global__ void k_to_bf16(const float *__restrict__ w, __nv_bfloat16 *__restrict
   if (i < n) wb[i] = __float2bfloat16_rn(w[i]);
 }
 
-__global__ void k_axpy(float *__restrict__ y, const float *__restrict__ x, float a, long n) {
-  const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) y[i] = fmaf(a, x[i], y[i]);
-}
-
 __global__ void k_fill(float *__restrict__ p, long n, float v) {
   const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) p[i] = v;
@@ -568,13 +563,6 @@ extern "C" int gb_unet_to_bf16(const float *w, uint16_t *wb, long n) {
   if (n <= 0) return 0;
   k_to_bf16<<<blocks_for(n), kThreads, 0, gb__stream()>>>(w, (__nv_bfloat16 *) wb, n);
   GB_CHECK_LAUNCH("gb_unet_to_bf16");
-  return 0;
-}
-
-extern "C" int gb_unet_axpy(float *y, const float *x, float a, long n) {
-  if (n <= 0) return 0;
-  k_axpy<<<blocks_for(n), kThreads, 0, gb__stream()>>>(y, x, a, n);
-  GB_CHECK_LAUNCH("gb_unet_axpy");
   return 0;
 }
 

@@ -92,7 +92,6 @@ def _bind(lib):
         "gb_unet_adam": [V, V, V, V, V, L, F, F, F, F, F, F],
         "gb_unet_to_bf16": [V, V, L],
         "gb_unet_fill": [V, L, F],
-        "gb_unet_axpy": [V, V, F, L],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -671,9 +670,10 @@ def host_dataset(api, xs, ys):
 
 
 def train(net: DeviceUNet, ds: DeviceSet, epochs=60, batch=8, lr=2e-3, seed=0, log=None, monitor=8):
-    """Adam over minibatches of samples of a device-resident set.  Returns
-    the mean squared error on the first `monitor` samples after the last
-    epoch."""
+    """Adam over minibatches of samples of a device-resident set: a batch-nb
+    network takes each minibatch (of nb samples) in one graph launch, a
+    batch-1 network one sample per launch.  Returns the mean squared error
+    on the first `monitor` samples after the last epoch."""
     nb, vol = ds.count, net.vol[0]
     rng = np.random.default_rng(seed)
     last = float("nan")
