@@ -51,6 +51,8 @@ struct CnAxis {
   double coord_off;
   double step;
   const double2 *tab;  // fast path: m[n], rb[n], z[n]
+  long klo, khi;       // fast path: rows klo..khi take m, rb, Q from mc, rbc, qc
+  double2 mc, rbc, qc;
   double2 beta, gamma, den;
   gb_potential pre, post;
   int absorb;
@@ -323,6 +325,8 @@ __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast(double2 *__restrict__ 
   const long S = (n + kSeg - 1) / kSeg;
   const long a0 = seg * S, e0 = (a0 + S < n) ? a0 + S : n;
   const int cnt = a0 < e0 ? (int) (e0 - a0) : 0;
+  const long klo = a.klo, khi = a.khi;
+  const double2 mc = a.mc, rbc = a.rbc, qc = a.qc;
   const bool active = (lane < nl) && (cnt > 0);
   const int bc = a.boundary;
 
@@ -346,7 +350,8 @@ __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast(double2 *__restrict__ 
       const long i = a0 + k;
       const double2 pp = (k + 1 < cnt) ? tile_at<CONTIG>(sm, lane, i + 1, row) : p_after;
       const double2 b = cn_rhs(i, n, bc, a.cp, a.c2, zero, pm, p0, pp, pfirst, plast);
-      u = (k == 0) ? b : cs(b, cm(__ldg(tm + i), u));
+      const double2 mi = (i >= klo && i <= khi) ? mc : __ldg(tm + i);
+      u = (k == 0) ? b : cs(b, cm(mi, u));
       tile_at<CONTIG>(sm, lane, i, row) = u;
       pm = p0;
       p0 = pp;
@@ -373,7 +378,9 @@ __global__ void __launch_bounds__(32 * kSeg, 2) k_cn_fast(double2 *__restrict__ 
     seg_loop_rev<SMAX>(cnt, [&](int k) {
       const long i = a0 + k;
       const double2 v = ca(tile_at<CONTIG>(sm, lane, i, row), cm(__ldg(tH + i), vin));
-      y = (k == cnt - 1) ? cm(__ldg(trb + i), v) : ca(cm(__ldg(trb + i), v), cm(__ldg(tQ + i), y));
+      const bool cst = i >= klo && i <= khi;
+      const double2 rbi = cst ? rbc : __ldg(trb + i), qi = cst ? qc : __ldg(tQ + i);
+      y = (k == cnt - 1) ? cm(rbi, v) : ca(cm(rbi, v), cm(qi, y));
       tile_at<CONTIG>(sm, lane, i, row) = y;
     });
   }
@@ -800,6 +807,8 @@ __global__ void k_cn_general(double2 *__restrict__ psi, CnAxis a) {
 struct FastTables {
   std::vector<double2> tab;  // 6 n: m, rb, z, H, Q, G; then (32 segments) the scan tables
   double2 beta, inv_gamma, inv_den;
+  long klo, khi;             // rows whose m, rb and Q equal those of row klo bit for bit
+  double2 mc, rbc, qc;
 };
 
 // nseg segments per line: kSeg for the segment-per-warp kernel, 32 for the
@@ -879,6 +888,35 @@ static void build_fast_tables(long n, int bc, cd cp, cd c2, int nseg, FastTables
   put(3 * n, H);
   put(4 * n, q);
   put(5 * n, G);
+  // The elimination of a diagonally dominant constant-coefficient matrix
+  // reaches a fixed point within a few rows: m, rb and Q of the interior
+  // rows are then the same numbers.  The widest such run of rows lets the
+  // solver take these three from registers instead of the tables.
+  {
+    auto same = [&](long i, long j) {
+      return m[i] == m[j] && rb[i] == rb[j] && q[i] == q[j];
+    };
+    long best_lo = n, best_hi = -1;
+    for (long i = 0; i < n;) {
+      long j = i;
+      while (j + 1 < n && same(j + 1, i)) j++;
+      if (j - i > best_hi - best_lo) {
+        best_lo = i;
+        best_hi = j;
+      }
+      i = j + 1;
+    }
+    if (best_hi - best_lo < 8) {  // no useful run: tables everywhere
+      best_lo = n;
+      best_hi = -1;
+    }
+    t.klo = best_lo;
+    t.khi = best_hi;
+    const long k = best_lo < n ? best_lo : 0;
+    t.mc = make_double2(m[k].real(), m[k].imag());
+    t.rbc = make_double2(rb[k].real(), rb[k].imag());
+    t.qc = make_double2(q[k].real(), q[k].imag());
+  }
   const cd ig = 1.0 / gamma, id = 1.0 / den;
   t.beta = make_double2(beta.real(), beta.imag());
   t.inv_gamma = make_double2(ig.real(), ig.imag());
@@ -937,6 +975,11 @@ static double2 *fast_tables(int slot, long n, int bc, cd cp, cd c2, int nseg, cu
   a->beta = e.ft.beta;
   a->gamma = e.ft.inv_gamma;
   a->den = e.ft.inv_den;
+  a->klo = e.ft.klo;
+  a->khi = e.ft.khi;
+  a->mc = e.ft.mc;
+  a->rbc = e.ft.rbc;
+  a->qc = e.ft.qc;
   return tab;
 }
 
