@@ -686,6 +686,10 @@ def train(net: DeviceUNet, ds: DeviceSet, epochs=60, batch=8, lr=2e-3, seed=0, l
         net.prepare_training([2.0 / (vol * L) for L in lens], lens)
     else:
         net.prepare_training([2.0 / (vol * L) for L in lens])
+    # learning rate: linear warm-up over the first epoch's minibatches (from
+    # a tenth), then a cosine decay to 5% by epoch
+    warm = max(1, (nb + batch - 1) // batch)
+    step = 0
     for ep in range(epochs):
         order = rng.permutation(nb)
         for b0 in range(0, nb, batch):
@@ -695,7 +699,9 @@ def train(net: DeviceUNet, ds: DeviceSet, epochs=60, batch=8, lr=2e-3, seed=0, l
             else:
                 for i in idx:
                     net.train_sample(ds.xp(i), ds.yp(i), 2.0 / (vol * len(idx)))
-            net.adam(lr * (0.5 * (1 + math.cos(math.pi * ep / epochs)) * 0.95 + 0.05))
+            ramp = min(1.0, 0.1 + 0.9 * step / warm)
+            net.adam(lr * ramp * (0.5 * (1 + math.cos(math.pi * ep / epochs)) * 0.95 + 0.05))
+            step += 1
         if log is not None or ep == epochs - 1:
             errs = []
             for i in range(min(nb, monitor)):
