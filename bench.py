@@ -663,9 +663,10 @@ def run_b200(args, world, rank, local):
 
 
 def warm_start_report(timeout_s: int = 300):
-    """Imaginary-time time-to-convergence (|dE| < 1e-8 Ha over 10 steps) from
-    the learned U-Net guess against a Gaussian guess, on held-out 32^3 GP
-    potentials: data generation, training and evaluation in a child process
+    """Imaginary-time steps and seconds to convergence (stopping rule, and to
+    1e-8 Ha of the tightly converged limit) from the learned U-Net guess
+    against a Gaussian guess, on held-out 32^3 GP potentials (512 training
+    potentials): data generation, training and evaluation in a child process
     (python -m libgrid_b200.warmstart), summary without the per-potential rows."""
     try:
         p = subprocess.run([sys.executable, "-m", "libgrid_b200.warmstart"], cwd=ROOT, capture_output=True,

@@ -811,7 +811,7 @@ def main(argv=None):
     import libgrid_b200
 
     ap = argparse.ArgumentParser()
-    ap.add_argument("--train", type=int, default=128)
+    ap.add_argument("--train", type=int, default=512)
     ap.add_argument("--test", type=int, default=16)
     ap.add_argument("--epochs", type=int, default=100)
     ap.add_argument("--batch", type=int, default=8)
