@@ -4,7 +4,7 @@ The reference relaxes to a ground state with a caller-composed loop:
 grid_wf_propagate(wf, V, -i dt) -> grid_wf_normalize -> grid_wf_energy every M
 steps (src/grid_wf.c:379-556, 681-700, 215-221), started from a guess the
 caller maps in (a Gaussian in examples/).  This module keeps that loop as the
-judge and only replaces the guess: a small 3-D convolutional U-Net, run and
+arbiter of convergence and only replaces the guess: a small 3-D convolutional U-Net, run and
 trained entirely by this library's own device kernels (gb_unet_* in
 csrc/cuda/gb_unet.cu: bf16 weights, FP32 activations and accumulation, Adam on
 FP32 master weights), maps the external potential, the coupling g and the
