@@ -483,6 +483,25 @@ class Geom(C.Structure):
     _fields_ = [("nx", C.c_long), ("ny", C.c_long), ("nz", C.c_long), ("step", C.c_double), ("prec", C.c_int)]
 
 
+def converged(a, a_prev, tol, rule="remainder"):
+    """One check of the imaginary-time stopping rule on the decrement
+    a = E_(k-1) - E_k over the last m steps (a_prev: the previous positive
+    decrement or None).  Returns (stop, a_prev for the next check).  "change":
+    |a| < tol.  "remainder": the energy falls geometrically, so the distance
+    left to the limit is about a q / (1 - q) with q = a / a_prev; stop when
+    it and a are below tol / 2, or when the energy stops moving (|a| below
+    1e-3 tol)."""
+    if rule == "change":
+        return abs(a) < tol, a_prev
+    if abs(a) < 1e-3 * tol:
+        return True, a_prev
+    if a_prev is not None and 0.0 < a < a_prev:
+        q = a / a_prev
+        if a < 0.5 * tol and a * q / (1.0 - q) < 0.5 * tol:
+            return True, a_prev
+    return False, (a if a > 0.0 else None)
+
+
 class Relaxer:
     """The plain imaginary-time loop on the device through the libgrid API:
     grid_wf_propagate_gp(-i dt) and a renormalisation every step
@@ -595,17 +614,9 @@ class Relaxer:
             e = self.energy()
             self.trace.append((steps, e, time.perf_counter()))
             a = e_prev - e
-            if rule == "change":
-                if abs(a) < tol:
-                    break
-            else:
-                if abs(a) < 1e-3 * tol:
-                    break
-                if a_prev is not None and 0.0 < a < a_prev:
-                    q = a / a_prev
-                    if a < 0.5 * tol and a * q / (1.0 - q) < 0.5 * tol:
-                        break
-                a_prev = a if a > 0.0 else None
+            stop, a_prev = converged(a, a_prev, tol, rule)
+            if stop:
+                break
             e_prev = e
         return e, steps
 
