@@ -735,6 +735,8 @@ def evaluate(api, net: DeviceUNet, seeds, n=32, step=0.1, tol=1e-8, ref_tol=1e-1
     converged state and include building its guess (for the network: the
     Thomas-Fermi features and the inference).  The converged energies are
     compared with each other and with a reference relaxed to ref_tol."""
+    if net.nb != 1:
+        raise ValueError("evaluate: the inference network must have batch 1 (use net.clone(1))")
     r = Relaxer(api, n, step)
     lib = r.lib
     rows = []
