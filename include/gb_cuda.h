@@ -456,14 +456,24 @@ int gb_unet_adam(float *w, uint16_t *wb, float *m, float *v, float *g, long n, f
 int gb_unet_to_bf16(const float *w, uint16_t *wb, long n);
 /* p[0..n) = v. */
 int gb_unet_fill(float *p, long n, float v);
+/* Minibatch gather, one launch: for b < count, sample idx[b] of a
+ * device-resident set of nset samples (inputs xs [nset][cin][vol], targets
+ * ys [nset][vol]) goes to slot b of a batch-nb network's input in
+ * ([cin][nb][vol]) and target tgt ([nb][vol]).  count <= nb and
+ * count <= GB_UNET_MAX_GATHER; idx is a host array read during the call;
+ * an index outside [0, nset) is an error (1101) and nothing is copied.
+ * (No reference counterpart.) */
+#define GB_UNET_MAX_GATHER 32
+int gb_unet_gather(float *in, float *tgt, const float *xs, const float *ys, const int *idx, int count, int cin,
+                   long vol, int nb, long nset);
 /* Convolution engine: 1 (the default) runs the forward and data-gradient
  * convolutions as tcgen05 implicit GEMMs (bf16 operands in shared memory,
  * FP32 accumulators in tensor memory) and the weight gradient on mma.sync
  * bf16 tensor-core instructions (FP32 accumulate), with activations and
  * gradients rounded to bf16 as operands; 0 runs the FP32 SIMT kernels
  * (FP32 activations, bf16 weights).  Shapes without a tensor-core plan
- * (weight gradients of volumes narrower than 16 points, more than 64
- * output channels) always run SIMT.  -1 only queries; returns the previous
+ * (weight gradients of volumes narrower than 8 points or not a multiple of
+ * 8 wide, more than 64 output channels) always run SIMT.  -1 only queries; returns the previous
  * setting.  (No reference counterpart.) */
 int gb_unet_tensor_cores(int on);
 /* Warm-start inputs and guesses built on the device (no host round trip of

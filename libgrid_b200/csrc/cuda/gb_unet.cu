@@ -573,6 +573,40 @@ extern "C" int gb_unet_fill(float *p, long n, float v) {
   return 0;
 }
 
+// Minibatch gather: slot b of a batch-nb network's input ([cin][nb][vol])
+// and target ([nb][vol]) from sample ix.i[b] of a device-resident set
+// (inputs [N][cin][vol], targets [N][vol]); blockIdx.y = channel (cin: the
+// target), blockIdx.z = slot.
+struct GatherIdx {
+  int i[GB_UNET_MAX_GATHER];
+};
+
+__global__ void k_gather(float *__restrict__ in, float *__restrict__ tgt, const float *__restrict__ xs,
+                         const float *__restrict__ ys, GatherIdx ix, int cin, long vol, int nb) {
+  const int c = blockIdx.y, b = blockIdx.z;
+  const long s = ix.i[b];
+  const float *src = c < cin ? xs + (s * cin + c) * vol : ys + s * vol;
+  float *dst = c < cin ? in + ((long) c * nb + b) * vol : tgt + (long) b * vol;
+  for (long k = (long) blockIdx.x * blockDim.x + threadIdx.x; k < vol; k += (long) gridDim.x * blockDim.x)
+    dst[k] = __ldg(src + k);
+}
+
+extern "C" int gb_unet_gather(float *in, float *tgt, const float *xs, const float *ys, const int *idx, int count,
+                              int cin, long vol, int nb, long nset) {
+  if (count < 1 || count > GB_UNET_MAX_GATHER || count > nb || cin < 1 || vol < 1 || !idx)
+    return gb__set_error(1101, "gb_unet_gather: bad count or shape");
+  GatherIdx ix;
+  for (int b = 0; b < count; b++) {
+    if (idx[b] < 0 || idx[b] >= nset) return gb__set_error(1101, "gb_unet_gather: sample index out of range");
+    ix.i[b] = idx[b];
+  }
+  const unsigned gx = (unsigned) std::min<long>((vol + kThreads - 1) / kThreads, 256);
+  k_gather<<<dim3(gx, (unsigned) cin + 1, (unsigned) count), kThreads, 0, gb__stream()>>>(in, tgt, xs, ys, ix, cin,
+                                                                                        vol, nb);
+  GB_CHECK_LAUNCH("gb_unet_gather");
+  return 0;
+}
+
 extern "C" int gb_unet_potential(double *v, int nx, int ny, int nz, long vrow, double step, double k,
                                  const gb_unet_bumps *bumps) {
   if (shape_ok("gb_unet_potential: bad shape", nx, ny, nz, vrow) || bumps->n < 0 || bumps->n > GB_UNET_MAX_BUMPS)

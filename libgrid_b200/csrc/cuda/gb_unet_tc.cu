@@ -327,21 +327,21 @@ __global__ void k_pack_b(const __nv_bfloat16 *__restrict__ w, __nv_bfloat16 *__r
 constexpr int kWgThreads = 256;  // 8 warps, warp w takes taps w, w + 8, ...
 constexpr int kWgTaps = 4;       // ceil(27 / 8)
 constexpr int kWgCo16 = 4;       // up to 64 output channels
-constexpr int kWgXB = 4;         // 32-wide chunks of a staged row loaded together
+constexpr int kWgItems = 8;      // staging items a warp loads before any store
 
 struct TcWgrad {
   const float *x, *gy;
   float *part;  // [cta][cz][co][8][27] partial sums; bias partials [cta][co] after them
   int cin, cout, d, h, w;  // d: all samples' planes (nb x dp)
   int dp;                  // planes per sample
-  int tz, ty;
   int co16;     // output channels / 16, rounded up
   int nblk, ncz;
   int qp;       // gy row pitch (bf16)
   int xrp;      // x staged row pitch (bf16) = w
   int xpp;      // x staged plane pitch (bf16)
   int xcp;      // x staged copy pitch (bf16) = 8 * xpp
-  int dobias;
+  int rpi;      // rows per staging item: 32 / w for w = 8 or 16, else 1
+  int lgc;      // log2 of the 32-wide chunks per row (rpi == 1)
 };
 
 __device__ __forceinline__ void ldsm_x4(uint32_t addr, uint32_t &r0, uint32_t &r1, uint32_t &r2, uint32_t &r3) {
@@ -361,16 +361,34 @@ __device__ __forceinline__ void mma_bf16(float (&d)[4], uint32_t a0, uint32_t a1
       : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
 }
 
-// grid: (voxel blocks, input-channel chunks of 8)
+// Staging item it of a loop over rows of w points -> this lane's (row, x):
+// rows of 32 or more points are split into 2^lgc chunks of 32 lanes; rows of
+// 8 or 16 points are packed rpi = 32 / w to an item (lane = sub-row, x).
+__device__ __forceinline__ void wg_item(int it, int rpi, int lgc, int lsub, int lx, int &row, int &x) {
+  if (rpi > 1) {
+    row = it * rpi + lsub;
+    x = lx;
+  } else {
+    row = it >> lgc;
+    x = ((it & ((1 << lgc) - 1)) << 5) + lx;
+  }
+}
+
+// grid: (CTAs, input-channel chunks of 8); each CTA loops over the voxel
+// blocks blockIdx.x, + gridDim.x, ... of TZ x TY x w points
+template <int TZ, int TY>
 __global__ void __launch_bounds__(kWgThreads, 2) k_conv3_wgrad_mma(TcWgrad p) {
+  constexpr int BZ = TZ * TY, SY = TY + 2, SROWS = (TZ + 2) * SY, NW = kWgThreads / 32;
   extern __shared__ __align__(128) unsigned char smraw[];
   __nv_bfloat16 *gys = (__nv_bfloat16 *) smraw;                           // [16 co16][qp]
   __nv_bfloat16 *xs = gys + (size_t) 16 * p.co16 * p.qp;                   // [3][8][rows][w]
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int nby = p.h / p.ty;
+  const int nby = p.h / TY;
   const int cz = blockIdx.y;
   const long vol = (long) p.d * p.h * p.w;
-  const int nq = p.tz * p.ty * p.w;
+  const int nq = BZ * p.w;
+  const int rpi = p.rpi, lgc = p.lgc;
+  const int lsub = rpi > 1 ? lane / p.w : 0, lx = rpi > 1 ? lane - lsub * p.w : lane;
   // accumulators persist over the voxel blocks blockIdx.x, + gridDim.x, ...
   float acc[kWgTaps][kWgCo16][4];
 #pragma unroll
@@ -379,123 +397,69 @@ __global__ void __launch_bounds__(kWgThreads, 2) k_conv3_wgrad_mma(TcWgrad p) {
     for (int b = 0; b < kWgCo16; b++)
 #pragma unroll
       for (int c = 0; c < 4; c++) acc[a][b][c] = 0.f;
-  float bacc = 0.f;  // bias partial of output channel tid (tid < cout)
   for (int blk = blockIdx.x; blk < p.nblk; blk += gridDim.x) {
-  const int z0 = (blk / nby) * p.tz, y0 = (blk % nby) * p.ty;
+  const int z0 = (blk / nby) * TZ, y0 = (blk % nby) * TY;
   // gy of the block, bf16 [co][q] (rows past cout are zero), rows
-  // (co, zi, yi) with lanes along x; the warp also sums each row (FP32,
-  // unrounded) for the bias gradient
-  const int bz = p.tz * p.ty;
-  __shared__ float brow[64 * 16];  // [co][zi ty + yi] row sums (co < 64, tz ty <= 16)
-  // (a warp takes two rows at a time and issues the loads of both rows'
-  // chunks, up to kWgXB per row, before any store; the row sum adds the
-  // chunks in x order per lane).  Rows of channels past cout stay zero:
-  // they are written by the CTA's first block only.
+  // (co, zi, yi).  A warp issues the loads of kWgItems items before any
+  // store.  Rows of channels past cout are written by the CTA's first block
+  // only.
   {
-    constexpr int NW = kWgThreads / 32, RB = 2;
-    const int nrows = (blk == (int) blockIdx.x ? 16 * p.co16 : p.cout) * bz;
-    for (int r0 = warp; r0 < nrows; r0 += RB * NW) {
-      const float *src[RB];
-      __nv_bfloat16 *dst[RB];
-      bool ok[RB], live[RB];
-      int cos[RB], rrs[RB];
+    const int nrows = (blk == (int) blockIdx.x ? 16 * p.co16 : p.cout) * BZ;
+    const int nit = rpi > 1 ? (nrows + rpi - 1) / rpi : nrows << lgc;
+    for (int i0 = warp; i0 < nit; i0 += kWgItems * NW) {
+      float v[kWgItems];
+      int off[kWgItems];
 #pragma unroll
-      for (int q = 0; q < RB; q++) {
-        const int row = r0 + q * NW;
-        ok[q] = row < nrows;
-        const int co = ok[q] ? row / bz : 0, rr = ok[q] ? row - co * bz : 0, zi = rr / p.ty, yi = rr - zi * p.ty;
-        cos[q] = co;
-        rrs[q] = rr;
-        live[q] = ok[q] && co < p.cout;
-        src[q] = live[q] ? p.gy + (size_t) co * vol + ((long) (z0 + zi) * p.h + (y0 + yi)) * p.w : p.gy;
-        dst[q] = gys + (size_t) co * p.qp + (size_t) rr * p.w;
+      for (int q = 0; q < kWgItems; q++) {
+        int row, x;
+        wg_item(i0 + q * NW, rpi, lgc, lsub, lx, row, x);
+        const bool ok = i0 + q * NW < nit && row < nrows && x < p.w;
+        const int co = row / BZ, rr = row - co * BZ, zi = rr / TY, yi = rr - zi * TY;
+        v[q] = (ok && co < p.cout)
+                   ? __ldg(p.gy + (size_t) co * vol + ((long) (z0 + zi) * p.h + (y0 + yi)) * p.w + x)
+                   : 0.f;
+        off[q] = ok ? co * p.qp + rr * p.w + x : -1;
       }
-      float sum[RB] = {};
-      for (int xb = 0; xb < p.w; xb += 32 * kWgXB) {
-        float v[RB][kWgXB];
 #pragma unroll
-        for (int q = 0; q < RB; q++)
-#pragma unroll
-          for (int j = 0; j < kWgXB; j++) {
-            const int x = xb + 32 * j + lane;
-            v[q][j] = (live[q] && x < p.w) ? __ldg(src[q] + x) : 0.f;
-          }
-#pragma unroll
-        for (int q = 0; q < RB; q++) {
-          if (!ok[q]) continue;
-#pragma unroll
-          for (int j = 0; j < kWgXB; j++) {
-            const int x = xb + 32 * j + lane;
-            if (x < p.w) {
-              dst[q][x] = __float2bfloat16_rn(v[q][j]);
-              sum[q] += v[q][j];
-            }
-          }
-        }
-      }
-      if (p.dobias && cz == 0) {
-#pragma unroll
-        for (int q = 0; q < RB; q++) {
-          float t = sum[q];
-          for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-          if (lane == 0 && live[q]) brow[cos[q] * 16 + rrs[q]] = t;
-        }
-      }
+      for (int q = 0; q < kWgItems; q++)
+        if (off[q] >= 0) gys[off[q]] = __float2bfloat16_rn(v[q]);
     }
   }
   // three x-shifted copies of the x halo block for this chunk of 8 channels:
   // copy cp holds x[. + cp - 1]; each input value is loaded once and stored
-  // into the three copies.  A warp takes two staged rows at a time (rows
-  // warp, warp + 8, ...), lanes along x, and issues the loads of both rows'
-  // chunks (up to kWgXB per row) before any store.
+  // into the three copies.  Rows (c, zs, ys) of the (TZ + 2) x (TY + 2) halo;
+  // a warp issues the loads of kWgItems items before any store.  off packs
+  // the element's offset in a copy with two flags: x == 0 (bit 0) and
+  // x == w - 1 (bit 1), where copies 0 and 2 take the zero padding.
   {
-    constexpr int NW = kWgThreads / 32, RB = 2;
-    const int srows = (p.tz + 2) * (p.ty + 2);
-    const int nrows = 8 * srows;
+    const int nrows = 8 * SROWS;
+    const int nit = rpi > 1 ? (nrows + rpi - 1) / rpi : nrows << lgc;
+    const int zlo = (z0 / p.dp) * p.dp;
     const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
-    for (int r0 = warp; r0 < nrows; r0 += RB * NW) {
-      const float *src[RB];
-      __nv_bfloat16 *dst[RB];
-      bool ok[RB], inrow[RB];
+    for (int i0 = warp; i0 < nit; i0 += kWgItems * NW) {
+      float v[kWgItems];
+      int off[kWgItems];
 #pragma unroll
-      for (int q = 0; q < RB; q++) {
-        const int row = r0 + q * NW;
-        ok[q] = row < nrows;
-        const int c = ok[q] ? row / srows : 0, r = ok[q] ? row - c * srows : 0;
-        const int zs = r / (p.ty + 2), ys = r - zs * (p.ty + 2);
+      for (int q = 0; q < kWgItems; q++) {
+        int row, x;
+        wg_item(i0 + q * NW, rpi, lgc, lsub, lx, row, x);
+        const bool ok = i0 + q * NW < nit && row < nrows && x < p.w;
+        const int c = row / SROWS, r = row - c * SROWS, zs = r / SY, ys = r - zs * SY;
         const int z = z0 + zs - 1, y = y0 + ys - 1, ci = cz * 8 + c;
-        const int zlo = (z0 / p.dp) * p.dp;
-        inrow[q] = ok[q] && ci < p.cin && z >= zlo && z < zlo + p.dp && y >= 0 && y < p.h;
-        src[q] = inrow[q] ? p.x + (size_t) ci * vol + ((long) z * p.h + y) * p.w : p.x;
-        dst[q] = xs + (size_t) c * p.xpp + (size_t) r * p.xrp;
+        const bool in = ok && ci < p.cin && z >= zlo && z < zlo + p.dp && y >= 0 && y < p.h;
+        v[q] = in ? __ldg(p.x + (size_t) ci * vol + ((long) z * p.h + y) * p.w + x) : 0.f;
+        off[q] = ok ? ((c * p.xpp + r * p.xrp + x) << 2) | (x == 0 ? 1 : 0) | (x == p.w - 1 ? 2 : 0) : -1;
       }
-      for (int xb = 0; xb < p.w; xb += 32 * kWgXB) {
-        float v[RB][kWgXB];
 #pragma unroll
-        for (int q = 0; q < RB; q++)
-#pragma unroll
-          for (int j = 0; j < kWgXB; j++) {
-            const int x = xb + 32 * j + lane;
-            v[q][j] = (inrow[q] && x < p.w) ? __ldg(src[q] + x) : 0.f;
-          }
-#pragma unroll
-        for (int q = 0; q < RB; q++) {
-          if (!ok[q]) continue;
-          __nv_bfloat16 *d0 = dst[q];
-          __nv_bfloat16 *d1 = d0 + p.xcp, *d2 = d0 + 2 * (size_t) p.xcp;
-#pragma unroll
-          for (int j = 0; j < kWgXB; j++) {
-            const int x = xb + 32 * j + lane;
-            if (x < p.w) {
-              const __nv_bfloat16 b = __float2bfloat16_rn(v[q][j]);
-              d1[x] = b;
-              if (x + 1 < p.w) d0[x + 1] = b;
-              if (x >= 1) d2[x - 1] = b;
-              if (x == 0) d0[0] = zero;
-              if (x == p.w - 1) d2[p.w - 1] = zero;
-            }
-          }
-        }
+      for (int q = 0; q < kWgItems; q++) {
+        if (off[q] < 0) continue;
+        const int o = off[q] >> 2;
+        const __nv_bfloat16 b = __float2bfloat16_rn(v[q]);
+        xs[p.xcp + o] = b;                              // copy 1 at x
+        if (!(off[q] & 2)) xs[o + 1] = b;               // copy 0 at x + 1
+        else xs[2 * p.xcp + o] = zero;                  // copy 2 at w - 1: padding
+        if (!(off[q] & 1)) xs[2 * p.xcp + o - 1] = b;   // copy 2 at x - 1
+        else xs[o] = zero;                              // copy 0 at 0: padding
       }
     }
   }
@@ -504,7 +468,9 @@ __global__ void __launch_bounds__(kWgThreads, 2) k_conv3_wgrad_mma(TcWgrad p) {
   // ldmatrix row addresses: A (x4) lanes 0-15 rows 0-15 at k 0, lanes 16-31
   // rows 0-15 at k 8; B (x2) lanes 0-7 rows (channels) at k 0, 8-15 at k 8.
   // The byte offsets that depend only on the lane and the warp's taps are
-  // formed once per block; a q-step adds its row and x position.
+  // formed once per block; a q-step adds the staged position of the lane's
+  // first B voxel, q0 + bcol, kept as (qx, qy, qz) and advanced by 16 voxels
+  // per step (two rows when w = 8).
   const int arow = lane & 15, acol = (lane >> 4) * 8;
   const int bch = lane & 7, bcol = ((lane >> 3) & 1) * 8;
   const uint32_t a_lane = gys_u + (uint32_t) (arow * p.qp + acol) * 2u;
@@ -513,12 +479,15 @@ __global__ void __launch_bounds__(kWgThreads, 2) k_conv3_wgrad_mma(TcWgrad p) {
   for (int k = 0; k < kWgTaps; k++) {
     const int t = min(warp + 8 * k, 26);
     const int dz = t / 9 - 1, dy = (t / 3) % 3 - 1, dx = t % 3 - 1;
-    b_tap[k] = xs_u + (uint32_t) ((dx + 1) * p.xcp + bch * p.xpp + ((1 + dz) * (p.ty + 2) + (1 + dy)) * p.xrp + bcol) *
-                          2u;
+    b_tap[k] = xs_u + (uint32_t) ((dx + 1) * p.xcp + bch * p.xpp + ((1 + dz) * SY + (1 + dy)) * p.xrp) * 2u;
+  }
+  int qx = bcol, qy = 0, qz = 0;
+  while (qx >= p.w) {
+    qx -= p.w;
+    if (++qy == TY) { qy = 0; ++qz; }
   }
   for (int q0 = 0; q0 < nq; q0 += 16) {
-    const int x0 = q0 % p.w, yz = q0 / p.w, yi = yz % p.ty, zi = yz / p.ty;
-    const uint32_t q_off = (uint32_t) ((zi * (p.ty + 2) + yi) * p.xrp + x0) * 2u;
+    const uint32_t q_off = (uint32_t) ((qz * SY + qy) * p.xrp + qx) * 2u;
     uint32_t a[kWgCo16][4];
 #pragma unroll
     for (int g = 0; g < kWgCo16; g++)
@@ -534,10 +503,12 @@ __global__ void __launch_bounds__(kWgThreads, 2) k_conv3_wgrad_mma(TcWgrad p) {
           if (g < p.co16) mma_bf16(acc[k][g], a[g][0], a[g][1], a[g][2], a[g][3], b0, b1);
       }
     }
+    qx += 16;
+    while (qx >= p.w) {
+      qx -= p.w;
+      if (++qy == TY) { qy = 0; ++qz; }
+    }
   }
-  // bias: this block's row sums of gy, in row order
-  if (p.dobias && cz == 0 && tid < p.cout)
-    for (int rr = 0; rr < bz; rr++) bacc += brow[tid * 16 + rr];
   __syncthreads();  // the next block's staging overwrites the buffers
   }
   // partials: D[m = co][n = ci]; thread holds rows lane/4 (+8), columns 2 (lane%4) (+1)
@@ -556,9 +527,28 @@ __global__ void __launch_bounds__(kWgThreads, 2) k_conv3_wgrad_mma(TcWgrad p) {
       }
     }
   }
-  // bias partials (the first channel chunk's CTAs)
-  if (p.dobias && cz == 0 && tid < p.cout)
-    p.part[(size_t) gridDim.x * p.ncz * p.cout * 8 * 27 + (size_t) blockIdx.x * p.cout + tid] = bacc;
+}
+
+// Bias partials: pb[b][co] = sum of gy[co] over the b-th of nparts equal
+// voxel ranges, unrounded FP32 in a fixed order (thread strides, then a
+// fixed shuffle and warp tree), so every run gives the same sums.
+__global__ void k_wgrad_bias_part(const float *__restrict__ gy, float *__restrict__ pb, int cout, long vol,
+                                  int nparts) {
+  const int b = blockIdx.x, co = blockIdx.y;
+  const long lo = vol * b / nparts, hi = vol * (b + 1) / nparts;
+  const float *g = gy + (size_t) co * vol;
+  float s = 0.f;
+  for (long i = lo + threadIdx.x; i < hi; i += blockDim.x) s += __ldg(g + i);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  __shared__ float red[kWgThreads / 32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float t = 0.f;
+    for (int w = 0; w < kWgThreads / 32; w++) t += red[w];
+    pb[(size_t) b * cout + co] = t;
+  }
 }
 
 // gw[co][ci][t] += sum over the CTAs' partials: one warp per weight, lanes
@@ -690,6 +680,61 @@ int run_conv_tc(const float *x, const uint16_t *w, const float *bias, float *y, 
   return 0;
 }
 
+// Voxel block shapes of the weight gradient (tz x ty planes and rows of w
+// points), one kernel instance each.
+constexpr int kWgShapes[7][2] = {{4, 4}, {4, 2}, {2, 4}, {2, 2}, {2, 1}, {1, 2}, {1, 1}};
+
+using WgKernel = void (*)(TcWgrad);
+WgKernel wg_kernel(int s) {
+  switch (s) {
+    case 0: return k_conv3_wgrad_mma<4, 4>;
+    case 1: return k_conv3_wgrad_mma<4, 2>;
+    case 2: return k_conv3_wgrad_mma<2, 4>;
+    case 3: return k_conv3_wgrad_mma<2, 2>;
+    case 4: return k_conv3_wgrad_mma<2, 1>;
+    case 5: return k_conv3_wgrad_mma<1, 2>;
+    default: return k_conv3_wgrad_mma<1, 1>;
+  }
+}
+
+size_t wg_smem(int co16, int tz, int ty, int wd) {
+  const size_t qp = (size_t) tz * ty * wd + 8, xpp = (size_t) (tz + 2) * (ty + 2) * wd + 8;
+  return (16 * co16 * qp + 3 * 8 * xpp) * 2;
+}
+
+// Block shape of the weight gradient: the one with the least estimated time
+// per CTA, i.e. rounds of blocks (over the CTAs of one resident wave) times
+// a block's staging passes (kWgItems items per warp) and MMA steps; shapes
+// whose staging fits 108 KB run two CTAs per SM, up to 160 KB one.  -1 if
+// none fits.
+int wg_plan(int cin, int cout, int nb, int d, int h, int wd, int nsm, int rpi, int lgc) {
+  const int co16 = (cout + 15) / 16, ncz = (cin + 7) / 8;
+  int best = -1;
+  double best_cost = 0;
+  for (int s = 0; s < 7; s++) {
+    const int tz = kWgShapes[s][0], ty = kWgShapes[s][1];
+    if (tz > d || ty > h || d % tz || h % ty || (tz * ty * wd) % 16) continue;
+    const size_t smem = wg_smem(co16, tz, ty, wd);
+    if (smem > 160 * 1024) continue;
+    const int per = smem <= 108 * 1024 ? 2 : 1;
+    const long nctas = std::max(1, per * nsm / ncz);
+    const long nblk = (long) (nb * d / tz) * (h / ty);
+    const long rounds = (nblk + nctas - 1) / nctas;
+    auto passes = [&](long rows) {
+      const long items = rpi > 1 ? (rows + rpi - 1) / rpi : rows << lgc;
+      return (double) ((items + kWgItems * 8 - 1) / (kWgItems * 8));
+    };
+    const double block = passes(8L * (tz + 2) * (ty + 2)) + passes((long) cout * tz * ty) +
+                         0.15 * co16 * (tz * ty * wd / 16);
+    const double cost = rounds * block;
+    if (best < 0 || cost < best_cost) {
+      best = s;
+      best_cost = cost;
+    }
+  }
+  return best;
+}
+
 int run_wgrad_mma(const float *x, const float *gy, float *gw, float *gbias, int cin, int cout, int nb, int d, int h,
                   int wd) {
   TcWgrad p;
@@ -703,66 +748,54 @@ int run_wgrad_mma(const float *x, const float *gy, float *gw, float *gbias, int 
   p.w = wd;
   p.co16 = (cout + 15) / 16;
   p.ncz = (cin + 7) / 8;
-  p.dobias = gbias != nullptr;
-  // voxel block: tz x ty x w with tz ty w a multiple of 16; the largest
-  // block whose staging lets two CTAs share an SM (<= 108 KB), else the
-  // largest within 160 KB
-  const int cand[4][2] = {{2, 2}, {2, 1}, {1, 2}, {1, 1}};
-  const size_t caps[2] = {108 * 1024, 160 * 1024};
-  bool found = false;
-  size_t smem = 0;
-  for (int pass = 0; pass < 2 && !found; pass++) {
-    for (auto &c : cand) {
-      const int tz = c[0], ty = c[1];
-      if (tz > d || ty > h || d % tz || h % ty || (tz * ty * wd) % 16) continue;
-      const int nq = tz * ty * wd;
-      const int qp = nq + 8;
-      const int xpp = (tz + 2) * (ty + 2) * wd + 8;
-      smem = ((size_t) 16 * p.co16 * qp + (size_t) 3 * 8 * xpp) * 2;
-      if (smem > caps[pass]) continue;
-      p.tz = tz;
-      p.ty = ty;
-      p.qp = qp;
-      p.xrp = wd;
-      p.xpp = xpp;
-      p.xcp = 8 * xpp;
-      found = true;
-      break;
-    }
+  p.rpi = (wd < 32 && 32 % wd == 0) ? 32 / wd : 1;
+  p.lgc = 0;
+  if (p.rpi == 1)
+    while ((32 << p.lgc) < wd) p.lgc++;
+  int nsm = 148, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int s = wg_plan(cin, cout, nb, d, h, wd, nsm, p.rpi, p.lgc);
+  if (s < 0) return gb__set_error(1105, "unet weight gradient: no block plan fits");
+  const int tz = kWgShapes[s][0], ty = kWgShapes[s][1];
+  p.qp = tz * ty * wd + 8;
+  p.xrp = wd;
+  p.xpp = (tz + 2) * (ty + 2) * wd + 8;
+  p.xcp = 8 * p.xpp;
+  const size_t smem = wg_smem(p.co16, tz, ty, wd);
+  p.nblk = (nb * d / tz) * (h / ty);
+  const WgKernel kern = wg_kernel(s);
+  static bool attr[7] = {};
+  if (!attr[s]) {
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+    attr[s] = true;
   }
-  if (!found) return gb__set_error(1105, "unet weight gradient: no block plan fits");
-  p.nblk = (nb * d / p.tz) * (h / p.ty);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_conv3_wgrad_mma, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-    attr = true;
+  // CTAs per channel chunk: one resident wave over all chunks (all CTAs of
+  // the launch on the SMs at once), each CTA looping over its share of the
+  // voxel blocks
+  int per = 1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kern, kWgThreads, smem) != cudaSuccess || per < 1) {
+    cudaGetLastError();
+    per = 1;
   }
-  // CTAs per channel chunk: one resident wave over all chunks, each CTA
-  // looping over its share of the voxel blocks
-  int nsm = 148, per = 1;
-  {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_conv3_wgrad_mma, kWgThreads, smem) != cudaSuccess ||
-        per < 1) {
-      cudaGetLastError();
-      per = 1;
-    }
-  }
-  int nctas = (per * nsm + p.ncz - 1) / p.ncz;
+  int nctas = per * nsm / p.ncz;
   if (nctas > p.nblk) nctas = p.nblk;
   if (nctas < 1) nctas = 1;
   const size_t nwp = (size_t) nctas * p.ncz * cout * 8 * 27;
-  const size_t nparts = nwp + (p.dobias ? (size_t) nctas * cout : 0);
+  const size_t nparts = nwp + (gbias ? (size_t) nctas * cout : 0);
   p.part = (float *) gb__scratch(GB_SCR_UNET, nparts * sizeof(float));
   if (!p.part) return gb_last_error();
   cudaStream_t st = gb__stream();
-  k_conv3_wgrad_mma<<<dim3((unsigned) nctas, (unsigned) p.ncz), kWgThreads, smem, st>>>(p);
+  kern<<<dim3((unsigned) nctas, (unsigned) p.ncz), kWgThreads, smem, st>>>(p);
   GB_CHECK_LAUNCH("unet weight gradient");
-  const long nw = (long) cout * cin * 27 + (p.dobias ? cout : 0);
+  if (gbias) {
+    k_wgrad_bias_part<<<dim3((unsigned) nctas, (unsigned) cout), kWgThreads, 0, st>>>(gy, p.part + nwp, cout,
+                                                                                       (long) p.d * h * wd, nctas);
+    GB_CHECK_LAUNCH("unet bias gradient partials");
+  }
+  const long nw = (long) cout * cin * 27 + (gbias ? cout : 0);
   k_wgrad_reduce<<<(unsigned) ((nw * 32 + 255) / 256), 256, 0, st>>>(p.part, gw, gbias, cin, cout, nctas, p.ncz,
-                                                                       p.dobias);
+                                                                       gbias != nullptr);
   GB_CHECK_LAUNCH("unet weight gradient reduce");
   return 0;
 }
@@ -789,6 +822,14 @@ int gb__unet_conv_tc(const float *x, const uint16_t *w, const float *b, float *y
 
 int gb__unet_wgrad_tc(const float *x, const float *gy, float *gw, float *gb, int cin, int cout, int nb, int d, int h,
                       int wd) {
-  if (!g_tc_on || cout > 16 * kWgCo16 || wd < 16 || wd % 16) return -1;
+  if (!g_tc_on || cout > 16 * kWgCo16 || wd < 8 || wd % 8) return -1;
+  int nsm = 148, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int rpi = (wd < 32 && 32 % wd == 0) ? 32 / wd : 1;
+  int lgc = 0;
+  if (rpi == 1)
+    while ((32 << lgc) < wd) lgc++;
+  if (wg_plan(cin, cout, nb, d, h, wd, nsm, rpi, lgc) < 0) return -1;
   return run_wgrad_mma(x, gy, gw, gb, cin, cout, nb, d, h, wd);
 }

@@ -92,6 +92,7 @@ def _bind(lib):
         "gb_unet_adam": [V, V, V, V, V, L, F, F, F, F, F, F],
         "gb_unet_to_bf16": [V, V, L],
         "gb_unet_fill": [V, L, F],
+        "gb_unet_gather": [V, V, V, V, C.POINTER(C.c_int), I, I, L, I, L],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -354,6 +355,22 @@ class DeviceUNet:
                                % (scale, count))
         for b, (xp, yp) in enumerate(zip(x_dptrs, y_dptrs)):
             self.load_slot(b, xp, yp)
+        _ok(self.lib.gb_graph_launch(g), "graph launch")
+
+    def train_set_batch(self, ds, idx, scale):
+        """train_batch for samples idx of a device-resident set (DeviceSet):
+        one gather launch fills the batch slots (inputs and targets), then
+        one graph launch runs forward, loss gradient and backward."""
+        count = len(idx)
+        if not 1 <= count <= self.nb:
+            raise ValueError("train_set_batch: %d samples for a batch of %d" % (count, self.nb))
+        g = self._graphs.get(("train", float(scale), count))
+        if g is None:
+            raise RuntimeError("train_set_batch: no graph for loss scale %r and %d samples (call prepare_training "
+                               "first)" % (scale, count))
+        ix = (C.c_int * count)(*[int(i) for i in idx])
+        _ok(self.lib.gb_unet_gather(self._act("in"), self._tgt, ds.x, ds.y, ix, count, self.chan["in"], self.vol[0],
+                                    self.nb, ds.count), "gather")
         _ok(self.lib.gb_graph_launch(g), "graph launch")
 
     def prepare_training(self, scales, counts=None):
@@ -706,7 +723,7 @@ def train(net: DeviceUNet, ds: DeviceSet, epochs=60, batch=8, lr=2e-3, seed=0, l
         for b0 in range(0, nb, batch):
             idx = order[b0 : b0 + batch]
             if net.nb > 1:
-                net.train_batch([ds.xp(i) for i in idx], [ds.yp(i) for i in idx], 2.0 / (vol * len(idx)))
+                net.train_set_batch(ds, idx, 2.0 / (vol * len(idx)))
             else:
                 for i in idx:
                     net.train_sample(ds.xp(i), ds.yp(i), 2.0 / (vol * len(idx)))
@@ -802,7 +819,7 @@ def time_training_step(net: DeviceUNet, ds: DeviceSet, reps: int = 10):
             if r == 3:
                 _ok(lib.gb_event_record(0), "event")
             if with_bwd:
-                net.train_batch(xs, ys, 2.0 / (v * nb))
+                net.train_set_batch(ds, [0] * nb, 2.0 / (v * nb))
             else:
                 for b in range(nb):
                     net.load_slot(b, xs[b])
@@ -873,7 +890,8 @@ def main(argv=None):
         stopping="energy read every 10 steps; stop when the geometric estimate of the remaining distance to "
         "the limit and the last 10-step decrement are below %.0e Ha" % (a.tol / 2),
         params=int(net.nparam), epochs=a.epochs, batch=a.batch, samples_per_launch=net.nb, train_loss=loss,
-        data_seconds=t_data, train_seconds=t_train,
+        data_seconds=t_data, train_seconds=t_train, train_samples=a.train * a.epochs,
+        train_ms_per_sample=1e3 * t_train / (a.train * a.epochs),
         forward_ms=step_ms[0], forward_backward_ms=step_ms[1],
         data_steps_mean=float(np.mean([m["steps"] for m in meta])),
         steps_gauss=mean("steps_gauss"), steps_tf=mean("steps_tf"), steps_net=mean("steps_net"),

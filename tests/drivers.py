@@ -83,9 +83,10 @@ def run_batch_steps(steps: int = 8, prec: int = 0) -> None:
         api.free(o)
 
 
-def run_unet_step(n: int = 128, tensor_cores: int = 1, reps: int = 1) -> None:
+def run_unet_step(n: int = 128, tensor_cores: int = 1, reps: int = 1, batch: int = 1) -> None:
     """One forward and backward pass of the warm-start U-Net at n^3 with
-    random weights and inputs (tensor-core or SIMT convolutions)."""
+    random weights and inputs (tensor-core or SIMT convolutions), over
+    `batch` samples stacked in one launch per layer."""
     import ctypes as C
 
     import numpy as np
@@ -98,9 +99,10 @@ def run_unet_step(n: int = 128, tensor_cores: int = 1, reps: int = 1) -> None:
     api.lib.gb_unet_tensor_cores.argtypes = [C.c_int]
     api.lib.gb_unet_tensor_cores(tensor_cores)
     rng = np.random.default_rng(1)
-    net = ws.DeviceUNet(api, n, cin=3, seed=0)
-    net.set_input(rng.standard_normal((3, n, n, n)).astype(np.float32))
-    tgt = net.set_target(rng.standard_normal((n, n, n)).astype(np.float32))
+    net = ws.DeviceUNet(api, n, cin=3, seed=0, batch=batch)
+    x = rng.standard_normal((3, batch, n, n, n)).astype(np.float32)
+    api.lib.gb_h2d(net._act("in"), x.ctypes.data, x.nbytes)
+    tgt = net.set_target(rng.standard_normal((batch, n, n, n)).astype(np.float32))
     for _ in range(reps):
         net.forward()
         net.loss_grad(tgt)
@@ -155,7 +157,7 @@ if __name__ == "__main__":
     usage = ("usage: python tests/drivers.py gp [n] [steps] [prec: 0 FP64, 1 FP32]\n"
              "       python tests/drivers.py cn [n] [steps]\n"
              "       python tests/drivers.py batch [steps] [prec]\n"
-             "       python tests/drivers.py unet [n] [tensor cores: 1 or 0] [reps]\n"
+             "       python tests/drivers.py unet [n] [tensor cores: 1 or 0] [reps] [batch]\n"
              "       python tests/drivers.py ops [n]")
     if len(sys.argv) < 2 or sys.argv[1] not in ("gp", "cn", "batch", "unet", "ops"):
         sys.exit(usage)

@@ -62,10 +62,18 @@ class Dev:
             self.lib.gb_device_free(p)
 
 
+def _wgrad_on_tensor_cores(cout, shape):
+    d, h, w = shape
+    return (cout <= 64 and w % 8 == 0 and
+            any(d % tz == 0 and h % ty == 0 and (tz * ty * w) % 16 == 0 for tz in (1, 2, 4) for ty in (1, 2, 4)))
+
+
 @pytest.mark.parametrize("cin,cout,shape", [(5, 6, (6, 8, 10)), (24, 8, (8, 8, 8)), (96, 32, (4, 4, 4)), (3, 1, (5, 7, 3)),
                                             (8, 7, (16, 16, 20)), (64, 64, (4, 4, 4)), (8, 8, (4, 4, 128)),
                                             (24, 8, (4, 2, 32)), (16, 32, (2, 8, 16)), (96, 32, (4, 4, 32)),
-                                            (64, 64, (2, 2, 16)), (3, 8, (8, 4, 64)), (8, 1, (2, 4, 48))])
+                                            (64, 64, (2, 2, 16)), (3, 8, (8, 4, 64)), (8, 1, (2, 4, 48)),
+                                            (96, 32, (8, 8, 8)), (16, 17, (1, 2, 8)), (5, 9, (2, 1, 40)),
+                                            (8, 8, (2, 2, 24))])
 def test_conv_kernels_vs_oracle(lib, engine, cin, cout, shape):
     rng = np.random.default_rng(cin * 100 + cout)
     d = Dev(lib)
@@ -75,9 +83,10 @@ def test_conv_kernels_vs_oracle(lib, engine, cin, cout, shape):
     gy = rng.standard_normal((cout,) + shape).astype(np.float32)
     wr = uo.bf16_round(w)
     tc, tol = bool(engine), (TOL_TC if engine else TOL)
-    # the weight gradient runs on tensor cores for volumes 16 or more points
-    # wide (a multiple of 16) and up to 64 output channels
-    tc_w = tc and shape[2] % 16 == 0 and cout <= 64
+    # the weight gradient runs on tensor cores for volumes a multiple of 8
+    # points wide with a voxel block of a multiple of 16 points (tz x ty
+    # planes and rows, tz, ty in 1, 2, 4) and up to 64 output channels
+    tc_w = tc and _wgrad_on_tensor_cores(cout, shape)
     dx, dw, db, dgy = d.put(x), d.put(uo.bf16_bits(w)), d.put(b), d.put(gy)
     dy = d.put(np.zeros((cout,) + shape, np.float32))
     for relu in (0, 1):
@@ -330,3 +339,38 @@ def test_batched_network_matches_per_sample(b200, lib, engine):
         dev.free()
         one.free()
         four.free()
+
+
+def test_gather_fills_batch_slots(b200, lib):
+    """gb_unet_gather puts samples idx[b] of a device set into batch slots b
+    (inputs [cin][nb][vol], target [nb][vol]) as per-sample copies do, and
+    rejects an index outside the set without copying."""
+    rng = np.random.default_rng(5)
+    n, nset = 16, 5
+    vol = n**3
+    net = ws.DeviceUNet(b200, n, cin=3, seed=0, batch=4)
+    ds = ws.DeviceSet(lib, nset, vol)
+    try:
+        xs = rng.standard_normal((nset, 3, vol)).astype(np.float32)
+        ys = rng.standard_normal((nset, vol)).astype(np.float32)
+        assert lib.gb_h2d(ds.x, xs.ctypes.data, xs.nbytes) == 0
+        assert lib.gb_h2d(ds.y, ys.ctypes.data, ys.nbytes) == 0
+        idx = [4, 0, 4]
+        assert lib.gb_unet_fill(net._act("in"), 3 * 4 * vol, -1.0) == 0
+        assert lib.gb_unet_gather(net._act("in"), net._tgt, ds.x, ds.y, (C.c_int * 3)(*idx), 3, 3, vol, 4, nset) == 0
+        got = net.activation("in").reshape(3, 4, vol)
+        tgt = np.empty((4, vol), np.float32)
+        assert lib.gb_d2h(tgt.ctypes.data, net._tgt, tgt.nbytes) == 0
+        assert lib.gb_synchronize() == 0
+        for b, i in enumerate(idx):
+            assert np.array_equal(got[:, b], xs[i])
+            assert np.array_equal(tgt[b], ys[i])
+        assert np.all(got[:, 3] == -1.0)  # slot past count untouched
+        bad = (C.c_int * 2)(1, nset)
+        assert lib.gb_unet_gather(net._act("in"), net._tgt, ds.x, ds.y, bad, 2, 3, vol, 4, nset) == 1101
+        assert lib.gb_last_error() == 1101
+        lib.gb_clear_error()
+        assert np.array_equal(net.activation("in").reshape(3, 4, vol), got)
+    finally:
+        ds.free()
+        net.free()
