@@ -93,6 +93,7 @@ def _bind(lib):
         "gb_unet_to_bf16": [V, V, L],
         "gb_unet_fill": [V, L, F],
         "gb_unet_gather": [V, V, V, V, C.POINTER(C.c_int), I, I, L, I, L],
+        "gb_unet_tensor_cores": [I],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -831,6 +832,21 @@ def time_training_step(net: DeviceUNet, ds: DeviceSet, reps: int = 10):
     return out
 
 
+def time_simt_step(api, n, ds, reps: int = 10):
+    """Forward + loss + backward ms per sample of a batch-1 network on the
+    FP32 SIMT convolutions (gb_unet_tensor_cores(0)), the per-sample
+    training the tensor-core kernels and minibatch launches replace; the
+    tensor-core setting is restored afterwards."""
+    lib = api.lib
+    old = lib.gb_unet_tensor_cores(0)
+    net = DeviceUNet(api, n, cin=3, seed=0)
+    try:
+        return time_training_step(net, ds, reps)[1]
+    finally:
+        lib.gb_unet_tensor_cores(old)
+        net.free()
+
+
 def main(argv=None):
     """python -m libgrid_b200.warmstart [--n N] [--step H] [--train N] [--test N]
     [--epochs E] [--out report.json]: generate, train, evaluate and print one
@@ -875,6 +891,7 @@ def main(argv=None):
         api.lib.gb_synchronize()
         t_train = time.perf_counter() - t0
         step_ms = time_training_step(net, ds)
+        simt_ms = time_simt_step(api, a.n, ds)
         ds.free()
         note("trained in %.1f s" % t_train)
         inf = net.clone(1) if net.nb > 1 else net  # inference one potential at a time
@@ -893,6 +910,7 @@ def main(argv=None):
         data_seconds=t_data, train_seconds=t_train, train_samples=a.train * a.epochs,
         train_ms_per_sample=1e3 * t_train / (a.train * a.epochs),
         forward_ms=step_ms[0], forward_backward_ms=step_ms[1],
+        simt_forward_backward_ms=simt_ms, training_speedup_vs_simt=simt_ms / step_ms[1],
         data_steps_mean=float(np.mean([m["steps"] for m in meta])),
         steps_gauss=mean("steps_gauss"), steps_tf=mean("steps_tf"), steps_net=mean("steps_net"),
         sec_gauss=mean("sec_gauss"), sec_tf=mean("sec_tf"), sec_net=mean("sec_net"),
