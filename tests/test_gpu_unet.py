@@ -73,7 +73,7 @@ def _wgrad_on_tensor_cores(cout, shape):
                                             (24, 8, (4, 2, 32)), (16, 32, (2, 8, 16)), (96, 32, (4, 4, 32)),
                                             (64, 64, (2, 2, 16)), (3, 8, (8, 4, 64)), (8, 1, (2, 4, 48)),
                                             (96, 32, (8, 8, 8)), (16, 17, (1, 2, 8)), (5, 9, (2, 1, 40)),
-                                            (8, 8, (2, 2, 24))])
+                                            (8, 8, (2, 2, 24)), (32, 64, (2, 2, 8))])
 def test_conv_kernels_vs_oracle(lib, engine, cin, cout, shape):
     rng = np.random.default_rng(cin * 100 + cout)
     d = Dev(lib)
@@ -102,6 +102,33 @@ def test_conv_kernels_vs_oracle(lib, engine, cin, cout, shape):
     gw, gb = uo.conv3_bwd_weight(x, gy, tc_w)
     assert _rel(d.get(dgw, gw.shape), gw + gw0) < (TOL_TC if tc_w else TOL)
     assert _rel(d.get(dgb, gb.shape), gb + gb0) < TOL
+    assert lib.gb_last_error() == 0
+    d.free()
+
+
+@pytest.mark.parametrize("cin,cout,shape", [(24, 8, (4, 4, 8)), (16, 32, (4, 2, 16)), (8, 8, (2, 4, 32)),
+                                            (5, 3, (2, 3, 10))])
+def test_batched_weight_gradient_vs_oracle(lib, engine, cin, cout, shape):
+    """gb_unet_conv3_bwd_weight_nb over 3 samples stacked along depth gives
+    the sum of the samples' own weight and bias gradients: no tap reaches
+    across a sample boundary."""
+    rng = np.random.default_rng(cin + 7 * cout)
+    nb = 3
+    d = Dev(lib)
+    x = rng.standard_normal((cin, nb) + shape).astype(np.float32)
+    gy = rng.standard_normal((cout, nb) + shape).astype(np.float32)
+    tc_w = bool(engine) and _wgrad_on_tensor_cores(cout, shape)
+    gw = np.zeros((cout, cin, 27))
+    gb = np.zeros(cout)
+    for s in range(nb):
+        w_s, b_s = uo.conv3_bwd_weight(x[:, s], gy[:, s], tc_w)
+        gw += w_s
+        gb += b_s
+    dgw, dgb = d.put(np.zeros((cout, cin, 27), np.float32)), d.put(np.zeros(cout, np.float32))
+    dx, dgy = d.put(x), d.put(gy)
+    assert lib.gb_unet_conv3_bwd_weight_nb(dx, dgy, dgw, dgb, cin, cout, nb, *shape) == 0
+    assert _rel(d.get(dgw, gw.shape), gw) < (TOL_TC if tc_w else TOL)
+    assert _rel(d.get(dgb, gb.shape), gb) < TOL
     assert lib.gb_last_error() == 0
     d.free()
 
