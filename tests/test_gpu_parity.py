@@ -406,6 +406,34 @@ def test_predict_correct_vs_reference(b200, ref):
     assert rel(out[0][1], out[1][1]) < TOL_PSI
 
 
+@pytest.mark.parametrize("prop,tstep,cons,absorb", [
+    (FFT2, 0.05, 0.0, None),
+    (FFT2, 0.05, 0.013, None),
+    (FFT2, -0.05j, 0.0, None),
+    (FFT2, 0.04 - 0.01j, 0.002, None),
+    (FFT2, 0.05, 0.0, (3, 12, 2, 5, 4, 25)),  # FFT ignores the absorbing ramp here (src/grid_wf.c:593)
+    (CN2, 0.05, 0.0, (3, 12, 2, 5, 4, 25)),
+    (CN2, -0.05j, 0.01, None),
+])
+def test_propagate_potential_vs_reference(b200, ref, prop, tstep, cons, absorb):
+    """grid_wf_propagate_potential on its own (src/grid_wf.c:569-602):
+    psi *= exp(-i c (cons + V) / hbar), with the absorbing-region time
+    ramp of the CN propagators, against the compiled reference."""
+    shape, step, mass = (16, 8, 32), 0.4, 1.0
+    rng = np.random.default_rng(91)
+    psi0 = smooth_state(shape, step) + 0.01 * rand_c(rng, shape)
+    v = 0.05 * rng.standard_normal(shape) + 0.01j * rng.standard_normal(shape)
+    out = []
+    for api in (b200, ref):
+        w = api.wf(*shape, step, mass, PER, prop, values=psi0)
+        if absorb is not None:
+            api.lib.grid_wf_boundary(w.ptr, None, *absorb)
+        pot = api.cgrid(*shape, step, values=v)
+        api.lib.grid_wf_propagate_potential(w.ptr, capi.Complex.of(tstep), pot.ptr, cons)
+        out.append(w.grid.get())
+    assert rel(out[0], out[1]) < TOL_PSI
+
+
 def test_energy_and_error_vs_reference(b200, ref):
     shape, step, mass = (16, 16, 16), 0.4, 1.0
     x, y, z = workloads.mesh(*shape, step)
