@@ -28,10 +28,15 @@
 // A CTA stages gy of a voxel block (bf16, [co][q]) and three x-shifted copies
 // of the x halo block (dx = -1, 0, 1, bf16, [ci][row][x]), so every tap's
 // operand rows are 16-byte aligned for ldmatrix.  Warps split the taps.  A
-// resident wave of CTAs loops over the voxel blocks (CTA b takes blocks b,
-// b + grid, ...) with the accumulators in registers; each CTA's partial
-// sums go to scratch and a fixed-order pass (one warp per weight) adds them
-// to gw (deterministic, no atomics).
+// voxel block is tz x ty planes and rows of w >= 8 points (one kernel
+// instance per shape, chosen on the host by estimated time); the staging
+// issues eight loads per lane before any store, with rows of 8 or 16 points
+// packed several to a warp.  A resident wave of CTAs loops over the voxel
+// blocks (CTA b takes blocks b, b + grid, ...) with the accumulators in
+// registers; each CTA's partial sums go to scratch and a fixed-order pass
+// (one warp per weight) adds them to gw.  The bias gradient sums the
+// unrounded FP32 gy in its own fixed-order kernel (deterministic, no
+// atomics).
 //
 // Operands are rounded to bf16 (round to nearest even) and accumulated in
 // FP32; the numpy oracle applies the same rounding.
