@@ -34,7 +34,8 @@
 // packed several to a warp.  A resident wave of CTAs loops over the voxel
 // blocks (CTA b takes blocks b, b + grid, ...) with the accumulators in
 // registers; each CTA's partial sums go to scratch and a fixed-order pass
-// (one warp per weight) adds them to gw.  The bias gradient sums the
+// (one warp per weight, or one thread per weight when there are few
+// partials) adds them to gw.  The bias gradient sums the
 // unrounded FP32 gy in its own fixed-order kernel (deterministic, no
 // atomics).
 //
@@ -333,6 +334,7 @@ constexpr int kWgThreads = 256;  // 8 warps, warp w takes taps w, w + 8, ...
 constexpr int kWgTaps = 4;       // ceil(27 / 8)
 constexpr int kWgCo16 = 4;       // up to 64 output channels
 constexpr int kWgItems = 8;      // staging items a warp loads before any store
+constexpr int kWgReduceThreadParts = 64;  // up to this many partials: one thread per weight
 
 struct TcWgrad {
   const float *x, *gy;
@@ -586,6 +588,33 @@ __global__ void k_wgrad_reduce(const float *__restrict__ part, float *__restrict
   }
 }
 
+// The same sums with one thread per weight, for launches with few partials
+// (the coarse levels' few CTAs): partials b = 0, 1, ... in order, so every
+// run gives the same sum; consecutive threads read consecutive partials.
+__global__ void k_wgrad_reduce_t(const float *__restrict__ part, float *__restrict__ gw, float *__restrict__ gbias,
+                                 int cin, int cout, int nparts, int ncz, int dobias) {
+  const long nw = (long) cout * cin * 27;
+  const long i = (long) blockIdx.x * blockDim.x + threadIdx.x;
+  float s = 0.f;
+  if (i < nw) {
+    const int t = (int) (i % 27);
+    const long rest = i / 27;
+    const int ci = (int) (rest % cin), co = (int) (rest / cin);
+    const int cz = ci / 8, n = ci % 8;
+    const size_t stride = (size_t) ncz * cout * 8 * 27;
+    const float *p0 = part + ((size_t) cz * cout + co) * 8 * 27 + (size_t) n * 27 + t;
+#pragma unroll 8
+    for (int b = 0; b < nparts; b++) s += __ldg(p0 + (size_t) b * stride);
+    gw[i] += s;
+  } else if (dobias && i < nw + cout) {
+    const int co = (int) (i - nw);
+    const float *bp = part + (size_t) nparts * ncz * cout * 8 * 27;
+#pragma unroll 8
+    for (int b = 0; b < nparts; b++) s += __ldg(bp + (size_t) b * cout + co);
+    gbias[co] += s;
+  }
+}
+
 // ------------------------------------------------------------------ host side
 
 int g_tc_on = 1;
@@ -799,8 +828,12 @@ int run_wgrad_mma(const float *x, const float *gy, float *gw, float *gbias, int 
     GB_CHECK_LAUNCH("unet bias gradient partials");
   }
   const long nw = (long) cout * cin * 27 + (gbias ? cout : 0);
-  k_wgrad_reduce<<<(unsigned) ((nw * 32 + 255) / 256), 256, 0, st>>>(p.part, gw, gbias, cin, cout, nctas, p.ncz,
-                                                                       gbias != nullptr);
+  if (nctas <= kWgReduceThreadParts)
+    k_wgrad_reduce_t<<<(unsigned) ((nw + 255) / 256), 256, 0, st>>>(p.part, gw, gbias, cin, cout, nctas, p.ncz,
+                                                                     gbias != nullptr);
+  else
+    k_wgrad_reduce<<<(unsigned) ((nw * 32 + 255) / 256), 256, 0, st>>>(p.part, gw, gbias, cin, cout, nctas, p.ncz,
+                                                                         gbias != nullptr);
   GB_CHECK_LAUNCH("unet weight gradient reduce");
   return 0;
 }
